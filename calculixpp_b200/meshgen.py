@@ -1,0 +1,198 @@
+"""Seeded synthetic box meshes for the hex/wedge solid families.
+
+The reference has no mesh generator on this path (its decks come from .inp files);
+these structured meshes stand in for the decks the benchmark configurations describe.
+Node numbering follows a doubled lattice ordered x-fastest, then y, then z, so the
+CSR matrix has a narrow bandwidth and neighbouring elements share cache lines.
+
+Element node orders follow CalculiX / the reference:
+  C3D8  : shape8h.f corner order (src/fem/element.cpp:160-175)
+  C3D20 : corners then edge midsides 9-20 (src/fem/element.cpp:177-239)
+  C3D6  : triangle base then top (src/fem/element.cpp:241-253)
+  C3D15 : corners then midsides 1-2,2-3,3-1,4-5,5-6,6-4,1-4,2-5,3-6 (element.cpp:255-330)
+Wedges come from splitting each hex cell along the xy face diagonal between its
+corners 1 and 3 (0-based), giving two positively oriented prisms per cell.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+C3D8, C3D8R, C3D20, C3D20R, C3D6, C3D15 = 2, 3, 4, 5, 6, 7
+NODES = {C3D8: 8, C3D8R: 8, C3D20: 20, C3D20R: 20, C3D6: 6, C3D15: 15}
+NGP = {C3D8: 8, C3D8R: 1, C3D20: 27, C3D20R: 8, C3D6: 2, C3D15: 6}
+NAMES = {C3D8: "C3D8", C3D8R: "C3D8R", C3D20: "C3D20", C3D20R: "C3D20R",
+         C3D6: "C3D6", C3D15: "C3D15"}
+BY_NAME = {v: k for k, v in NAMES.items()}
+
+# Hex corner offsets in C3D8 order, on the unit cell.
+_HEX = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                 [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], dtype=np.int64)
+# C3D20 edges (pairs of corner indices) for midside nodes 9-20.
+_HEX_EDGES = np.array([[0, 1], [1, 2], [2, 3], [3, 0], [4, 5], [5, 6],
+                       [6, 7], [7, 4], [0, 4], [1, 5], [2, 6], [3, 7]])
+# Wedge splits of a hex cell (corner indices into _HEX): bottom triangle + top.
+_WEDGES = np.array([[0, 1, 3, 4, 5, 7], [1, 2, 3, 5, 6, 7]])
+_W15_EDGES = np.array([[0, 1], [1, 2], [2, 0], [3, 4], [4, 5], [5, 3],
+                       [0, 3], [1, 4], [2, 5]])
+
+
+@dataclass
+class Mesh:
+    """Nodes (N,3) float64, connectivity (E,n) int32 (0-based), one element type."""
+
+    coords: np.ndarray
+    conn: np.ndarray
+    etype: int
+    shape: tuple = ()
+    young: np.ndarray | None = None
+    poisson: np.ndarray | None = None
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n_nodes(self) -> int:
+        return int(self.coords.shape[0])
+
+    @property
+    def n_elems(self) -> int:
+        return int(self.conn.shape[0])
+
+
+def _lattice_nodes(n2, mask_fn):
+    """Compact index for doubled-lattice points (x fastest) selected by mask_fn."""
+    nx2, ny2, nz2 = n2
+    z, y, x = np.meshgrid(np.arange(nz2), np.arange(ny2), np.arange(nx2), indexing="ij")
+    mask = mask_fn(x, y, z)
+    index = np.full(mask.shape, -1, dtype=np.int64)
+    index[mask] = np.arange(int(mask.sum()))
+    pts = np.stack([x[mask], y[mask], z[mask]], axis=1)
+    return index, pts
+
+
+def box_mesh(etype: int, nx: int, ny: int, nz: int, lx=1.0, ly=1.0, lz=1.0,
+             jitter=0.0, seed=0) -> Mesh:
+    """Structured box [0,lx]x[0,ly]x[0,lz] of nx*ny*nz hex cells.
+
+    Hex types give one element per cell, wedge types two. Interior nodes (not on
+    the box faces) move by uniform(-jitter*h, +jitter*h) per axis, h the cell size
+    on that axis, drawn from numpy's default_rng(seed).
+    """
+    if etype not in NODES:
+        raise ValueError(f"unsupported element type {etype}")
+    quadratic = etype in (C3D20, C3D20R, C3D15)
+    nc = np.array([nx, ny, nz], dtype=np.int64)
+    if quadratic:
+        n2 = 2 * nc + 1
+        if etype == C3D15:
+            def mask(x, y, z):
+                return (z % 2 == 0) | ((x % 2 == 0) & (y % 2 == 0))
+        else:
+            def mask(x, y, z):
+                return ((x % 2) + (y % 2) + (z % 2)) <= 1
+        index, pts = _lattice_nodes(n2, mask)
+        scale = np.array([lx, ly, lz]) / (2 * nc)
+    else:
+        n2 = nc + 1
+        index, pts = _lattice_nodes(n2, lambda x, y, z: np.ones_like(x, dtype=bool))
+        scale = np.array([lx, ly, lz]) / nc
+    coords = pts.astype(np.float64) * scale
+
+    # Cell origins, x fastest.
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    cell = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1)
+    step = 2 if quadratic else 1
+    corner_lat = cell[:, None, :] * step + _HEX[None, :, :] * step  # (C,8,3)
+
+    def lat_index(p):
+        return index[p[..., 2], p[..., 1], p[..., 0]]
+
+    if etype in (C3D8, C3D8R):
+        conn = lat_index(corner_lat)
+    elif etype in (C3D20, C3D20R):
+        mids = (corner_lat[:, _HEX_EDGES[:, 0]] + corner_lat[:, _HEX_EDGES[:, 1]]) // 2
+        conn = np.concatenate([lat_index(corner_lat), lat_index(mids)], axis=1)
+    else:
+        w = corner_lat[:, _WEDGES]  # (C,2,6,3)
+        w = w.reshape(-1, 6, 3)
+        if etype == C3D6:
+            conn = lat_index(w)
+        else:
+            mids = (w[:, _W15_EDGES[:, 0]] + w[:, _W15_EDGES[:, 1]]) // 2
+            conn = np.concatenate([lat_index(w), lat_index(mids)], axis=1)
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    if np.any(conn < 0):
+        raise AssertionError("lattice index miss while building connectivity")
+
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        h = np.array([lx / nx, ly / ny, lz / nz])
+        lo = np.zeros(3)
+        hi = np.array([lx, ly, lz])
+        eps = 1e-9 * hi
+        interior = np.all((coords > lo + eps) & (coords < hi - eps), axis=1)
+        d = rng.uniform(-1.0, 1.0, size=coords.shape) * (jitter * h)
+        coords = coords + d * interior[:, None]
+    return Mesh(coords=np.ascontiguousarray(coords), conn=conn, etype=etype,
+                shape=(nx, ny, nz))
+
+
+def face_nodes(mesh: Mesh, axis: int, value: float, tol=1e-9) -> np.ndarray:
+    """Node indices on the plane coords[:, axis] == value."""
+    return np.nonzero(np.abs(mesh.coords[:, axis] - value) <= tol * max(1.0, abs(value) + 1.0))[0]
+
+
+def clamp_face_spc(mesh: Mesh, axis=0, value=0.0):
+    """SPC arrays (node, comp, value) fixing all three components on one face."""
+    nodes = face_nodes(mesh, axis, value)
+    spc_node = np.repeat(nodes, 3).astype(np.int32)
+    spc_comp = np.tile(np.arange(3), nodes.size).astype(np.int32)
+    return spc_node, spc_comp, np.zeros(spc_node.size)
+
+
+def dof_map(n_nodes: int, spc_node, spc_comp, spc_val):
+    """Free-DOF numbering of an SPC-only model, restating constraint_transform.cpp:78-82:
+    free DOFs are numbered in global order g = 3*node + comp."""
+    ndof = 3 * n_nodes
+    constrained = np.zeros(ndof, dtype=bool)
+    prescribed = np.zeros(ndof)
+    g = 3 * np.asarray(spc_node, dtype=np.int64) + np.asarray(spc_comp, dtype=np.int64)
+    constrained[g] = True
+    prescribed[g] = spc_val
+    dof_eq = np.full(ndof, -1, dtype=np.int32)
+    free = ~constrained
+    dof_eq[free] = np.arange(int(free.sum()), dtype=np.int32)
+    return dof_eq, prescribed, int(free.sum())
+
+
+def cantilever_c3d8_config1(seed=0) -> dict:
+    """Plain FP64 linear-static C3D8 cantilever: 20x4x4 hexes of a 100x10x10 box,
+    interior nodes jittered by uniform +-0.1*h, E=210000, nu=0.3, face x=0 clamped,
+    total load -1000 in z split evenly over the x=100 face nodes."""
+    m = box_mesh(C3D8, 20, 4, 4, 100.0, 10.0, 10.0, jitter=0.1, seed=seed)
+    m.young = np.full(m.n_elems, 210000.0)
+    m.poisson = np.full(m.n_elems, 0.3)
+    spc = clamp_face_spc(m, 0, 0.0)
+    tip = face_nodes(m, 0, 100.0)
+    f_ext = np.zeros(3 * m.n_nodes)
+    f_ext[3 * tip + 2] = -1000.0 / tip.size
+    return {"mesh": m, "spc": spc, "f_ext": f_ext, "tip": tip}
+
+
+def lognormal_young(n, median=200000.0, sigma=0.3, seed=0):
+    rng = np.random.default_rng(seed + 7919)
+    return median * np.exp(sigma * rng.standard_normal(n))
+
+
+def c3d20_block(n=64, seed=0) -> dict:
+    """C3D20 full-integration block: n^3 quadratic hexes of a unit cube, node jitter
+    uniform +-0.05*h, per-element E lognormal (median 200000, sigma 0.3), nu=0.3.
+    For displacement checks: z=0 face clamped, unit total load in +x on z=1."""
+    m = box_mesh(C3D20, n, n, n, 1.0, 1.0, 1.0, jitter=0.05, seed=seed)
+    m.young = lognormal_young(m.n_elems, seed=seed)
+    m.poisson = np.full(m.n_elems, 0.3)
+    spc = clamp_face_spc(m, 2, 0.0)
+    top = face_nodes(m, 2, 1.0)
+    f_ext = np.zeros(3 * m.n_nodes)
+    f_ext[3 * top + 0] = 1.0 / top.size
+    return {"mesh": m, "spc": spc, "f_ext": f_ext}

@@ -1,0 +1,938 @@
+/* cxo — CPU restatement of CalculiX++'s element-integration / J2 / assembly path.
+ * TEST INFRASTRUCTURE ONLY (see cxo.h). Every function names the reference file:line
+ * it restates. Operation order follows the reference so that, compiled with
+ * -ffp-contract=off, results are bit-identical to the reference's own code. */
+#include "cxo.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+static _Thread_local char g_err[256];
+
+static int fail(const char* msg) {
+  snprintf(g_err, sizeof g_err, "%s", msg);
+  return -1;
+}
+
+const char* cxo_last_error(void) { return g_err; }
+
+enum { T_C3D8 = 2, T_C3D8R = 3, T_C3D20 = 4, T_C3D20R = 5, T_C3D6 = 6, T_C3D15 = 7 };
+#define MAXN 20
+
+/* include/calculixpp/core/element.hpp:24-44 */
+int cxo_nodes_per_element(int type) {
+  switch (type) {
+    case T_C3D8: case T_C3D8R: return 8;
+    case T_C3D20: case T_C3D20R: return 20;
+    case T_C3D6: return 6;
+    case T_C3D15: return 15;
+    default: return 0;
+  }
+}
+
+/* ---- Gauss rules: src/fem/element.cpp:22-126 ------------------------------------ */
+static const double kG2 = 0.577350269189625764;
+static const double kG3 = 0.774596669241483377;
+
+int cxo_gauss_rule(int type, double* out) {
+  int n = 0;
+#define GP(a, b, c, w) do { out[4*n] = (a); out[4*n+1] = (b); out[4*n+2] = (c); out[4*n+3] = (w); ++n; } while (0)
+  switch (type) {
+    case T_C3D8:
+    case T_C3D20R:
+      /* 2x2x2, xi fastest (element.cpp:32-37) */
+      for (int c = 0; c < 2; ++c)
+        for (int b = 0; b < 2; ++b)
+          for (int a = 0; a < 2; ++a)
+            GP(a ? kG2 : -kG2, b ? kG2 : -kG2, c ? kG2 : -kG2, 1.0);
+      break;
+    case T_C3D8R:
+      GP(0.0, 0.0, 0.0, 8.0); /* element.cpp:40 */
+      break;
+    case T_C3D20: {
+      /* 3x3x3 Gauss-Legendre (element.cpp:43-62) */
+      const double nodes[3] = {-kG3, 0.0, kG3};
+      const double wts[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+      for (int c = 0; c < 3; ++c)
+        for (int b = 0; b < 3; ++b)
+          for (int a = 0; a < 3; ++a) GP(nodes[a], nodes[b], nodes[c], wts[a] * wts[b] * wts[c]);
+      break;
+    }
+    case T_C3D6:
+      GP(1.0 / 3.0, 1.0 / 3.0, -kG2, 0.5); /* element.cpp:68-71 */
+      GP(1.0 / 3.0, 1.0 / 3.0, kG2, 0.5);
+      break;
+    case T_C3D15: {
+      const double kT = 1.0 / 6.0, kU = 2.0 / 3.0; /* element.cpp:72-77 */
+      GP(kT, kT, -kG2, kT); GP(kU, kT, -kG2, kT); GP(kT, kU, -kG2, kT);
+      GP(kT, kT, kG2, kT); GP(kU, kT, kG2, kT); GP(kT, kU, kG2, kT);
+      break;
+    }
+    default:
+      return 0;
+  }
+#undef GP
+  return n;
+}
+
+/* ---- shape functions: src/fem/element.cpp:160-359 ------------------------------- */
+static const int kHexSign[8][3] = {
+    {-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+    {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1},
+};
+static const int kMidHex[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                   {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+static const int kEdgeAxis[12] = {0, 1, 0, 1, 0, 1, 0, 1, 2, 2, 2, 2};
+
+static void shape_c3d8(double xi, double et, double ze, double* N, double* dN) {
+  for (int k = 0; k < 8; ++k) {
+    const double sg = kHexSign[k][0], sh = kHexSign[k][1], sr = kHexSign[k][2];
+    const double g = 1.0 + sg * xi, h = 1.0 + sh * et, r = 1.0 + sr * ze;
+    N[k] = g * h * r / 8.0;
+    dN[3 * k + 0] = sg * h * r / 8.0;
+    dN[3 * k + 1] = sh * g * r / 8.0;
+    dN[3 * k + 2] = sr * g * h / 8.0;
+  }
+}
+
+static void shape_c3d20(double xi, double et, double ze, double* N, double* dN) {
+  const double p[3] = {xi, et, ze};
+  for (int k = 0; k < 8; ++k) {
+    const double sgn[3] = {kHexSign[k][0], kHexSign[k][1], kHexSign[k][2]};
+    const double g = 1.0 + sgn[0] * xi, h = 1.0 + sgn[1] * et, r = 1.0 + sgn[2] * ze;
+    const double q = sgn[0] * xi + sgn[1] * et + sgn[2] * ze - 2.0;
+    N[k] = g * h * r * q / 8.0;
+    const double fac[3] = {g, h, r};
+    for (int d = 0; d < 3; ++d) {
+      double others = 1.0;
+      for (int m = 0; m < 3; ++m)
+        if (m != d) others *= fac[m];
+      dN[3 * k + d] = (sgn[d] * others * q + g * h * r * sgn[d]) / 8.0;
+    }
+  }
+  for (int j = 0; j < 12; ++j) {
+    const int node = 8 + j;
+    const int a = kEdgeAxis[j];
+    const int c0 = kMidHex[j][0];
+    const double sgn[3] = {kHexSign[c0][0], kHexSign[c0][1], kHexSign[c0][2]};
+    const double pa = p[a];
+    double plane = 1.0;
+    for (int m = 0; m < 3; ++m)
+      if (m != a) plane *= 1.0 + sgn[m] * p[m];
+    N[node] = (1.0 - pa * pa) * plane / 4.0;
+    for (int d = 0; d < 3; ++d) {
+      if (d == a) {
+        dN[3 * node + d] = (-2.0 * pa) * plane / 4.0;
+      } else {
+        double other = 1.0;
+        for (int m = 0; m < 3; ++m)
+          if (m != a && m != d) other *= 1.0 + sgn[m] * p[m];
+        dN[3 * node + d] = (1.0 - pa * pa) * sgn[d] * other / 4.0;
+      }
+    }
+  }
+}
+
+static void shape_c3d6(double xi, double et, double ze, double* N, double* dN) {
+  const double a = 1.0 - xi - et;
+  const double m = 0.5 * (1.0 - ze), p = 0.5 * (1.0 + ze);
+  const double n6[6] = {a * m, xi * m, et * m, a * p, xi * p, et * p};
+  const double d6[18] = {-m, -m, -0.5 * a, m, 0.0, -0.5 * xi, 0.0, m, -0.5 * et,
+                         -p, -p, 0.5 * a,  p, 0.0, 0.5 * xi,  0.0, p, 0.5 * et};
+  memcpy(N, n6, sizeof n6);
+  memcpy(dN, d6, sizeof d6);
+}
+
+static void shape_c3d15(double xi, double et, double ze, double* N, double* dN) {
+  const double a = 1.0 - xi - et;
+  const double omz = 1.0 - ze, opz = 1.0 + ze, omz2 = 1.0 - ze * ze;
+  N[0] = -0.5 * a * omz * (2 * xi + 2 * et + ze);
+  N[1] = 0.5 * xi * omz * (2 * xi - 2 - ze);
+  N[2] = 0.5 * et * omz * (2 * et - 2 - ze);
+  N[3] = -0.5 * a * opz * (2 * xi + 2 * et - ze);
+  N[4] = 0.5 * xi * opz * (2 * xi - 2 + ze);
+  N[5] = 0.5 * et * opz * (2 * et - 2 + ze);
+  N[6] = 2 * xi * a * omz;
+  N[7] = 2 * xi * et * omz;
+  N[8] = 2 * et * a * omz;
+  N[9] = 2 * xi * a * opz;
+  N[10] = 2 * xi * et * opz;
+  N[11] = 2 * et * a * opz;
+  N[12] = a * omz2;
+  N[13] = xi * omz2;
+  N[14] = et * omz2;
+  const double dxi[15] = {0.5 * omz * (4 * xi + 4 * et + ze - 2),
+                          0.5 * omz * (4 * xi - ze - 2),
+                          0.0,
+                          0.5 * opz * (4 * xi + 4 * et - ze - 2),
+                          0.5 * opz * (4 * xi + ze - 2),
+                          0.0,
+                          2 * omz * (1 - 2 * xi - et),
+                          2 * et * omz,
+                          -2 * et * omz,
+                          2 * opz * (1 - 2 * xi - et),
+                          2 * et * opz,
+                          -2 * et * opz,
+                          -omz2,
+                          omz2,
+                          0.0};
+  const double det[15] = {0.5 * omz * (4 * xi + 4 * et + ze - 2),
+                          0.0,
+                          0.5 * omz * (4 * et - ze - 2),
+                          0.5 * opz * (4 * xi + 4 * et - ze - 2),
+                          0.0,
+                          0.5 * opz * (4 * et + ze - 2),
+                          -2 * xi * omz,
+                          2 * xi * omz,
+                          2 * omz * (1 - xi - 2 * et),
+                          -2 * xi * opz,
+                          2 * xi * opz,
+                          2 * opz * (1 - xi - 2 * et),
+                          -omz2,
+                          0.0,
+                          omz2};
+  double dz[15];
+  dz[0] = -0.5 * a * (-1.0 * (2 * xi + 2 * et + ze) + omz * 1.0);
+  dz[1] = 0.5 * xi * (-1.0 * (2 * xi - 2 - ze) + omz * (-1.0));
+  dz[2] = 0.5 * et * (-1.0 * (2 * et - 2 - ze) + omz * (-1.0));
+  dz[3] = -0.5 * a * (1.0 * (2 * xi + 2 * et - ze) + opz * (-1.0));
+  dz[4] = 0.5 * xi * (1.0 * (2 * xi - 2 + ze) + opz * (1.0));
+  dz[5] = 0.5 * et * (1.0 * (2 * et - 2 + ze) + opz * (1.0));
+  dz[6] = -2 * xi * a;
+  dz[7] = -2 * xi * et;
+  dz[8] = -2 * et * a;
+  dz[9] = 2 * xi * a;
+  dz[10] = 2 * xi * et;
+  dz[11] = 2 * et * a;
+  dz[12] = a * (-2 * ze);
+  dz[13] = xi * (-2 * ze);
+  dz[14] = et * (-2 * ze);
+  for (int k = 0; k < 15; ++k) {
+    dN[3 * k] = dxi[k];
+    dN[3 * k + 1] = det[k];
+    dN[3 * k + 2] = dz[k];
+  }
+}
+
+int cxo_shape(int type, double xi, double et, double ze, double* N, double* dN) {
+  switch (type) {
+    case T_C3D8: case T_C3D8R: shape_c3d8(xi, et, ze, N, dN); return 8;
+    case T_C3D20: case T_C3D20R: shape_c3d20(xi, et, ze, N, dN); return 20;
+    case T_C3D6: shape_c3d6(xi, et, ze, N, dN); return 6;
+    case T_C3D15: shape_c3d15(xi, et, ze, N, dN); return 15;
+    default: return 0;
+  }
+}
+
+/* ---- physical gradients: src/fem/element.cpp:80-102, 361-380 ------------------- */
+static int gradients_from_shape(int n, const double* dN, const double* x, double* g,
+                                double* det_out) {
+  double J[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < n; ++k) v += x[3 * k + i] * dN[3 * k + j];
+      J[i][j] = v;
+    }
+  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  if (det <= 0.0) return fail("non-positive element Jacobian (bad connectivity?)");
+  const double inv = 1.0 / det;
+  const double Jinv[3][3] = {
+      {c00 * inv, (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * inv,
+       (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * inv},
+      {c01 * inv, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * inv,
+       (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * inv},
+      {c02 * inv, (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * inv,
+       (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * inv},
+  };
+  double invT[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) invT[i][j] = Jinv[j][i];
+  for (int k = 0; k < n; ++k)
+    for (int i = 0; i < 3; ++i) {
+      double v = 0.0;
+      for (int j = 0; j < 3; ++j) v += invT[i][j] * dN[3 * k + j];
+      g[3 * k + i] = v;
+    }
+  *det_out = det;
+  return 0;
+}
+
+int cxo_physical_gradients(int type, double xi, double et, double ze,
+                           const double* coords, double* grad, double* det) {
+  double N[MAXN], dN[3 * MAXN];
+  const int n = cxo_shape(type, xi, et, ze, N, dN);
+  if (n == 0) return fail("unsupported element type");
+  return gradients_from_shape(n, dN, coords, grad, det);
+}
+
+/* element.cpp:424-433 */
+int cxo_element_volume(int type, const double* coords, double* vol) {
+  double gp[4 * 27], g[3 * MAXN], det;
+  const int ng = cxo_gauss_rule(type, gp);
+  double v = 0.0;
+  for (int q = 0; q < ng; ++q) {
+    if (cxo_physical_gradients(type, gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], coords, g, &det))
+      return -1;
+    v += det * gp[4 * q + 3];
+  }
+  *vol = v;
+  return 0;
+}
+
+/* ---- constitutive pieces --------------------------------------------------------- */
+/* element.cpp:382-392 */
+static double b_entry(int row, const double* gk, int dir) {
+  const double gx = gk[0], gy = gk[1], gz = gk[2];
+  switch (row) {
+    case 0: return dir == 0 ? gx : 0.0;
+    case 1: return dir == 1 ? gy : 0.0;
+    case 2: return dir == 2 ? gz : 0.0;
+    case 3: return dir == 0 ? gy : (dir == 1 ? gx : 0.0);
+    case 4: return dir == 0 ? gz : (dir == 2 ? gx : 0.0);
+    default: return dir == 1 ? gz : (dir == 2 ? gy : 0.0);
+  }
+}
+
+/* element.cpp:410-422 */
+static void elastic_D(double E, double nu, double* D) {
+  const double um2 = E / (1.0 + nu);
+  const double lam = nu * um2 / (1.0 - 2.0 * nu);
+  const double mu = um2 / 2.0;
+  const double lam2mu = lam + um2;
+  memset(D, 0, 36 * sizeof(double));
+  D[0] = D[7] = D[14] = lam2mu;
+  D[1] = D[2] = D[6] = D[8] = D[12] = D[13] = lam;
+  D[21] = D[28] = D[35] = mu;
+}
+
+/* element.cpp:440-462 */
+static void accumulate_ktangent(const double* g, int ndof, const double* D, double scale,
+                                double* Ke) {
+  for (int a = 0; a < ndof; ++a) {
+    const int ka = a / 3, da = a % 3;
+    double DBa[6];
+    for (int row = 0; row < 6; ++row) {
+      double v = 0.0;
+      for (int r = 0; r < 6; ++r) v += D[6 * row + r] * b_entry(r, g + 3 * ka, da);
+      DBa[row] = v;
+    }
+    for (int b = a; b < ndof; ++b) {
+      const int kb = b / 3, db = b % 3;
+      double v = 0.0;
+      for (int row = 0; row < 6; ++row) v += b_entry(row, g + 3 * kb, db) * DBa[row];
+      Ke[a * ndof + b] += scale * v;
+    }
+  }
+}
+
+/* element.cpp:465-475 */
+static void accumulate_fint(const double* g, int ndof, const double* sigma, double scale,
+                            double* fe) {
+  for (int a = 0; a < ndof; ++a) {
+    const int ka = a / 3, da = a % 3;
+    double v = 0.0;
+    for (int row = 0; row < 6; ++row) v += b_entry(row, g + 3 * ka, da) * sigma[row];
+    fe[a] += scale * v;
+  }
+}
+
+/* element.cpp:511-518 */
+static void mirror_upper(int ndof, double* Ke) {
+  for (int a = 0; a < ndof; ++a)
+    for (int b = a + 1; b < ndof; ++b) Ke[b * ndof + a] = Ke[a * ndof + b];
+}
+
+/* element.cpp:394-408 */
+static void strain_from_gradients(const double* g, int n, const double* ue, double* eps) {
+  double du[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < n; ++k) v += g[3 * k + j] * ue[3 * k + i];
+      du[i][j] = v;
+    }
+  eps[0] = du[0][0];
+  eps[1] = du[1][1];
+  eps[2] = du[2][2];
+  eps[3] = du[0][1] + du[1][0];
+  eps[4] = du[0][2] + du[2][0];
+  eps[5] = du[1][2] + du[2][1];
+}
+
+/* ---- C3D8R hourglass control: element.cpp:529-610 ------------------------------- */
+static const double kHgGamma[4][8] = {
+    {1, 1, -1, -1, -1, -1, 1, 1},
+    {1, -1, -1, 1, -1, 1, 1, -1},
+    {1, -1, 1, -1, 1, -1, 1, -1},
+    {-1, 1, -1, 1, 1, -1, 1, -1},
+};
+
+typedef struct {
+  double gamma[4][8];
+  double kappa;
+} hourglass_t;
+
+static int build_hourglass(const double* x, double mu, hourglass_t* hg) {
+  double N[8], dN[24], b[24], det;
+  shape_c3d8(0.0, 0.0, 0.0, N, dN);
+  if (gradients_from_shape(8, dN, x, b, &det)) return -1;
+  const double vol = 8.0 * det;
+  for (int al = 0; al < 4; ++al) {
+    double gx[3] = {0, 0, 0};
+    for (int j = 0; j < 8; ++j)
+      for (int d = 0; d < 3; ++d) gx[d] += kHgGamma[al][j] * x[3 * j + d];
+    for (int j = 0; j < 8; ++j) {
+      double corr = 0.0;
+      for (int d = 0; d < 3; ++d) corr += gx[d] * b[3 * j + d];
+      hg->gamma[al][j] = kHgGamma[al][j] - corr;
+    }
+  }
+  double b2 = 0.0;
+  for (int j = 0; j < 8; ++j)
+    for (int d = 0; d < 3; ++d) b2 += b[3 * j + d] * b[3 * j + d];
+  const double c_hg = 0.05;
+  hg->kappa = c_hg * mu * vol * b2;
+  return 0;
+}
+
+static void accumulate_hourglass(const hourglass_t* hg, double* Ke) {
+  for (int al = 0; al < 4; ++al)
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j) {
+        const double kij = hg->kappa * hg->gamma[al][i] * hg->gamma[al][j];
+        for (int d = 0; d < 3; ++d) {
+          const int a = i * 3 + d, bc = j * 3 + d;
+          if (bc >= a) Ke[a * 24 + bc] += kij;
+        }
+      }
+}
+
+static void accumulate_hourglass_force(const hourglass_t* hg, const double* ue, double* fe) {
+  for (int al = 0; al < 4; ++al) {
+    double gu[3] = {0, 0, 0};
+    for (int j = 0; j < 8; ++j)
+      for (int d = 0; d < 3; ++d) gu[d] += hg->gamma[al][j] * ue[3 * j + d];
+    for (int i = 0; i < 8; ++i)
+      for (int d = 0; d < 3; ++d) fe[i * 3 + d] += hg->kappa * hg->gamma[al][i] * gu[d];
+  }
+}
+
+/* ---- element_stiffness: element.cpp:614-634 ------------------------------------- */
+int cxo_element_stiffness(int type, const double* x, double E, double nu, double* Ke) {
+  const int n = cxo_nodes_per_element(type);
+  if (n == 0) return fail("unsupported element type");
+  const int ndof = 3 * n;
+  double D[36], gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det;
+  elastic_D(E, nu, D);
+  memset(Ke, 0, (size_t)ndof * ndof * sizeof(double));
+  const int ng = cxo_gauss_rule(type, gp);
+  for (int q = 0; q < ng; ++q) {
+    cxo_shape(type, gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
+    if (gradients_from_shape(n, dN, x, g, &det)) return -1;
+    accumulate_ktangent(g, ndof, D, det * gp[4 * q + 3], Ke);
+  }
+  if (type == T_C3D8R) {
+    const double mu = E / (2.0 * (1.0 + nu));
+    hourglass_t hg;
+    if (build_hourglass(x, mu, &hg)) return -1;
+    accumulate_hourglass(&hg, Ke);
+  }
+  mirror_upper(ndof, Ke);
+  return 0;
+}
+
+/* ---- J2 plasticity: src/fem/plasticity.cpp:20-236 ------------------------------- */
+static const double kSqrt3_2 = 1.224744871391589;
+
+typedef struct {
+  double E, nu, mu, h_kin;
+  int n;
+  const double* ep;
+  double sy[64];
+  double De[36];
+} j2_t;
+
+/* plasticity.cpp:42-65 */
+static int j2_init(const cxo_material* m, j2_t* j) {
+  if (m->n_plastic <= 0) return fail("J2PlasticMaterial needs a non-empty *PLASTIC table");
+  if (m->n_plastic > 64) return fail("*PLASTIC table longer than 64 points");
+  j->E = m->E;
+  j->nu = m->nu;
+  j->mu = m->E / (2.0 * (1.0 + m->nu));
+  j->h_kin = m->h_kin;
+  j->n = m->n_plastic;
+  j->ep = m->eqplastic;
+  for (int i = 0; i < j->n; ++i) j->sy[i] = m->yield[i];
+  if (m->hardening == 1 || m->hardening == 2) {
+    if (j->h_kin == 0.0 && j->n >= 2 && j->ep[1] > j->ep[0])
+      j->h_kin = (j->sy[1] - j->sy[0]) / (j->ep[1] - j->ep[0]);
+    if (m->hardening == 1)
+      for (int i = 0; i < j->n; ++i) j->sy[i] = j->sy[0];
+  }
+  elastic_D(m->E, m->nu, j->De);
+  return 0;
+}
+
+/* plasticity.cpp:67-88 */
+static void j2_hardening(const j2_t* j, double ep, double* sigma_y, double* h_iso) {
+  const int n = j->n;
+  if (n == 1 || ep <= j->ep[0]) {
+    *sigma_y = j->sy[0];
+    *h_iso = 0.0;
+    return;
+  }
+  if (ep >= j->ep[n - 1]) {
+    *sigma_y = j->sy[n - 1];
+    *h_iso = 0.0;
+    return;
+  }
+  for (int i = 0; i + 1 < n; ++i) {
+    if (ep >= j->ep[i] && ep <= j->ep[i + 1]) {
+      *h_iso = (j->sy[i + 1] - j->sy[i]) / (j->ep[i + 1] - j->ep[i]);
+      *sigma_y = j->sy[i] + *h_iso * (ep - j->ep[i]);
+      return;
+    }
+  }
+  *sigma_y = j->sy[n - 1];
+  *h_iso = 0.0;
+}
+
+static double contract6(const double* s) {
+  return s[0] * s[0] + s[1] * s[1] + s[2] * s[2] + 2.0 * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+}
+
+/* plasticity.cpp:90-236. committed/trial: eps_p[6], ep, alpha[6]. */
+static void j2_evaluate(const j2_t* j, const double* strain, const double* cs, double* ts,
+                        double* stress, double* tangent) {
+  double el[6], sig_tr[6], s_tr[6], xi[6];
+  for (int i = 0; i < 6; ++i) el[i] = strain[i] - cs[i];
+  for (int i = 0; i < 6; ++i) {
+    double v = 0.0;
+    for (int k = 0; k < 6; ++k) v += j->De[6 * i + k] * el[k];
+    sig_tr[i] = v;
+  }
+  {
+    const double p = (sig_tr[0] + sig_tr[1] + sig_tr[2]) / 3.0;
+    s_tr[0] = sig_tr[0] - p;
+    s_tr[1] = sig_tr[1] - p;
+    s_tr[2] = sig_tr[2] - p;
+    s_tr[3] = sig_tr[3];
+    s_tr[4] = sig_tr[4];
+    s_tr[5] = sig_tr[5];
+  }
+  for (int i = 0; i < 6; ++i) xi[i] = s_tr[i] - cs[7 + i];
+  const double xi_norm = sqrt(contract6(xi));
+  const double q_tr = kSqrt3_2 * xi_norm;
+  double sy0, h0;
+  j2_hardening(j, cs[6], &sy0, &h0);
+  const double f_tr = q_tr - sy0;
+  if (f_tr <= 0.0 || xi_norm == 0.0) {
+    memcpy(stress, sig_tr, sizeof sig_tr);
+    memcpy(tangent, j->De, 36 * sizeof(double));
+    memcpy(ts, cs, 13 * sizeof(double));
+    return;
+  }
+  const double ep0 = cs[6];
+  double dgamma = 0.0;
+  for (int it = 0; it < 50; ++it) {
+    double sy, h_iso;
+    j2_hardening(j, ep0 + dgamma, &sy, &h_iso);
+    const double g = q_tr - 3.0 * j->mu * dgamma - j->h_kin * dgamma - sy;
+    const double dg = -(3.0 * j->mu + j->h_kin + h_iso);
+    const double step = -g / dg;
+    dgamma += step;
+    if (dgamma < 0.0) dgamma = 0.0;
+    if (fabs(step) <= 1e-14 * (1.0 + fabs(dgamma))) break;
+  }
+  double n[6];
+  for (int i = 0; i < 6; ++i) n[i] = xi[i] / xi_norm;
+  const double dev_scale = 2.0 * j->mu * dgamma * kSqrt3_2;
+  const double alpha_scale = (2.0 / 3.0) * j->h_kin * dgamma * kSqrt3_2;
+  const double mean = (sig_tr[0] + sig_tr[1] + sig_tr[2]) / 3.0;
+  for (int i = 0; i < 6; ++i) {
+    const double dev = s_tr[i] - dev_scale * n[i];
+    stress[i] = dev + (i < 3 ? mean : 0.0);
+  }
+  const double dep_scale = dgamma * kSqrt3_2;
+  for (int i = 0; i < 6; ++i) {
+    const double dep_i = dep_scale * n[i] * (i < 3 ? 1.0 : 2.0);
+    ts[i] = cs[i] + dep_i;
+    ts[7 + i] = cs[7 + i] + alpha_scale * n[i];
+  }
+  ts[6] = ep0 + dgamma;
+  double sy, h_iso;
+  j2_hardening(j, ep0 + dgamma, &sy, &h_iso);
+  const double theta = 1.0 - (2.0 * j->mu * dgamma * kSqrt3_2) / xi_norm;
+  const double denom = 1.0 + (h_iso + j->h_kin) / (3.0 * j->mu);
+  const double theta_bar = 1.0 / denom - (1.0 - theta);
+  double Idev[36];
+  memset(Idev, 0, sizeof Idev);
+  for (int i = 0; i < 3; ++i)
+    for (int k = 0; k < 3; ++k) Idev[6 * i + k] = 2.0 * j->mu * ((i == k ? 1.0 : 0.0) - 1.0 / 3.0);
+  for (int i = 3; i < 6; ++i) Idev[6 * i + i] = j->mu;
+  for (int i = 0; i < 6; ++i)
+    for (int k = 0; k < 6; ++k)
+      tangent[6 * i + k] = j->De[6 * i + k] - (1.0 - theta) * Idev[6 * i + k] -
+                           2.0 * j->mu * theta_bar * n[i] * n[k];
+}
+
+/* Linear elasticity (element.cpp:859-871) or J2 (plasticity.cpp:90). */
+int cxo_material_evaluate(const cxo_material* m, const double* strain, const double* cs,
+                          double* ts, double* stress, double* tangent) {
+  if (m->n_plastic > 0) {
+    j2_t j;
+    if (j2_init(m, &j)) return -1;
+    j2_evaluate(&j, strain, cs, ts, stress, tangent);
+    return 0;
+  }
+  elastic_D(m->E, m->nu, tangent);
+  for (int i = 0; i < 6; ++i) {
+    double v = 0.0;
+    for (int k = 0; k < 6; ++k) v += tangent[6 * i + k] * strain[k];
+    stress[i] = v;
+  }
+  memcpy(ts, cs, 13 * sizeof(double));
+  return 0;
+}
+
+/* ---- element_tangent_force: element.cpp:708-743 --------------------------------- */
+static int tangent_force(int type, const double* x, const double* ue, const cxo_material* m,
+                         const j2_t* j, const double* sc, double* st, double* Ke, double* fe) {
+  const int n = cxo_nodes_per_element(type);
+  const int ndof = 3 * n;
+  double gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det, eps[6], sig[6], D[36];
+  memset(Ke, 0, (size_t)ndof * ndof * sizeof(double));
+  memset(fe, 0, (size_t)ndof * sizeof(double));
+  double De[36];
+  if (!j) elastic_D(m->E, m->nu, De);
+  const int ng = cxo_gauss_rule(type, gp);
+  double mu_hg = 0.0;
+  for (int q = 0; q < ng; ++q) {
+    cxo_shape(type, gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
+    if (gradients_from_shape(n, dN, x, g, &det)) return -1;
+    const double scale = det * gp[4 * q + 3];
+    strain_from_gradients(g, n, ue, eps);
+    if (j) {
+      j2_evaluate(j, eps, sc + 13 * q, st + 13 * q, sig, D);
+    } else {
+      memcpy(D, De, sizeof D);
+      for (int i = 0; i < 6; ++i) {
+        double v = 0.0;
+        for (int k = 0; k < 6; ++k) v += D[6 * i + k] * eps[k];
+        sig[i] = v;
+      }
+      memcpy(st + 13 * q, sc + 13 * q, 13 * sizeof(double));
+    }
+    accumulate_ktangent(g, ndof, D, scale, Ke);
+    accumulate_fint(g, ndof, sig, scale, fe);
+    mu_hg = D[21];
+  }
+  if (type == T_C3D8R) {
+    hourglass_t hg;
+    if (build_hourglass(x, mu_hg, &hg)) return -1;
+    accumulate_hourglass(&hg, Ke);
+    accumulate_hourglass_force(&hg, ue, fe);
+  }
+  mirror_upper(ndof, Ke);
+  return 0;
+}
+
+int cxo_element_tangent_force(int type, const double* x, const double* ue,
+                              const cxo_material* m, const double* sc, double* st,
+                              double* Ke, double* fe) {
+  if (cxo_nodes_per_element(type) == 0) return fail("unsupported element type");
+  j2_t j;
+  if (m->n_plastic > 0 && j2_init(m, &j)) return -1;
+  return tangent_force(type, x, ue, m, m->n_plastic > 0 ? &j : NULL, sc, st, Ke, fe);
+}
+
+/* ---- assembly: src/fem/assembly.cpp:19-257, 385-423 ----------------------------- */
+struct cxo_system {
+  int32_t n_free;
+  int64_t nnz;
+  int64_t* row_ptr;
+  int32_t* col_idx;
+  double* vals;
+  double* rhs;
+};
+
+/* constraint_transform.cpp:78-82 (SPC-only: free DOFs numbered in global order) */
+int32_t cxo_dof_map(int64_t n_nodes, int64_t n_spc, const int32_t* spc_node,
+                    const int32_t* spc_comp, const double* spc_val, int32_t* dof_eq,
+                    double* prescribed) {
+  const int64_t ndof = 3 * n_nodes;
+  for (int64_t g = 0; g < ndof; ++g) {
+    dof_eq[g] = 0;
+    prescribed[g] = 0.0;
+  }
+  for (int64_t i = 0; i < n_spc; ++i) {
+    const int64_t g = 3 * (int64_t)spc_node[i] + spc_comp[i];
+    dof_eq[g] = -1;
+    prescribed[g] = spc_val[i];
+  }
+  int32_t n_free = 0;
+  for (int64_t g = 0; g < ndof; ++g) dof_eq[g] = dof_eq[g] < 0 ? -1 : n_free++;
+  return n_free;
+}
+
+typedef struct {
+  int64_t* key;
+  double* val;
+  int64_t n, cap;
+} triplets_t;
+
+static int trip_push(triplets_t* t, int64_t key, double v) {
+  if (t->n == t->cap) {
+    const int64_t nc = t->cap ? 2 * t->cap : 1 << 16;
+    int64_t* k = realloc(t->key, (size_t)nc * sizeof(int64_t));
+    if (!k) return fail("out of memory");
+    t->key = k;
+    double* vv = realloc(t->val, (size_t)nc * sizeof(double));
+    if (!vv) return fail("out of memory");
+    t->val = vv;
+    t->cap = nc;
+  }
+  t->key[t->n] = key;
+  t->val[t->n] = v;
+  ++t->n;
+  return 0;
+}
+
+/* Stable LSD radix sort of (key, val) by key; keys are non-negative. */
+static int radix_sort(triplets_t* t) {
+  const int64_t n = t->n;
+  int64_t maxk = 0;
+  for (int64_t i = 0; i < n; ++i)
+    if (t->key[i] > maxk) maxk = t->key[i];
+  int64_t* k2 = malloc((size_t)(n ? n : 1) * sizeof(int64_t));
+  double* v2 = malloc((size_t)(n ? n : 1) * sizeof(double));
+  if (!k2 || !v2) {
+    free(k2);
+    free(v2);
+    return fail("out of memory");
+  }
+  for (int shift = 0; shift < 64 && (maxk >> shift) != 0; shift += 11) {
+    int64_t cnt[2049];
+    memset(cnt, 0, sizeof cnt);
+    for (int64_t i = 0; i < n; ++i) ++cnt[((t->key[i] >> shift) & 2047) + 1];
+    for (int b = 0; b < 2048; ++b) cnt[b + 1] += cnt[b];
+    for (int64_t i = 0; i < n; ++i) {
+      const int64_t p = cnt[(t->key[i] >> shift) & 2047]++;
+      k2[p] = t->key[i];
+      v2[p] = t->val[i];
+    }
+    int64_t* tk = t->key;
+    t->key = k2;
+    k2 = tk;
+    double* tv = t->val;
+    t->val = v2;
+    v2 = tv;
+  }
+  free(k2);
+  free(v2);
+  return 0;
+}
+
+/* scatter_block for an SPC-only transform (assembly.cpp:76-100): free rows receive
+ * kab at (eqA, eqB) for free columns and -kab*u_c into rhs for prescribed columns;
+ * exact zeros are skipped. */
+static int scatter(const double* Ke, int ndof, const int64_t* gd, const int32_t* dof_eq,
+                   const double* prescribed, int32_t n_free, triplets_t* t, double* rhs) {
+  for (int a = 0; a < ndof; ++a) {
+    const int32_t ea = dof_eq[gd[a]];
+    const double ca = ea < 0 ? prescribed[gd[a]] : 0.0;
+    if (ea < 0 && ca == 0.0) continue;
+    for (int b = 0; b < ndof; ++b) {
+      const double kab = Ke[a * ndof + b];
+      if (kab == 0.0) continue;
+      if (ea < 0) continue; /* prescribed row: no free terms */
+      const int32_t eb = dof_eq[gd[b]];
+      if (eb >= 0) {
+        if (trip_push(t, (int64_t)ea * n_free + eb, 1.0 * kab * 1.0)) return -1;
+      } else {
+        const double cb = prescribed[gd[b]];
+        if (cb != 0.0) rhs[ea] -= 1.0 * kab * cb;
+      }
+    }
+  }
+  return 0;
+}
+
+static cxo_system* finish(triplets_t* t, int32_t n_free, double* rhs) {
+  cxo_system* s = calloc(1, sizeof *s);
+  if (!s || radix_sort(t)) {
+    free(s);
+    return NULL;
+  }
+  int64_t nnz = 0;
+  for (int64_t i = 0; i < t->n; ++i)
+    if (i == 0 || t->key[i] != t->key[i - 1]) ++nnz;
+  s->n_free = n_free;
+  s->nnz = nnz;
+  s->row_ptr = calloc((size_t)n_free + 1, sizeof(int64_t));
+  s->col_idx = malloc((size_t)(nnz ? nnz : 1) * sizeof(int32_t));
+  s->vals = malloc((size_t)(nnz ? nnz : 1) * sizeof(double));
+  s->rhs = rhs;
+  int64_t p = -1;
+  for (int64_t i = 0; i < t->n; ++i) {
+    if (i == 0 || t->key[i] != t->key[i - 1]) {
+      ++p;
+      const int32_t r = (int32_t)(t->key[i] / n_free);
+      s->col_idx[p] = (int32_t)(t->key[i] % n_free);
+      s->vals[p] = 0.0;
+      ++s->row_ptr[r + 1];
+    }
+    s->vals[p] += t->val[i];
+  }
+  for (int32_t r = 0; r < n_free; ++r) s->row_ptr[r + 1] += s->row_ptr[r];
+  free(t->key);
+  free(t->val);
+  return s;
+}
+
+/* add_external_load (assembly.cpp:200-208) */
+static void add_external(const double* f_ext, int64_t ndof, const int32_t* dof_eq,
+                         double* rhs) {
+  if (!f_ext) return;
+  for (int64_t g = 0; g < ndof; ++g) {
+    if (f_ext[g] == 0.0) continue;
+    if (dof_eq[g] >= 0) rhs[dof_eq[g]] += 1.0 * f_ext[g];
+  }
+}
+
+static cxo_system* assemble(int64_t n_nodes, const double* coords, int64_t n_elems,
+                            const int32_t* types, const int64_t* conn_ptr,
+                            const int32_t* conn, const int32_t* elem_mat,
+                            const cxo_material* mats, const int32_t* dof_eq,
+                            const double* prescribed, int32_t n_free, const double* f_ext,
+                            const double* u, const double* sc, double* st, double* f_int) {
+  triplets_t t = {0};
+  double* rhs = calloc((size_t)n_free + 1, sizeof(double));
+  double x[3 * MAXN], ue[3 * MAXN], Ke[60 * 60], fe[60];
+  int64_t gd[60];
+  int64_t gp_off = 0;
+  if (f_int) memset(f_int, 0, (size_t)(3 * n_nodes) * sizeof(double));
+  for (int64_t e = 0; e < n_elems; ++e) {
+    const int type = types[e];
+    const int n = cxo_nodes_per_element(type);
+    if (n == 0 || conn_ptr[e + 1] - conn_ptr[e] != n) {
+      fail("unsupported element type or bad connectivity length");
+      goto error;
+    }
+    const int32_t* c = conn + conn_ptr[e];
+    for (int k = 0; k < n; ++k) {
+      if (c[k] < 0 || c[k] >= n_nodes) {
+        fail("element references unknown node");
+        goto error;
+      }
+      for (int d = 0; d < 3; ++d) {
+        x[3 * k + d] = coords[3 * (int64_t)c[k] + d];
+        gd[3 * k + d] = 3 * (int64_t)c[k] + d;
+        if (u) ue[3 * k + d] = u[3 * (int64_t)c[k] + d];
+      }
+    }
+    const cxo_material* m = &mats[elem_mat[e]];
+    double gpb[4 * 27];
+    const int ng = cxo_gauss_rule(type, gpb);
+    if (u) {
+      if (cxo_element_tangent_force(type, x, ue, m, sc + 13 * gp_off, st + 13 * gp_off, Ke, fe))
+        goto error;
+    } else {
+      if (cxo_element_stiffness(type, x, m->E, m->nu, Ke)) goto error;
+    }
+    gp_off += ng;
+    if (scatter(Ke, 3 * n, gd, dof_eq, prescribed, n_free, &t, rhs)) goto error;
+    if (f_int)
+      for (int a = 0; a < 3 * n; ++a) f_int[gd[a]] += fe[a];
+  }
+  add_external(f_ext, 3 * n_nodes, dof_eq, rhs);
+  {
+    cxo_system* s = finish(&t, n_free, rhs);
+    if (!s) goto error;
+    return s;
+  }
+error:
+  free(t.key);
+  free(t.val);
+  free(rhs);
+  return NULL;
+}
+
+cxo_system* cxo_assemble_linear(int64_t n_nodes, const double* coords, int64_t n_elems,
+                                const int32_t* types, const int64_t* conn_ptr,
+                                const int32_t* conn, const int32_t* elem_mat,
+                                const cxo_material* mats, const int32_t* dof_eq,
+                                const double* prescribed, int32_t n_free,
+                                const double* f_ext) {
+  return assemble(n_nodes, coords, n_elems, types, conn_ptr, conn, elem_mat, mats, dof_eq,
+                  prescribed, n_free, f_ext, NULL, NULL, NULL, NULL);
+}
+
+cxo_system* cxo_assemble_tangent(int64_t n_nodes, const double* coords, int64_t n_elems,
+                                 const int32_t* types, const int64_t* conn_ptr,
+                                 const int32_t* conn, const int32_t* elem_mat,
+                                 const cxo_material* mats, const int32_t* dof_eq,
+                                 const double* prescribed, int32_t n_free,
+                                 const double* f_ext, const double* u, const double* sc,
+                                 double* st, double* f_int) {
+  if (!u || !sc || !st || !f_int) {
+    fail("tangent assembly needs u, committed state, trial state and f_int");
+    return NULL;
+  }
+  return assemble(n_nodes, coords, n_elems, types, conn_ptr, conn, elem_mat, mats, dof_eq,
+                  prescribed, n_free, f_ext, u, sc, st, f_int);
+}
+
+int cxo_system_info(const cxo_system* s, int32_t* n_free, int64_t* nnz) {
+  *n_free = s->n_free;
+  *nnz = s->nnz;
+  return 0;
+}
+
+int cxo_system_copy(const cxo_system* s, int64_t* row_ptr, int32_t* col_idx, double* vals,
+                    double* rhs) {
+  memcpy(row_ptr, s->row_ptr, ((size_t)s->n_free + 1) * sizeof(int64_t));
+  memcpy(col_idx, s->col_idx, (size_t)s->nnz * sizeof(int32_t));
+  memcpy(vals, s->vals, (size_t)s->nnz * sizeof(double));
+  memcpy(rhs, s->rhs, (size_t)s->n_free * sizeof(double));
+  return 0;
+}
+
+void cxo_system_free(cxo_system* s) {
+  if (!s) return;
+  free(s->row_ptr);
+  free(s->col_idx);
+  free(s->vals);
+  free(s->rhs);
+  free(s);
+}
+
+/* ---- per-element compliance derivative by central differences ------------------- */
+int cxo_element_compliance_grad_fd(int type, const double* coords, const double* ue,
+                                   double E, double nu, double h, double* dcdX) {
+  const int n = cxo_nodes_per_element(type);
+  if (n == 0) return fail("unsupported element type");
+  const int ndof = 3 * n;
+  double xp[3 * MAXN], Kp[60 * 60], Km[60 * 60];
+  for (int v = 0; v < ndof; ++v) {
+    memcpy(xp, coords, (size_t)ndof * sizeof(double));
+    xp[v] = coords[v] + h;
+    if (cxo_element_stiffness(type, xp, E, nu, Kp)) return -1;
+    xp[v] = coords[v] - h;
+    if (cxo_element_stiffness(type, xp, E, nu, Km)) return -1;
+    double s = 0.0;
+    for (int a = 0; a < ndof; ++a) {
+      double r = 0.0;
+      for (int b = 0; b < ndof; ++b) r += (Kp[a * ndof + b] - Km[a * ndof + b]) * ue[b];
+      s += ue[a] * r;
+    }
+    dcdX[v] = -s / (2.0 * h);
+  }
+  return 0;
+}

@@ -1,0 +1,362 @@
+"""ctypes front end of the two CPU oracles. TEST INFRASTRUCTURE ONLY.
+
+`Port`  wraps oracle/_lib/libcxo.so, the C restatement of the reference path (cxo.c).
+`Ref`   wraps oracle/_ref/libcxpp_ref.so, the reference's own C++ sources compiled by
+        oracle/Makefile with the shim in ref_shim.cpp (only present where the
+        reference tree was available at build time).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module;
+the product package never imports it. Both classes expose the same element-level
+methods so a test can run one against the other.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "_lib", "libcxo.so")
+REF_SO = os.path.join(HERE, "_ref", "libcxpp_ref.so")
+
+NODES = {2: 8, 3: 8, 4: 20, 5: 20, 6: 6, 7: 15}
+NGP = {2: 8, 3: 1, 4: 27, 5: 8, 6: 2, 7: 6}
+
+_vp = C.c_void_p
+
+
+class Material(C.Structure):
+    """Layout shared by cxo_material, ref_material and cxg_material."""
+
+    _fields_ = [("E", C.c_double), ("nu", C.c_double), ("n_plastic", C.c_int32),
+                ("eqplastic", _vp), ("yield_", _vp), ("hardening", C.c_int32),
+                ("h_kin", C.c_double)]
+
+
+def make_material(E, nu, plastic=None, hardening=0, h_kin=0.0):
+    """plastic: None (elastic) or (eqplastic[], yield[]). The returned object keeps its
+    table arrays alive."""
+    m = Material()
+    m.E, m.nu, m.hardening, m.h_kin = float(E), float(nu), int(hardening), float(h_kin)
+    if plastic is None:
+        m.n_plastic, m.eqplastic, m.yield_ = 0, None, None
+        m._keep = ()
+    else:
+        ep = np.ascontiguousarray(plastic[0], dtype=np.float64)
+        sy = np.ascontiguousarray(plastic[1], dtype=np.float64)
+        m.n_plastic = int(ep.size)
+        m.eqplastic, m.yield_ = ep.ctypes.data, sy.ctypes.data
+        m._keep = (ep, sy)
+    return m
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _i64(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+class _Base:
+    prefix = ""
+
+    def __init__(self, path):
+        if not os.path.exists(path):
+            raise OracleError(f"oracle library missing: {path} (run make -C oracle)")
+        self.lib = C.CDLL(path)
+        self.lib[f"{self.prefix}_last_error"].restype = C.c_char_p
+
+    def _fn(self, name):
+        return self.lib[f"{self.prefix}_{name}"]
+
+    def _check(self, rc):
+        if rc != 0:
+            raise OracleError(self._fn("last_error")().decode())
+
+    # ---- element level (same signatures in both libraries) -----------------------
+    def gauss_rule(self, etype):
+        out = np.zeros(4 * 27)
+        n = self._fn("gauss_rule")(int(etype), _p(out))
+        return out[: 4 * n].reshape(n, 4)
+
+    def shape(self, etype, xi, et, ze):
+        N = np.zeros(20)
+        dN = np.zeros(60)
+        f = self._fn("shape")
+        f.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _vp, _vp]
+        n = f(int(etype), xi, et, ze, _p(N), _p(dN))
+        return N[:n].copy(), dN[: 3 * n].reshape(n, 3).copy()
+
+    def physical_gradients(self, etype, xi, et, ze, coords):
+        n = NODES[etype]
+        g = np.zeros(3 * n)
+        det = C.c_double()
+        f = self._fn("physical_gradients")
+        f.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]
+        self._check(f(int(etype), xi, et, ze, _p(_f64(coords)), _p(g), C.byref(det)))
+        return g.reshape(n, 3), det.value
+
+    def element_volume(self, etype, coords):
+        v = C.c_double()
+        self._check(self._fn("element_volume")(int(etype), _p(_f64(coords)), C.byref(v)))
+        return v.value
+
+    def element_stiffness(self, etype, coords, E, nu):
+        n = NODES[etype]
+        Ke = np.zeros((3 * n) * (3 * n))
+        f = self._fn("element_stiffness")
+        f.argtypes = [C.c_int, _vp, C.c_double, C.c_double, _vp]
+        self._check(f(int(etype), _p(_f64(coords)), float(E), float(nu), _p(Ke)))
+        return Ke.reshape(3 * n, 3 * n)
+
+    def material_evaluate(self, mat, strain, committed=None):
+        committed = np.zeros(13) if committed is None else _f64(committed)
+        trial = np.zeros(13)
+        s = np.zeros(6)
+        D = np.zeros(36)
+        self._check(self._fn("material_evaluate")(C.byref(mat), _p(_f64(strain)),
+                                                  _p(committed), _p(trial), _p(s), _p(D)))
+        return s, D.reshape(6, 6), trial
+
+    def element_tangent_force(self, etype, coords, ue, mat, committed=None):
+        n = NODES[etype]
+        ng = NGP[etype]
+        committed = np.zeros(13 * ng) if committed is None else _f64(committed)
+        trial = np.zeros(13 * ng)
+        Ke = np.zeros((3 * n) ** 2)
+        fe = np.zeros(3 * n)
+        self._check(self._fn("element_tangent_force")(
+            int(etype), _p(_f64(coords)), _p(_f64(ue)), C.byref(mat), _p(committed),
+            _p(trial), _p(Ke), _p(fe)))
+        return Ke.reshape(3 * n, 3 * n), fe, trial.reshape(ng, 13)
+
+
+class Port(_Base):
+    """The C restatement (oracle/cxo.c)."""
+
+    prefix = "cxo"
+
+    def __init__(self, path=PORT_SO):
+        super().__init__(path)
+        for name in ("assemble_linear", "assemble_tangent"):
+            self._fn(name).restype = _vp
+        self.lib.cxo_dof_map.restype = C.c_int32
+
+    def _system(self, s):
+        if not s:
+            raise OracleError(self._fn("last_error")().decode())
+        n_free = C.c_int32()
+        nnz = C.c_int64()
+        self.lib.cxo_system_info(_vp(s), C.byref(n_free), C.byref(nnz))
+        rp = np.zeros(n_free.value + 1, dtype=np.int64)
+        ci = np.zeros(nnz.value, dtype=np.int32)
+        v = np.zeros(nnz.value)
+        rhs = np.zeros(n_free.value)
+        self.lib.cxo_system_copy(_vp(s), _p(rp), _p(ci), _p(v), _p(rhs))
+        self.lib.cxo_system_free(_vp(s))
+        return rp, ci, v, rhs
+
+    @staticmethod
+    def _mesh_arrays(mesh, mats, elem_mat):
+        E = mesh.n_elems
+        n = mesh.conn.shape[1]
+        types = np.full(E, mesh.etype, dtype=np.int32)
+        conn_ptr = np.arange(E + 1, dtype=np.int64) * n
+        conn = _i32(mesh.conn.ravel())
+        arr = (Material * len(mats))(*mats)
+        em = _i32(elem_mat if elem_mat is not None else np.zeros(E, dtype=np.int32))
+        return types, conn_ptr, conn, arr, em
+
+    def assemble_linear(self, mesh, mats, elem_mat, dof_eq, prescribed, n_free, f_ext=None):
+        """Reduced K_ff (canonical CSR) and rhs = T^T f_ext - K_fc u_c."""
+        types, conn_ptr, conn, arr, em = self._mesh_arrays(mesh, mats, elem_mat)
+        f = self._fn("assemble_linear")
+        s = f(C.c_int64(mesh.n_nodes), _p(_f64(mesh.coords)), C.c_int64(mesh.n_elems),
+              _p(types), _p(conn_ptr), _p(conn), _p(em), arr, _p(_i32(dof_eq)),
+              _p(_f64(prescribed)), C.c_int32(n_free),
+              _p(None if f_ext is None else _f64(f_ext)))
+        return self._system(s)
+
+    def assemble_tangent(self, mesh, mats, elem_mat, dof_eq, prescribed, n_free, u,
+                         committed, f_ext=None):
+        types, conn_ptr, conn, arr, em = self._mesh_arrays(mesh, mats, elem_mat)
+        committed = _f64(committed)
+        trial = np.zeros_like(committed)
+        f_int = np.zeros(3 * mesh.n_nodes)
+        f = self._fn("assemble_tangent")
+        s = f(C.c_int64(mesh.n_nodes), _p(_f64(mesh.coords)), C.c_int64(mesh.n_elems),
+              _p(types), _p(conn_ptr), _p(conn), _p(em), arr, _p(_i32(dof_eq)),
+              _p(_f64(prescribed)), C.c_int32(n_free),
+              _p(None if f_ext is None else _f64(f_ext)), _p(_f64(u)), _p(committed),
+              _p(trial), _p(f_int))
+        rp, ci, v, rhs = self._system(s)
+        return rp, ci, v, rhs, f_int, trial
+
+    def element_compliance_grad_fd(self, etype, coords, ue, E, nu, h):
+        n = NODES[etype]
+        out = np.zeros(3 * n)
+        f = self._fn("element_compliance_grad_fd")
+        f.argtypes = [C.c_int, _vp, _vp, C.c_double, C.c_double, C.c_double, _vp]
+        self._check(f(int(etype), _p(_f64(coords)), _p(_f64(ue)), E, nu, h, _p(out)))
+        return out.reshape(n, 3)
+
+
+def coo_to_csr(n, rows, cols, vals):
+    """Canonical CSR (rows asc, cols asc, duplicates summed in input order)."""
+    rows = np.asarray(rows, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    key = rows * n + cols
+    order = np.argsort(key, kind="stable")
+    key = key[order]
+    v = np.asarray(vals)[order]
+    uniq, start = np.unique(key, return_index=True)
+    sums = np.add.reduceat(v, start) if v.size else v
+    r = (uniq // n).astype(np.int64)
+    c = (uniq % n).astype(np.int32)
+    rp = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(rp, r + 1, 1)
+    return np.cumsum(rp), c, sums
+
+
+class Ref(_Base):
+    """The reference itself (oracle/_ref/libcxpp_ref.so)."""
+
+    prefix = "ref"
+
+    def __init__(self, path=REF_SO):
+        super().__init__(path)
+        for name in ("model_create", "assemble_linear_static", "mp_create",
+                     "assemble_material_tangent"):
+            self._fn(name).restype = _vp
+        self.lib.ref_mp_num_points.restype = C.c_int64
+
+    @staticmethod
+    def available(path=REF_SO):
+        return os.path.exists(path)
+
+    def model(self, mesh, mats, elem_mat=None, spc=None, cloads=None):
+        """Build a reference Model. spc=(node, comp, value) arrays, cloads likewise."""
+        E = mesh.n_elems
+        n = mesh.conn.shape[1]
+        types = np.full(E, mesh.etype, dtype=np.int32)
+        conn_ptr = np.arange(E + 1, dtype=np.int64) * n
+        em = _i32(elem_mat if elem_mat is not None else np.zeros(E, dtype=np.int32))
+        arr = (Material * len(mats))(*mats)
+        sn, sc, sv = spc if spc is not None else (np.zeros(0), np.zeros(0), np.zeros(0))
+        cn, cc, cv = cloads if cloads is not None else (np.zeros(0), np.zeros(0), np.zeros(0))
+        sn, sc, sv, cn, cc, cv = _i32(sn), _i32(sc), _f64(sv), _i32(cn), _i32(cc), _f64(cv)
+        h = self._fn("model_create")(
+            C.c_int64(mesh.n_nodes), _p(_f64(mesh.coords)), C.c_int64(E), _p(types),
+            _p(conn_ptr), _p(_i32(mesh.conn.ravel())), _p(em), C.c_int32(len(mats)), arr,
+            C.c_int64(sn.size), _p(sn), _p(sc), _p(sv), C.c_int64(cn.size), _p(cn),
+            _p(cc), _p(cv))
+        if not h:
+            raise OracleError(self._fn("last_error")().decode())
+        return RefModel(self, h, mesh)
+
+    def _sys(self, s):
+        if not s:
+            raise OracleError(self._fn("last_error")().decode())
+        n_free = C.c_int64()
+        nnz = C.c_int64()
+        self.lib.ref_sys_info(_vp(s), C.byref(n_free), C.byref(nnz))
+        rows = np.zeros(nnz.value, dtype=np.int32)
+        cols = np.zeros(nnz.value, dtype=np.int32)
+        vals = np.zeros(nnz.value)
+        rhs = np.zeros(n_free.value)
+        return n_free.value, rows, cols, vals, rhs, s
+
+    def assemble_csr_threads(self, mesh, dof_eq, prescribed, row_ptr, col_idx, nthreads):
+        vals = np.zeros(col_idx.size)
+        rhs = np.zeros(row_ptr.size - 1)
+        f = self._fn("assemble_csr_threads")
+        f.argtypes = [C.c_int, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                      _vp, C.c_int]
+        self._check(f(int(mesh.etype), _p(_f64(mesh.coords)), mesh.n_elems,
+                      _p(_i32(mesh.conn.ravel())), _p(_f64(mesh.young)),
+                      _p(_f64(mesh.poisson)), _p(_i32(dof_eq)), _p(_f64(prescribed)),
+                      _p(_i64(row_ptr)), _p(_i32(col_idx)), _p(vals), _p(rhs),
+                      int(nthreads)))
+        return vals, rhs
+
+
+class RefModel:
+    def __init__(self, ref, handle, mesh):
+        self.ref, self.h, self.mesh = ref, handle, mesh
+        self.mp = None
+
+    def __del__(self):
+        try:
+            if self.mp:
+                self.ref.lib.ref_mp_free(_vp(self.mp))
+            self.ref.lib.ref_model_free(_vp(self.h))
+        except Exception:
+            pass
+
+    def _take(self, s):
+        lib = self.ref.lib
+        n_free, rows, cols, vals, rhs, s = self.ref._sys(s)
+        dof_eq = np.zeros(3 * self.mesh.n_nodes, dtype=np.int32)
+        lib.ref_sys_copy(_vp(s), _p(rows), _p(cols), _p(vals), _p(rhs), _p(dof_eq))
+        lib.ref_sys_free(_vp(s))
+        return {"n_free": n_free, "rows": rows, "cols": cols, "vals": vals, "rhs": rhs,
+                "dof_eq": dof_eq}
+
+    def assemble_linear_static(self):
+        """Returns the reference LinearSystem (COO in hash-map order) as a dict."""
+        return self._take(self.ref._fn("assemble_linear_static")(_vp(self.h)))
+
+    def material_points(self):
+        lib = self.ref.lib
+        if self.mp is None:
+            self.mp = lib.ref_mp_create(_vp(self.h))
+            if not self.mp:
+                raise OracleError(lib.ref_last_error().decode())
+        return self.mp
+
+    def state(self, committed=True):
+        mp = self.material_points()
+        g = self.ref.lib.ref_mp_num_points(_vp(mp))
+        out = np.zeros(13 * g)
+        self.ref.lib.ref_mp_get_state(_vp(mp), int(committed), _p(out))
+        return out
+
+    def set_state(self, state, committed=True):
+        mp = self.material_points()
+        self.ref.lib.ref_mp_set_state(_vp(mp), int(committed), _p(_f64(state)))
+
+    def commit(self):
+        self.ref.lib.ref_mp_commit(_vp(self.material_points()))
+
+    def assemble_material_tangent(self, u):
+        mp = self.material_points()
+        f_int = np.zeros(3 * self.mesh.n_nodes)
+        s = self.ref._fn("assemble_material_tangent")(_vp(self.h), _vp(mp),
+                                                      _p(_f64(u)), _p(f_int))
+        out = self._take(s)
+        out["f_int"] = f_int
+        return out
+
+    def sensitivity_compliance(self, var_node, var_comp, h=1e-4):
+        var_node, var_comp = _i32(var_node), _i32(var_comp)
+        dg = np.zeros(var_node.size)
+        obj = C.c_double()
+        f = self.ref._fn("sensitivity_compliance")
+        f.argtypes = [_vp, C.c_int64, _vp, _vp, C.c_double, _vp, _vp]
+        self.ref._check(f(_vp(self.h), var_node.size, _p(var_node), _p(var_comp), h,
+                          _p(dg), C.byref(obj)))
+        return dg, obj.value
