@@ -1,0 +1,315 @@
+"""Python mirror of the reference's assembly interface, running on the B200 kernels.
+
+Reference interface (include/calculixpp/fem/assembly.hpp, element.hpp):
+    LinearSystem assemble_linear_static(const Model&)                    assembly.hpp:42
+    MaterialPoints make_material_points(const Model&)                   assembly.hpp:93
+    LinearSystem assemble_material_tangent(const Model&, u, mp, f_int)  assembly.hpp:105-108
+    std::vector<Real> element_stiffness(type, coords, ElasticIso)       element.hpp:64-65
+    ElementResponse element_tangent_force(type, coords, ue, material, state)
+                                                                        element.hpp:160-164
+Same names, same argument meaning, errors raised as exceptions carrying the reference's
+messages. Differences: the stiffness comes back in canonical CSR (the reference's COO
+triplets sorted by row then column), and arrays are torch tensors on the GPU. Every
+call goes through the C ABI of libcxg.so (include/cxg.h); nothing here computes on the
+CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from .meshgen import Mesh, NODES, NGP, dof_map
+
+_vp = C.c_void_p
+
+
+@dataclass
+class Material:
+    """ElasticIso + optional *PLASTIC table (core/material.hpp:81-115)."""
+
+    E: float
+    nu: float
+    plastic: tuple | None = None  # (eqplastic[], yield[])
+    hardening: int = 0            # 0 isotropic, 1 kinematic, 2 combined
+    h_kin: float = 0.0
+
+
+@dataclass
+class Model:
+    """The subset of cxpp::Model the assembly reads: mesh, per-element materials,
+    single-point constraints (node, comp 0..2, value) and concentrated loads."""
+
+    mesh: Mesh
+    materials: list
+    elem_mat: np.ndarray | None = None
+    spc: tuple | None = None
+    cloads: tuple | None = None
+
+    def dof_map(self):
+        sn, sc, sv = self.spc if self.spc is not None else (np.zeros(0, int), np.zeros(0, int), np.zeros(0))
+        return dof_map(self.mesh.n_nodes, sn, sc, sv)
+
+    def external_load_vector(self):
+        """Full-magnitude CLOAD vector (src/fem/loads.cpp:575-585)."""
+        f = np.zeros(3 * self.mesh.n_nodes)
+        if self.cloads is not None:
+            n, c, v = self.cloads
+            np.add.at(f, 3 * np.asarray(n, dtype=np.int64) + np.asarray(c, dtype=np.int64), v)
+        return f
+
+
+@dataclass
+class LinearSystem:
+    """Reduced free/free system (assembly.hpp:18-38) with K_ff in CSR."""
+
+    n_free: int
+    row_ptr: torch.Tensor
+    col_idx: torch.Tensor
+    vals: torch.Tensor
+    rhs: torch.Tensor
+    dof_eq: np.ndarray
+    prescribed: np.ndarray
+    extra: dict = field(default_factory=dict)
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.vals.cpu().numpy(), self.col_idx.cpu().numpy(),
+                              self.row_ptr.cpu().numpy()), shape=(self.n_free, self.n_free))
+
+
+def _ptr(t):
+    return None if t is None else _vp(t.data_ptr())
+
+
+def _dev(a, dtype, device):
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=device)
+
+
+def _stream():
+    return _vp(torch.cuda.current_stream().cuda_stream)
+
+
+def _c_material(m: Material, keep: list):
+    cm = _lib.CxgMaterial()
+    cm.E, cm.nu, cm.hardening, cm.h_kin = float(m.E), float(m.nu), int(m.hardening), float(m.h_kin)
+    if m.plastic is None:
+        cm.n_plastic, cm.eqplastic, cm.yield_ = 0, None, None
+    else:
+        ep = np.ascontiguousarray(m.plastic[0], dtype=np.float64)
+        sy = np.ascontiguousarray(m.plastic[1], dtype=np.float64)
+        keep += [ep, sy]
+        cm.n_plastic = int(ep.size)
+        cm.eqplastic, cm.yield_ = ep.ctypes.data, sy.ctypes.data
+    return cm
+
+
+class Plan:
+    """A cxg_plan: mesh, DOF map and CSR pattern resident on one GPU."""
+
+    def __init__(self, model: Model, precision: str = "fp64", device=None):
+        self.lib = _lib.load()
+        if not torch.cuda.is_available():
+            raise _lib.CxgError(_lib.CXG_ERR_NO_GPU, "no CUDA device")
+        self.device = torch.device(device or f"cuda:{torch.cuda.current_device()}")
+        self.model = model
+        m = model.mesh
+        dev = self.device
+        dof_eq, prescribed, n_free = model.dof_map()
+        self.dof_eq, self.prescribed, self.n_free = dof_eq, prescribed, n_free
+        keep = []
+        mats = (_lib.CxgMaterial * len(model.materials))(*[_c_material(x, keep) for x in model.materials])
+        coords = _dev(m.coords, torch.float64, dev)
+        conn = _dev(m.conn.reshape(-1), torch.int32, dev)
+        young = _dev(m.young, torch.float64, dev) if m.young is not None else None
+        poisson = _dev(m.poisson, torch.float64, dev) if m.poisson is not None else None
+        elem_mat = _dev(model.elem_mat, torch.int32, dev) if model.elem_mat is not None else None
+        d_dof = _dev(dof_eq, torch.int32, dev)
+        d_pre = _dev(prescribed, torch.float64, dev)
+        desc = _lib.CxgMeshDesc(m.n_nodes, m.n_elems, m.etype, _ptr(coords), _ptr(conn), _ptr(young),
+                                _ptr(poisson), _ptr(elem_mat), len(model.materials),
+                                C.cast(mats, _vp))
+        dmap = _lib.CxgDofmapDesc(_ptr(d_dof), _ptr(d_pre), n_free)
+        handle = _vp()
+        with torch.cuda.device(dev):
+            torch.cuda.synchronize()
+            _lib.check(self.lib.cxg_plan_create(C.byref(desc), C.byref(dmap),
+                                                _lib.MIXED if precision == "mixed" else _lib.FP64,
+                                                C.byref(handle)))
+        self.h = handle
+        info = _lib.CxgPlanInfo()
+        _lib.check(self.lib.cxg_plan_get_info(self.h, C.byref(info)))
+        self.info = info
+        self.nnz = int(info.nnz)
+        self.n_gauss = int(info.n_gauss_points)
+        rp, ci = _vp(), _vp()
+        _lib.check(self.lib.cxg_plan_pattern_device(self.h, C.byref(rp), C.byref(ci)))
+        self._pattern = None
+
+    # -- lifetime ------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cxg_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- pattern / precision -------------------------------------------------------
+    def pattern(self):
+        if self._pattern is None:
+            rp = torch.empty(self.n_free + 1, dtype=torch.int64, device=self.device)
+            ci = torch.empty(self.nnz, dtype=torch.int32, device=self.device)
+            _lib.check(self.lib.cxg_plan_get_pattern(self.h, _ptr(rp), _ptr(ci)))
+            self._pattern = (rp, ci)
+        return self._pattern
+
+    def set_precision(self, precision: str):
+        _lib.check(self.lib.cxg_plan_set_precision(self.h, _lib.MIXED if precision == "mixed" else _lib.FP64))
+
+    def check(self):
+        bad = C.c_int64()
+        _lib.check(self.lib.cxg_plan_check(self.h, C.byref(bad)))
+
+    # -- assembly --------------------------------------------------------------------
+    def assemble_linear(self, f_ext=None, vals=None, rhs=None, check=True):
+        dev = self.device
+        vals = torch.empty(self.nnz, dtype=torch.float64, device=dev) if vals is None else vals
+        rhs = torch.empty(self.n_free, dtype=torch.float64, device=dev) if rhs is None else rhs
+        fe = None if f_ext is None else _dev(f_ext, torch.float64, dev)
+        with torch.cuda.device(dev):
+            _lib.check(self.lib.cxg_assemble_linear(self.h, _ptr(vals), _ptr(rhs), _ptr(fe), _stream()))
+            if check:
+                self.check()
+        return vals, rhs
+
+    def assemble_tangent(self, u, f_ext=None, vals=None, f_int=None, rhs=None, check=True):
+        dev = self.device
+        vals = torch.empty(self.nnz, dtype=torch.float64, device=dev) if vals is None else vals
+        f_int = torch.empty(3 * self.model.mesh.n_nodes, dtype=torch.float64, device=dev) if f_int is None else f_int
+        rhs = torch.empty(self.n_free, dtype=torch.float64, device=dev) if rhs is None else rhs
+        du = _dev(u, torch.float64, dev)
+        fe = None if f_ext is None else _dev(f_ext, torch.float64, dev)
+        with torch.cuda.device(dev):
+            _lib.check(self.lib.cxg_assemble_tangent(self.h, _ptr(du), _ptr(vals), _ptr(f_int), _ptr(rhs),
+                                                     _ptr(fe), _stream()))
+            if check:
+                self.check()
+        return vals, f_int, rhs
+
+    # -- material state -------------------------------------------------------------
+    def state(self, committed=True):
+        out = torch.empty(self.n_gauss * 13, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_state_get(self.h, _lib.COMMITTED if committed else _lib.TRIAL, _ptr(out)))
+        return out.view(self.n_gauss, 13)
+
+    def set_state(self, state, committed=True):
+        s = _dev(state, torch.float64, self.device).reshape(-1)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_state_set(self.h, _lib.COMMITTED if committed else _lib.TRIAL, _ptr(s)))
+
+    def commit(self):
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_state_commit(self.h, _stream()))
+
+    def update_coords(self, coords):
+        c = _dev(coords, torch.float64, self.device)
+        _lib.check(self.lib.cxg_plan_update_coords(self.h, _ptr(c)))
+
+    def update_young(self, young):
+        y = _dev(young, torch.float64, self.device)
+        _lib.check(self.lib.cxg_plan_update_young(self.h, _ptr(y)))
+
+
+# ---- the reference's function names ---------------------------------------------------
+
+def assemble_linear_static(model: Model, precision: str = "fp64", plan: Plan | None = None) -> LinearSystem:
+    """K_ff u_f = T^T f_ext - K_fc u_c (assembly.hpp:40-42)."""
+    plan = plan or Plan(model, precision)
+    vals, rhs = plan.assemble_linear(model.external_load_vector())
+    rp, ci = plan.pattern()
+    return LinearSystem(plan.n_free, rp, ci, vals, rhs, plan.dof_eq, plan.prescribed, {"plan": plan})
+
+
+@dataclass
+class MaterialPoints:
+    """Per-Gauss-point history held on the device by a plan (assembly.hpp:76-88)."""
+
+    plan: Plan
+
+    def commit(self):
+        self.plan.commit()
+
+    def state(self, committed=True):
+        return self.plan.state(committed)
+
+
+def make_material_points(model: Model, precision: str = "fp64") -> MaterialPoints:
+    return MaterialPoints(Plan(model, precision))
+
+
+def assemble_material_tangent(model: Model, u, mp: MaterialPoints, f_int=None) -> LinearSystem:
+    """Consistent tangent + internal force at the full displacement u (assembly.hpp:95-108).
+    `u` is (N,3) or (3N,); f_int (torch, 3N) is filled when given."""
+    plan = mp.plan
+    vals, fi, rhs = plan.assemble_tangent(np.asarray(u, dtype=np.float64).reshape(-1) if not isinstance(u, torch.Tensor) else u.reshape(-1),
+                                          model.external_load_vector(), f_int=f_int)
+    rp, ci = plan.pattern()
+    return LinearSystem(plan.n_free, rp, ci, vals, rhs, plan.dof_eq, plan.prescribed, {"f_int": fi})
+
+
+def element_stiffness(etype: int, coords, E, nu, precision: str = "fp64") -> torch.Tensor:
+    """Dense K_e for a batch of elements: coords (n,3) or (B,n,3); E, nu scalars or (B,)."""
+    lib = _lib.load()
+    dev = torch.device("cuda")
+    x = _dev(coords, torch.float64, dev)
+    single = x.dim() == 2
+    x = x.reshape(-1, NODES[etype], 3)
+    B = x.shape[0]
+    Ev = _dev(np.broadcast_to(np.asarray(E, dtype=np.float64), (B,)), torch.float64, dev)
+    nv = _dev(np.broadcast_to(np.asarray(nu, dtype=np.float64), (B,)), torch.float64, dev)
+    nd = 3 * NODES[etype]
+    Ke = torch.empty(B, nd, nd, dtype=torch.float64, device=dev)
+    _lib.check(lib.cxg_element_stiffness(etype, B, _ptr(x), _ptr(Ev), _ptr(nv),
+                                         _lib.MIXED if precision == "mixed" else _lib.FP64, _ptr(Ke), _stream()))
+    return Ke[0] if single else Ke
+
+
+def element_tangent_force(etype: int, coords, ue, material: Material, state=None, precision: str = "fp64"):
+    """(Ke, fe, trial_state) for a batch: coords/ue (B,n,3); state (B,ngp,13) committed history."""
+    lib = _lib.load()
+    dev = torch.device("cuda")
+    n, ngp = NODES[etype], NGP[etype]
+    x = _dev(coords, torch.float64, dev)
+    single = x.dim() == 2
+    x = x.reshape(-1, n, 3)
+    B = x.shape[0]
+    u = _dev(ue, torch.float64, dev).reshape(B, n, 3)
+    sc = None if state is None else _dev(state, torch.float64, dev).reshape(B, ngp, 13)
+    st = torch.empty(B, ngp, 13, dtype=torch.float64, device=dev)
+    nd = 3 * n
+    Ke = torch.empty(B, nd, nd, dtype=torch.float64, device=dev)
+    fe = torch.empty(B, nd, dtype=torch.float64, device=dev)
+    keep = []
+    cm = _c_material(material, keep)
+    _lib.check(lib.cxg_element_tangent_force(etype, B, _ptr(x), _ptr(u), C.byref(cm), _ptr(sc), _ptr(st),
+                                             _lib.MIXED if precision == "mixed" else _lib.FP64, _ptr(Ke),
+                                             _ptr(fe), _stream()))
+    if single:
+        return Ke[0], fe[0], st[0]
+    return Ke, fe, st

@@ -1,0 +1,663 @@
+// C ABI of libcxg.so (declared in include/cxg.h).
+//
+// Host-side runtime around the kernels: plan construction (mesh and DOF map made
+// resident in device memory, CSR pattern built on the device), host/device pointer
+// staging through plan-owned buffers, the assembly entry points, the per-Gauss-point
+// history round trips and the element-level batched entry points. No exception
+// crosses the ABI: every entry point returns a cxg_status and leaves a message for
+// cxg_last_error().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cxg.h"
+#include "cxg_internal.cuh"
+
+using namespace cxg;
+
+struct cxg_plan {
+  int device = 0;
+  int64_t n_nodes = 0, n_elems = 0, n_gauss = 0;
+  int32_t type = 0, n_free = 0, precision = 0;
+  double* coords = nullptr;
+  int32_t* conn = nullptr;
+  double* young = nullptr;
+  double* poisson = nullptr;
+  int32_t* elem_mat = nullptr;
+  J2Mat* mats = nullptr;
+  int32_t n_mats = 0;
+  bool has_plastic = false;
+  int32_t* dof_eq = nullptr;
+  double* prescribed = nullptr;
+  PatternOut pat;
+  double* state[2] = {nullptr, nullptr};  // SoA [13][G]: committed, trial
+  DevStatus* status = nullptr;
+  cudaStream_t last_stream = nullptr;
+  int64_t device_bytes = 0;
+  // staging buffers for host pointers, grown on demand and reused
+  void* stage[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  size_t stage_bytes[6] = {0, 0, 0, 0, 0, 0};
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_err(cudaError_t e, const char* where) {
+  if (e == cudaErrorMemoryAllocation)
+    return set_err(CXG_ERR_OUT_OF_MEMORY, std::string(where) + ": " + cudaGetErrorString(e));
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+    return set_err(CXG_ERR_NO_GPU, std::string(where) + ": " + cudaGetErrorString(e));
+  return set_err(CXG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CHECK_CUDA(expr, where)                 \
+  do {                                          \
+    cudaError_t _e = (expr);                    \
+    if (_e != cudaSuccess) return cuda_err(_e, where); \
+  } while (0)
+
+bool on_device(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+template <typename T>
+cudaError_t alloc_copy(T** dst, const T* src, size_t count, cudaStream_t s, int64_t* bytes) {
+  *bytes += static_cast<int64_t>(count * sizeof(T));
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess || !src || count == 0) return e;
+  return cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyDefault, s);
+}
+
+// Device view of a caller buffer: the pointer itself when it is device memory, else a
+// plan staging buffer (slot), filled from the host when `upload`.
+int staged(cxg_plan* p, int slot, const void* ptr, size_t bytes, bool upload, cudaStream_t s,
+           void** out) {
+  if (!ptr) {
+    *out = nullptr;
+    return CXG_OK;
+  }
+  if (on_device(ptr)) {
+    *out = const_cast<void*>(ptr);
+    return CXG_OK;
+  }
+  if (p->stage_bytes[slot] < bytes) {
+    cudaFree(p->stage[slot]);
+    p->stage[slot] = nullptr;
+    p->stage_bytes[slot] = 0;
+    CHECK_CUDA(cudaMalloc(&p->stage[slot], bytes), "staging allocation");
+    p->stage_bytes[slot] = bytes;
+  }
+  if (upload) CHECK_CUDA(cudaMemcpyAsync(p->stage[slot], ptr, bytes, cudaMemcpyHostToDevice, s), "upload");
+  *out = p->stage[slot];
+  return CXG_OK;
+}
+
+int build_mats(int32_t n, const cxg_material* m, std::vector<J2Mat>& out, bool* plastic) {
+  out.assign(static_cast<size_t>(n), J2Mat{});
+  *plastic = false;
+  for (int32_t i = 0; i < n; ++i) {
+    J2Mat& d = out[static_cast<size_t>(i)];
+    const cxg_material& s = m[i];
+    if (!(s.E > 0.0) || !(s.nu > -1.0 && s.nu < 0.5))
+      return set_err(CXG_ERR_INVALID_ARGUMENT, "material needs E > 0 and -1 < nu < 0.5");
+    d.plastic = s.n_plastic > 0 ? 1 : 0;
+    d.n = s.n_plastic > 0 ? s.n_plastic : 1;
+    d.h_kin = s.h_kin;
+    if (s.n_plastic > kMaxTable)
+      return set_err(CXG_ERR_UNSUPPORTED, "*PLASTIC table longer than 64 points");
+    if (s.n_plastic > 0) {
+      if (!s.eqplastic || !s.yield) return set_err(CXG_ERR_INVALID_ARGUMENT, "*PLASTIC table pointers are null");
+      for (int k = 0; k < s.n_plastic; ++k) {
+        d.ep[k] = s.eqplastic[k];
+        d.sy[k] = s.yield[k];
+      }
+      // J2PlasticMaterial constructor (src/fem/plasticity.cpp:57-63): kinematic /
+      // combined hardening takes H_kin from the first table slope when it is not given;
+      // pure kinematic hardening flattens the isotropic curve to the initial yield.
+      if (s.hardening == 1 || s.hardening == 2) {
+        if (d.h_kin == 0.0 && s.n_plastic >= 2 && d.ep[1] > d.ep[0])
+          d.h_kin = (d.sy[1] - d.sy[0]) / (d.ep[1] - d.ep[0]);
+        if (s.hardening == 1)
+          for (int k = 0; k < s.n_plastic; ++k) d.sy[k] = d.sy[0];
+      }
+      *plastic = true;
+    }
+  }
+  return CXG_OK;
+}
+
+__global__ void fill_props_kernel(const int32_t* elem_mat, const double* E, const double* nu, int n_mats,
+                                  int64_t n_elems, double* young, double* poisson, int* bad) {
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n_elems;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int m = elem_mat ? elem_mat[e] : 0;
+    if (m < 0 || m >= n_mats) {
+      atomicExch(bad, 1);
+      m = 0;
+    }
+    if (young) young[e] = E[m];
+    if (poisson) poisson[e] = nu[m];
+  }
+}
+
+int plan_status(cxg_plan* p, int64_t* bad) {
+  CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");
+  DevStatus st;
+  CHECK_CUDA(cudaMemcpy(&st, p->status, sizeof st, cudaMemcpyDeviceToHost), "status read");
+  if (bad) *bad = st.code ? static_cast<int64_t>(st.bad_elem) : -1;
+  if (st.code) {
+    DevStatus z{0, 0, ~0ull};
+    cudaMemcpy(p->status, &z, sizeof z, cudaMemcpyHostToDevice);
+    char buf[160];
+    if (st.code == CXG_ERR_NEGATIVE_JACOBIAN)
+      snprintf(buf, sizeof buf, "non-positive element Jacobian (bad connectivity?) at element index %llu",
+               st.bad_elem);
+    else
+      snprintf(buf, sizeof buf, "in-kernel error %d at element index %llu", st.code, st.bad_elem);
+    return set_err(st.code, buf);
+  }
+  return CXG_OK;
+}
+
+int ensure_state(cxg_plan* p, cudaStream_t s) {
+  if (p->state[0]) return CXG_OK;
+  const size_t bytes = sizeof(double) * kStateDoubles * static_cast<size_t>(std::max<int64_t>(p->n_gauss, 1));
+  for (int i = 0; i < 2; ++i) {
+    CHECK_CUDA(cudaMalloc(&p->state[i], bytes), "state allocation");
+    CHECK_CUDA(cudaMemsetAsync(p->state[i], 0, bytes, s), "state init");
+  }
+  p->device_bytes += 2 * static_cast<int64_t>(bytes);
+  return CXG_OK;
+}
+
+ElemArgs base_args(cxg_plan* p) {
+  ElemArgs a{};
+  a.n_elems = p->n_elems;
+  a.n_nodes = p->n_nodes;
+  a.coords = p->coords;
+  a.conn = p->conn;
+  a.young = p->young;
+  a.poisson = p->poisson;
+  a.elem_mat = p->elem_mat;
+  a.mats = p->mats;
+  a.node_base = p->pat.node_base;
+  a.node_rowlen = p->pat.node_rowlen;
+  a.node_mask = p->pat.node_mask;
+  a.node_eq0 = p->pat.node_eq0;
+  a.prescribed = p->prescribed;
+  a.slot = p->pat.slot;
+  a.n_gauss = p->n_gauss;
+  a.status = p->status;
+  return a;
+}
+
+int copy_out(void* dst, const void* dev, size_t bytes, cudaStream_t s) {
+  if (!dst || dst == dev) return CXG_OK;
+  CHECK_CUDA(cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDefault, s), "download");
+  return CXG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cxg_last_error(void) { return g_err.c_str(); }
+int cxg_abi_version(void) { return CXG_ABI_VERSION; }
+int cxg_nodes_per_element(int32_t t) { return nodes_of(t); }
+int cxg_gauss_points_per_element(int32_t t) { return gauss_of(t); }
+
+int cxg_plan_create(const cxg_mesh_desc* m, const cxg_dofmap_desc* d, int32_t precision, cxg_plan** out) {
+  if (!m || !d || !out) return set_err(CXG_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (!supported(m->elem_type)) return set_err(CXG_ERR_UNSUPPORTED, "unsupported element type");
+  if (m->n_nodes <= 0 || m->n_elems < 0 || !m->coords || (m->n_elems > 0 && !m->conn))
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "mesh needs n_nodes > 0, coords and conn");
+  if (m->n_materials < 1 || !m->materials) return set_err(CXG_ERR_INVALID_ARGUMENT, "mesh needs >= 1 material");
+  if (!d->dof_eq || !d->prescribed || d->n_free < 0) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad DOF map");
+  if (precision != CXG_FP64 && precision != CXG_MIXED) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad precision");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_err(CXG_ERR_NO_GPU, "no CUDA device");
+  }
+  CHECK_CUDA(ensure_tables(), "constant tables");
+
+  std::vector<J2Mat> mats;
+  bool plastic = false;
+  int rc = build_mats(m->n_materials, m->materials, mats, &plastic);
+  if (rc) return rc;
+
+  auto* p = new cxg_plan;
+  cudaGetDevice(&p->device);
+  p->n_nodes = m->n_nodes;
+  p->n_elems = m->n_elems;
+  p->type = m->elem_type;
+  p->n_free = d->n_free;
+  p->precision = precision;
+  p->n_gauss = m->n_elems * gauss_of(m->elem_type);
+  p->n_mats = m->n_materials;
+  p->has_plastic = plastic;
+  const int npe = nodes_of(m->elem_type);
+  cudaStream_t s = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete p;
+    return cuda_err(e, "stream");
+  }
+  auto fail = [&](int code) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    cxg_plan_destroy(p);
+    return code;
+  };
+#define TRYC(expr, where)                    \
+  do {                                       \
+    cudaError_t _e = (expr);                 \
+    if (_e != cudaSuccess) return fail(cuda_err(_e, where)); \
+  } while (0)
+  TRYC(alloc_copy(&p->coords, m->coords, 3 * static_cast<size_t>(m->n_nodes), s, &p->device_bytes), "coords");
+  TRYC(alloc_copy(&p->conn, m->conn, static_cast<size_t>(m->n_elems) * npe, s, &p->device_bytes), "conn");
+  TRYC(alloc_copy(&p->dof_eq, d->dof_eq, 3 * static_cast<size_t>(m->n_nodes), s, &p->device_bytes), "dof_eq");
+  TRYC(alloc_copy(&p->prescribed, d->prescribed, 3 * static_cast<size_t>(m->n_nodes), s, &p->device_bytes),
+       "prescribed");
+  TRYC(alloc_copy(&p->mats, mats.data(), mats.size(), s, &p->device_bytes), "materials");
+  if (m->elem_mat)
+    TRYC(alloc_copy(&p->elem_mat, m->elem_mat, static_cast<size_t>(m->n_elems), s, &p->device_bytes), "elem_mat");
+  TRYC(alloc_copy(&p->young, m->young, static_cast<size_t>(m->n_elems), s, &p->device_bytes), "young");
+  TRYC(alloc_copy(&p->poisson, m->poisson, static_cast<size_t>(m->n_elems), s, &p->device_bytes), "poisson");
+  {
+    std::vector<double> E(static_cast<size_t>(m->n_materials)), nu(E.size());
+    for (int32_t i = 0; i < m->n_materials; ++i) {
+      E[static_cast<size_t>(i)] = m->materials[i].E;
+      nu[static_cast<size_t>(i)] = m->materials[i].nu;
+    }
+    double *dE = nullptr, *dnu = nullptr;
+    int* dbad = nullptr;
+    int64_t dummy = 0;
+    TRYC(alloc_copy(&dE, E.data(), E.size(), s, &dummy), "material E");
+    TRYC(alloc_copy(&dnu, nu.data(), nu.size(), s, &dummy), "material nu");
+    TRYC(cudaMalloc(&dbad, sizeof(int)), "flag");
+    TRYC(cudaMemsetAsync(dbad, 0, sizeof(int), s), "flag");
+    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((m->n_elems + 255) / 256, 4096)));
+    fill_props_kernel<<<grid, 256, 0, s>>>(p->elem_mat, dE, dnu, m->n_materials, m->n_elems,
+                                           m->young ? nullptr : p->young, m->poisson ? nullptr : p->poisson, dbad);
+    TRYC(cudaGetLastError(), "material properties");
+    int bad = 0;
+    TRYC(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, s), "flag");
+    TRYC(cudaStreamSynchronize(s), "material properties");
+    cudaFree(dE);
+    cudaFree(dnu);
+    cudaFree(dbad);
+    if (bad) return fail(set_err(CXG_ERR_INVALID_ARGUMENT, "elem_mat index outside [0, n_materials)"));
+  }
+  TRYC(cudaMalloc(&p->status, sizeof(DevStatus)), "status");
+  {
+    DevStatus z{0, 0, ~0ull};
+    TRYC(cudaMemcpyAsync(p->status, &z, sizeof z, cudaMemcpyHostToDevice, s), "status");
+  }
+  const char* msg = nullptr;
+  rc = build_pattern(m->elem_type, m->n_nodes, m->n_elems, p->conn, p->dof_eq, d->n_free, &p->pat, &msg, s);
+  if (rc) return fail(set_err(rc, std::string("pattern: ") + (msg ? msg : "")));
+  p->device_bytes += p->pat.device_bytes;
+  TRYC(cudaStreamSynchronize(s), "plan build");
+#undef TRYC
+  cudaStreamDestroy(s);
+  *out = p;
+  return CXG_OK;
+}
+
+int cxg_plan_destroy(cxg_plan* p) {
+  if (!p) return CXG_OK;
+  if (p->last_stream) cudaStreamSynchronize(p->last_stream);
+  void* bufs[] = {p->coords, p->conn, p->young, p->poisson, p->elem_mat, p->mats, p->dof_eq, p->prescribed,
+                  p->pat.row_ptr, p->pat.col_idx, p->pat.node_base, p->pat.node_rowlen, p->pat.node_mask,
+                  p->pat.node_eq0, p->pat.slot, p->state[0], p->state[1], p->status};
+  for (void* b : bufs) cudaFree(b);
+  for (void* b : p->stage) cudaFree(b);
+  delete p;
+  return CXG_OK;
+}
+
+int cxg_plan_get_info(const cxg_plan* p, cxg_plan_info* info) {
+  if (!p || !info) return set_err(CXG_ERR_INVALID_ARGUMENT, "null argument");
+  info->n_nodes = p->n_nodes;
+  info->n_elems = p->n_elems;
+  info->elem_type = p->type;
+  info->n_free = p->n_free;
+  info->nnz = p->pat.nnz;
+  info->n_gauss_points = p->n_gauss;
+  info->precision = p->precision;
+  info->device = p->device;
+  info->device_bytes = p->device_bytes;
+  return CXG_OK;
+}
+
+int cxg_plan_set_precision(cxg_plan* p, int32_t precision) {
+  if (!p || (precision != CXG_FP64 && precision != CXG_MIXED))
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "bad precision");
+  p->precision = precision;
+  return CXG_OK;
+}
+
+int cxg_plan_get_pattern(const cxg_plan* p, int64_t* row_ptr, int32_t* col_idx) {
+  if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
+  if (row_ptr)
+    CHECK_CUDA(cudaMemcpy(row_ptr, p->pat.row_ptr, sizeof(int64_t) * (static_cast<size_t>(p->n_free) + 1),
+                          cudaMemcpyDefault), "row_ptr copy");
+  if (col_idx)
+    CHECK_CUDA(cudaMemcpy(col_idx, p->pat.col_idx, sizeof(int32_t) * static_cast<size_t>(p->pat.nnz),
+                          cudaMemcpyDefault), "col_idx copy");
+  return CXG_OK;
+}
+
+int cxg_plan_pattern_device(const cxg_plan* p, const int64_t** row_ptr, const int32_t** col_idx) {
+  if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
+  if (row_ptr) *row_ptr = p->pat.row_ptr;
+  if (col_idx) *col_idx = p->pat.col_idx;
+  return CXG_OK;
+}
+
+int cxg_plan_update_coords(cxg_plan* p, const double* coords) {
+  if (!p || !coords) return set_err(CXG_ERR_INVALID_ARGUMENT, "null argument");
+  CHECK_CUDA(cudaMemcpy(p->coords, coords, sizeof(double) * 3 * static_cast<size_t>(p->n_nodes), cudaMemcpyDefault),
+             "coords update");
+  return CXG_OK;
+}
+
+int cxg_plan_update_young(cxg_plan* p, const double* young) {
+  if (!p || !young) return set_err(CXG_ERR_INVALID_ARGUMENT, "null argument");
+  CHECK_CUDA(cudaMemcpy(p->young, young, sizeof(double) * static_cast<size_t>(p->n_elems), cudaMemcpyDefault),
+             "young update");
+  return CXG_OK;
+}
+
+int cxg_plan_check(cxg_plan* p, int64_t* bad) {
+  if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
+  return plan_status(p, bad);
+}
+
+int cxg_assemble_linear(cxg_plan* p, double* vals, double* rhs, const double* f_ext, void* stream) {
+  if (!p || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan and vals are required");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
+  const size_t rb = sizeof(double) * static_cast<size_t>(p->n_free);
+  const size_t fb = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
+  void *dv, *dr, *df;
+  int rc = staged(p, 0, vals, vb, false, s, &dv);
+  if (!rc) rc = staged(p, 1, rhs, rb, false, s, &dr);
+  if (!rc) rc = staged(p, 2, f_ext, fb, true, s, &df);
+  if (rc) return rc;
+  CHECK_CUDA(cudaMemsetAsync(dv, 0, vb, s), "zero vals");
+  if (dr) CHECK_CUDA(launch_rhs_init(p->dof_eq, static_cast<const double*>(df), 3 * p->n_nodes,
+                                     static_cast<double*>(dr), s), "rhs init");
+  ElemArgs a = base_args(p);
+  a.vals = static_cast<double*>(dv);
+  a.rhs = static_cast<double*>(dr);
+  CHECK_CUDA(launch_element_kernel(p->type, MODE_LINEAR, false, p->precision, a, s), "element kernel");
+  if ((rc = copy_out(vals, dv, vb, s))) return rc;
+  if ((rc = copy_out(rhs, dr, rb, s))) return rc;
+  if (dv != vals || (rhs && dr != rhs)) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
+  return CXG_OK;
+}
+
+int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_int, double* rhs,
+                         const double* f_ext, void* stream) {
+  if (!p || !u || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, u and vals are required");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  int rc = ensure_state(p, s);
+  if (rc) return rc;
+  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
+  const size_t rb = sizeof(double) * static_cast<size_t>(p->n_free);
+  const size_t fb = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
+  void *dv, *dr, *df, *du, *dfi;
+  rc = staged(p, 0, vals, vb, false, s, &dv);
+  if (!rc) rc = staged(p, 1, rhs, rb, false, s, &dr);
+  if (!rc) rc = staged(p, 2, f_ext, fb, true, s, &df);
+  if (!rc) rc = staged(p, 3, u, fb, true, s, &du);
+  if (!rc) rc = staged(p, 4, f_int, fb, false, s, &dfi);
+  if (rc) return rc;
+  CHECK_CUDA(cudaMemsetAsync(dv, 0, vb, s), "zero vals");
+  if (dfi) CHECK_CUDA(cudaMemsetAsync(dfi, 0, fb, s), "zero f_int");
+  if (dr) CHECK_CUDA(launch_rhs_init(p->dof_eq, static_cast<const double*>(df), 3 * p->n_nodes,
+                                     static_cast<double*>(dr), s), "rhs init");
+  ElemArgs a = base_args(p);
+  a.vals = static_cast<double*>(dv);
+  a.rhs = static_cast<double*>(dr);
+  a.f_int = static_cast<double*>(dfi);
+  a.u = static_cast<const double*>(du);
+  a.state_c = p->state[0];
+  a.state_t = p->state[1];
+  CHECK_CUDA(launch_element_kernel(p->type, MODE_TANGENT, false, p->precision, a, s), "element kernel");
+  if ((rc = copy_out(vals, dv, vb, s))) return rc;
+  if ((rc = copy_out(rhs, dr, rb, s))) return rc;
+  if ((rc = copy_out(f_int, dfi, fb, s))) return rc;
+  if (dv != vals || (rhs && dr != rhs) || (f_int && dfi != f_int)) CHECK_CUDA(cudaStreamSynchronize(s), "sync");
+  return CXG_OK;
+}
+
+int cxg_state_get(const cxg_plan* cp, int32_t slot, double* out) {
+  auto* p = const_cast<cxg_plan*>(cp);
+  if (!p || !out || (slot != 0 && slot != 1)) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");
+  const size_t bytes = sizeof(double) * kStateDoubles * static_cast<size_t>(p->n_gauss);
+  int rc = ensure_state(p, nullptr);
+  if (rc) return rc;
+  CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");
+  void* tmp = nullptr;
+  CHECK_CUDA(cudaMalloc(&tmp, std::max<size_t>(bytes, 8)), "state staging");
+  cudaError_t e = launch_state_transpose(p->state[slot], static_cast<double*>(tmp), p->n_gauss, false, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(out, tmp, bytes, cudaMemcpyDefault);
+  cudaFree(tmp);
+  CHECK_CUDA(e, "state read");
+  return CXG_OK;
+}
+
+int cxg_state_set(cxg_plan* p, int32_t slot, const double* in) {
+  if (!p || !in || (slot != 0 && slot != 1)) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");
+  const size_t bytes = sizeof(double) * kStateDoubles * static_cast<size_t>(p->n_gauss);
+  int rc = ensure_state(p, nullptr);
+  if (rc) return rc;
+  CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");
+  void* tmp = nullptr;
+  CHECK_CUDA(cudaMalloc(&tmp, std::max<size_t>(bytes, 8)), "state staging");
+  cudaError_t e = cudaMemcpy(tmp, in, bytes, cudaMemcpyDefault);
+  if (e == cudaSuccess) e = launch_state_transpose(static_cast<double*>(tmp), p->state[slot], p->n_gauss, true, nullptr);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(tmp);
+  CHECK_CUDA(e, "state write");
+  return CXG_OK;
+}
+
+int cxg_state_commit(cxg_plan* p, void* stream) {
+  if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = ensure_state(p, s);
+  if (rc) return rc;
+  p->last_stream = s;
+  CHECK_CUDA(cudaMemcpyAsync(p->state[0], p->state[1], sizeof(double) * kStateDoubles * static_cast<size_t>(p->n_gauss),
+                             cudaMemcpyDeviceToDevice, s), "commit");
+  return CXG_OK;
+}
+
+namespace {
+
+// Shared body of the two element-level entry points.
+int element_level(int32_t t, int64_t n_elems, const double* coords, const double* ue, const double* young,
+                  const double* poisson, const cxg_material* material, const double* sc, double* st,
+                  int32_t precision, double* Ke, double* fe, cudaStream_t s, bool tangent) {
+  if (!supported(t)) return set_err(CXG_ERR_UNSUPPORTED, "unsupported element type");
+  if (n_elems < 0 || !coords || !Ke) return set_err(CXG_ERR_INVALID_ARGUMENT, "coords and Ke are required");
+  if (tangent && (!ue || !material || !fe)) return set_err(CXG_ERR_INVALID_ARGUMENT, "ue, material, fe required");
+  if (precision != 0 && precision != 1) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad precision");
+  CHECK_CUDA(ensure_tables(), "constant tables");
+  const int n = nodes_of(t), nq = gauss_of(t), nd = 3 * n;
+  const size_t E = static_cast<size_t>(n_elems);
+  std::vector<void*> owned;
+  auto cleanup = [&]() {
+    for (void* b : owned) cudaFree(b);
+  };
+  auto dev_in = [&](const void* ptr, size_t bytes, void** outp) -> cudaError_t {
+    if (!ptr) {
+      *outp = nullptr;
+      return cudaSuccess;
+    }
+    if (on_device(ptr)) {
+      *outp = const_cast<void*>(ptr);
+      return cudaSuccess;
+    }
+    cudaError_t e = cudaMalloc(outp, std::max<size_t>(bytes, 8));
+    if (e != cudaSuccess) return e;
+    owned.push_back(*outp);
+    return cudaMemcpyAsync(*outp, ptr, bytes, cudaMemcpyHostToDevice, s);
+  };
+  auto dev_out = [&](void* ptr, size_t bytes, void** outp) -> cudaError_t {
+    if (!ptr) {
+      *outp = nullptr;
+      return cudaSuccess;
+    }
+    if (on_device(ptr)) {
+      *outp = ptr;
+      return cudaSuccess;
+    }
+    cudaError_t e = cudaMalloc(outp, std::max<size_t>(bytes, 8));
+    if (e == cudaSuccess) owned.push_back(*outp);
+    return e;
+  };
+  ElemArgs a{};
+  a.n_elems = n_elems;
+  void *dc = nullptr, *du = nullptr, *dE = nullptr, *dnu = nullptr, *dK = nullptr, *dfe = nullptr;
+  cudaError_t e = dev_in(coords, sizeof(double) * E * nd, &dc);
+  if (e == cudaSuccess) e = dev_in(ue, sizeof(double) * E * nd, &du);
+  std::vector<double> hE, hnu;
+  if (e == cudaSuccess) {
+    if (tangent) {
+      hE.assign(std::max<size_t>(E, 1), material->E);
+      hnu.assign(std::max<size_t>(E, 1), material->nu);
+      e = dev_in(hE.data(), sizeof(double) * E, &dE);
+      if (e == cudaSuccess) e = dev_in(hnu.data(), sizeof(double) * E, &dnu);
+    } else {
+      e = dev_in(young, sizeof(double) * E, &dE);
+      if (e == cudaSuccess) e = dev_in(poisson, sizeof(double) * E, &dnu);
+    }
+  }
+  if (e == cudaSuccess) e = dev_out(Ke, sizeof(double) * E * nd * nd, &dK);
+  if (e == cudaSuccess && tangent) e = dev_out(fe, sizeof(double) * E * nd, &dfe);
+  if (e != cudaSuccess) {
+    cleanup();
+    return cuda_err(e, "element-level staging");
+  }
+  if (!dE || !dnu) {
+    cleanup();
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "young and poisson are required");
+  }
+  DevStatus* dst = nullptr;
+  J2Mat* dmat = nullptr;
+  double *dsc = nullptr, *dst_t = nullptr, *aos = nullptr;
+  const int64_t G = n_elems * nq;
+  const size_t sbytes = sizeof(double) * kStateDoubles * static_cast<size_t>(std::max<int64_t>(G, 1));
+  e = cudaMalloc(&dst, sizeof(DevStatus));
+  if (e == cudaSuccess) owned.push_back(dst);
+  DevStatus z{0, 0, ~0ull};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dst, &z, sizeof z, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && tangent) {
+    std::vector<J2Mat> mats;
+    bool plastic = false;
+    int rc = build_mats(1, material, mats, &plastic);
+    if (rc) {
+      cleanup();
+      return rc;
+    }
+    int64_t counted = 0;
+    e = alloc_copy(&dmat, mats.data(), 1, s, &counted);
+    if (e == cudaSuccess) owned.push_back(dmat);
+    if (e == cudaSuccess) e = cudaMalloc(&dsc, sbytes);
+    if (e == cudaSuccess) owned.push_back(dsc);
+    if (e == cudaSuccess) e = cudaMalloc(&dst_t, sbytes);
+    if (e == cudaSuccess) owned.push_back(dst_t);
+    if (e == cudaSuccess) e = cudaMalloc(&aos, sbytes);
+    if (e == cudaSuccess) owned.push_back(aos);
+    if (e == cudaSuccess) {
+      if (sc)
+        e = cudaMemcpyAsync(aos, sc, sizeof(double) * kStateDoubles * G, cudaMemcpyDefault, s);
+      else
+        e = cudaMemsetAsync(aos, 0, sbytes, s);
+    }
+    if (e == cudaSuccess) e = launch_state_transpose(aos, dsc, G, true, s);
+  }
+  if (e != cudaSuccess) {
+    cleanup();
+    return cuda_err(e, "element-level setup");
+  }
+  a.elem_coords = static_cast<const double*>(dc);
+  a.u = static_cast<const double*>(du);
+  a.young = static_cast<const double*>(dE);
+  a.poisson = static_cast<const double*>(dnu);
+  a.mats = dmat;
+  a.state_c = dsc;
+  a.state_t = dst_t;
+  a.n_gauss = G;
+  a.Ke = static_cast<double*>(dK);
+  a.fe = static_cast<double*>(dfe);
+  a.status = dst;
+  e = launch_element_kernel(t, tangent ? MODE_TANGENT : MODE_LINEAR, true, precision, a, s);
+  if (e == cudaSuccess && Ke != dK) e = cudaMemcpyAsync(Ke, dK, sizeof(double) * E * nd * nd, cudaMemcpyDefault, s);
+  if (e == cudaSuccess && tangent && fe != dfe) e = cudaMemcpyAsync(fe, dfe, sizeof(double) * E * nd, cudaMemcpyDefault, s);
+  if (e == cudaSuccess && tangent && st) {
+    e = launch_state_transpose(dst_t, aos, G, false, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(st, aos, sizeof(double) * kStateDoubles * G, cudaMemcpyDefault, s);
+  }
+  DevStatus hs{};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, dst, sizeof hs, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cleanup();
+  if (e != cudaSuccess) return cuda_err(e, "element-level kernel");
+  if (hs.code) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "non-positive element Jacobian (bad connectivity?) at element index %llu", hs.bad_elem);
+    return set_err(hs.code, buf);
+  }
+  return CXG_OK;
+}
+
+}  // namespace
+
+int cxg_element_stiffness(int32_t t, int64_t n_elems, const double* coords, const double* young,
+                          const double* poisson, int32_t precision, double* Ke, void* stream) {
+  return element_level(t, n_elems, coords, nullptr, young, poisson, nullptr, nullptr, nullptr, precision, Ke,
+                       nullptr, static_cast<cudaStream_t>(stream), false);
+}
+
+int cxg_element_tangent_force(int32_t t, int64_t n_elems, const double* coords, const double* ue,
+                              const cxg_material* material, const double* sc, double* st, int32_t precision,
+                              double* Ke, double* fe, void* stream) {
+  return element_level(t, n_elems, coords, ue, nullptr, nullptr, material, sc, st, precision, Ke, fe,
+                       static_cast<cudaStream_t>(stream), true);
+}
+
+int cxg_adjoint_compliance(cxg_plan* p, const double* u, double* dc_dE, double* dc_dX, void* stream) {
+  (void)p;
+  (void)u;
+  (void)dc_dE;
+  (void)dc_dX;
+  (void)stream;
+  return set_err(CXG_ERR_UNSUPPORTED, "adjoint not built yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+// Internal declarations shared by the kernels (cxg_kernels.cu, cxg_pattern.cu) and
+// the C-ABI layer (cxg_api.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "cxg_elements.hpp"
+
+namespace cxg {
+
+constexpr int kStateDoubles = 13;  // plastic strain[6], eq. plastic strain, back stress[6]
+constexpr int kMaxTable = 64;      // *PLASTIC table points per material
+
+// Device record of one material (J2PlasticMaterial, src/fem/plasticity.cpp:42-65, with
+// the kinematic-hardening table adjustment of its constructor already applied).
+struct J2Mat {
+  int32_t plastic;  // 0: linear elastic
+  int32_t n;        // table length
+  double h_kin;
+  double ep[kMaxTable];
+  double sy[kMaxTable];
+};
+
+// In-kernel error reporting: first error code and the smallest offending element.
+struct DevStatus {
+  int32_t code;
+  int32_t pad;
+  unsigned long long bad_elem;
+};
+
+enum KernelMode : int { MODE_LINEAR = 0, MODE_TANGENT = 1 };
+
+// Everything an element-integration launch reads or writes. Pointers are device
+// pointers; optional ones may be null.
+struct ElemArgs {
+  int64_t n_elems;
+  int64_t n_nodes;
+  // geometry: either a mesh (coords + conn) or per-element coordinates (dense mode)
+  const double* coords;     // [3N]
+  const int32_t* conn;      // [E*n]
+  const double* elem_coords;  // [E*n*3] (dense element-level mode)
+  const double* young;      // [E]
+  const double* poisson;    // [E]
+  const int32_t* elem_mat;  // [E] or null -> material 0
+  const J2Mat* mats;        // [n_mats]
+  // DOF map / CSR addressing (scatter mode)
+  const int64_t* node_base;   // [N] CSR offset of the node's first free row
+  const int32_t* node_rowlen; // [N] length of each of the node's rows
+  const uint8_t* node_mask;   // [N] bit i: component i free
+  const int32_t* node_eq0;    // [N] first free equation of the node (or -1)
+  const double* prescribed;   // [3N]
+  const uint16_t* slot;       // [E*n*n] column offset of node b inside node a's rows
+  // state (tangent mode), SoA [13][G]
+  const double* state_c;
+  double* state_t;
+  int64_t n_gauss;
+  // displacement (tangent mode)
+  const double* u;           // [3N] (mesh) or [E*n*3] (dense)
+  // outputs
+  double* vals;   // [nnz]
+  double* rhs;    // [n_free]
+  double* f_int;  // [3N]
+  double* Ke;     // dense [E*(3n)^2]
+  double* fe;     // dense [E*3n]
+  DevStatus* status;
+};
+
+// Launchers (cxg_kernels.cu). `precision` 0 = FP64, 1 = mixed.
+cudaError_t launch_element_kernel(int elem_type, int mode, bool dense, int precision,
+                                  const ElemArgs& a, cudaStream_t s);
+cudaError_t launch_rhs_init(const int32_t* dof_eq, const double* f_ext, int64_t ndof,
+                            double* rhs, cudaStream_t s);
+cudaError_t launch_state_transpose(const double* src, double* dst, int64_t G, bool to_soa,
+                                   cudaStream_t s);
+cudaError_t launch_adjoint(int elem_type, const ElemArgs& a, double* dc_dE, double* dc_dX,
+                           cudaStream_t s);
+// Element tables (constant memory) are uploaded once per device.
+cudaError_t ensure_tables();
+
+// Pattern construction (cxg_pattern.cu).
+struct PatternOut {
+  int64_t nnz = 0;
+  int64_t* row_ptr = nullptr;   // [n_free+1]
+  int32_t* col_idx = nullptr;   // [nnz]
+  int64_t* node_base = nullptr;
+  int32_t* node_rowlen = nullptr;
+  uint8_t* node_mask = nullptr;
+  int32_t* node_eq0 = nullptr;
+  uint16_t* slot = nullptr;     // [E*n*n]
+  int64_t device_bytes = 0;
+};
+// Returns a cxg_status code; on error *msg is set.
+int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t* d_conn,
+                  const int32_t* d_dof_eq, int32_t n_free, PatternOut* out, const char** msg,
+                  cudaStream_t s);
+
+}  // namespace cxg

@@ -1,0 +1,372 @@
+// CSR pattern of the reduced free/free system, built on the device.
+//
+// The reference accumulates (row, col) keys into an unordered_map element by element
+// (src/fem/assembly.cpp:76-100) and flushes unordered COO triplets (211-221). Here the
+// pattern is built once per mesh and DOF map, in canonical sorted CSR form:
+//   1. every element emits the n^2 node-pair keys a*N + b; a device radix sort and
+//      unique give the node adjacency graph, sorted by (a, b);
+//   2. each node a gets its free-component mask; all rows of a share one column
+//      structure (the free components of a's neighbours, ascending), so per node
+//      rowlen(a) = sum over neighbours of their free-component count and the offset
+//      of neighbour b inside a's rows is the running sum before b;
+//   3. node_base(a) = exclusive scan of (free rows of a) * rowlen(a); row_ptr and
+//      col_idx follow. This relies on the reference's free numbering being ascending
+//      in g = 3*node + comp (constraint_transform.cpp:78-82), which is validated;
+//   4. the slot map stores, per element and ordered node pair (a, b), the column
+//      offset of b inside a's rows (uint16), so the element kernel addresses
+//      vals[node_base(a) + r*rowlen(a) + slot + rank_b(j)] with no search.
+// The pattern is topological: an entry whose every element contribution is exactly
+// zero is kept (the reference skips exact-zero contributions, assembly.cpp:90).
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "cxg_internal.cuh"
+
+namespace cxg {
+namespace {
+
+__global__ void check_conn_kernel(const int32_t* conn, int64_t total, int64_t n_nodes, int* flag,
+                                  unsigned long long* bad, int npe) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t v = conn[i];
+    if (v < 0 || v >= n_nodes) {
+      atomicExch(flag, 1);
+      atomicMin(bad, static_cast<unsigned long long>(i / npe));
+    }
+  }
+}
+
+__global__ void free_flags_kernel(const int32_t* dof_eq, int64_t ndof, int32_t* flags) {
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < ndof;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    flags[g] = dof_eq[g] >= 0 ? 1 : 0;
+}
+
+__global__ void check_numbering_kernel(const int32_t* dof_eq, const int32_t* scan, int64_t ndof,
+                                       int* flag) {
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < ndof;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t eq = dof_eq[g];
+    if (eq >= 0 && eq != scan[g]) atomicExch(flag, 1);
+    if (eq < -1) atomicExch(flag, 1);
+  }
+}
+
+__global__ void node_info_kernel(const int32_t* dof_eq, int64_t n_nodes, uint8_t* mask,
+                                 int32_t* eq0) {
+  for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a < n_nodes;
+       a += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int m = 0;
+    int32_t first = -1;
+    for (int d = 0; d < 3; ++d) {
+      const int32_t eq = dof_eq[3 * a + d];
+      if (eq >= 0) {
+        m |= 1 << d;
+        if (first < 0) first = eq;
+      }
+    }
+    mask[a] = static_cast<uint8_t>(m);
+    eq0[a] = first;
+  }
+}
+
+__global__ void pair_keys_kernel(const int32_t* conn, int64_t n_elems, int npe, uint64_t N,
+                                 uint64_t* keys) {
+  const int64_t total = n_elems * npe * npe;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t e = i / (npe * npe);
+    const int r = static_cast<int>(i % (npe * npe));
+    const int a = r / npe, b = r % npe;
+    keys[i] = static_cast<uint64_t>(conn[e * npe + a]) * N + static_cast<uint64_t>(conn[e * npe + b]);
+  }
+}
+
+__global__ void node_ptr_kernel(const uint64_t* uniq, int64_t M, int64_t n_nodes, uint64_t N,
+                                int64_t* node_ptr) {
+  for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a <= n_nodes;
+       a += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t key = static_cast<uint64_t>(a) * N;
+    int64_t lo = 0, hi = M;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (uniq[mid] < key)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    node_ptr[a] = lo;
+  }
+}
+
+__global__ void rowlen_kernel(const uint64_t* uniq, const int64_t* node_ptr, int64_t n_nodes,
+                              uint64_t N, const uint8_t* mask, int32_t* rowlen, int32_t* adj_off,
+                              int64_t* node_nnz) {
+  for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a < n_nodes;
+       a += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int32_t run = 0;
+    for (int64_t t = node_ptr[a]; t < node_ptr[a + 1]; ++t) {
+      adj_off[t] = run;
+      run += __popc(mask[uniq[t] % N]);
+    }
+    rowlen[a] = run;
+    node_nnz[a] = static_cast<int64_t>(__popc(mask[a])) * run;
+  }
+}
+
+__global__ void row_ptr_kernel(int64_t n_nodes, const uint8_t* mask, const int32_t* eq0,
+                               const int64_t* node_base, const int32_t* rowlen, int64_t* row_ptr) {
+  for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a < n_nodes;
+       a += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int nf = __popc(mask[a]);
+    for (int r = 0; r < nf; ++r) row_ptr[eq0[a] + r] = node_base[a] + static_cast<int64_t>(r) * rowlen[a];
+  }
+}
+
+__global__ void col_idx_kernel(const uint64_t* uniq, int64_t M, uint64_t N, const uint8_t* mask,
+                               const int32_t* eq0, const int64_t* node_base, const int32_t* rowlen,
+                               const int32_t* adj_off, int32_t* col_idx) {
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < M;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t a = static_cast<int64_t>(uniq[t] / N);
+    const int64_t b = static_cast<int64_t>(uniq[t] % N);
+    const int nfa = __popc(mask[a]);
+    const int nfb = __popc(mask[b]);
+    for (int r = 0; r < nfa; ++r) {
+      const int64_t pos = node_base[a] + static_cast<int64_t>(r) * rowlen[a] + adj_off[t];
+      for (int j = 0; j < nfb; ++j) col_idx[pos + j] = eq0[b] + j;
+    }
+  }
+}
+
+__global__ void slot_kernel(const int32_t* conn, int64_t n_elems, int npe, uint64_t N,
+                            const uint64_t* uniq, const int64_t* node_ptr, const int32_t* adj_off,
+                            uint16_t* slot, int* overflow) {
+  const int64_t total = n_elems * npe * npe;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t e = i / (npe * npe);
+    const int r = static_cast<int>(i % (npe * npe));
+    const int64_t na = conn[e * npe + r / npe];
+    const uint64_t key = static_cast<uint64_t>(na) * N + static_cast<uint64_t>(conn[e * npe + r % npe]);
+    int64_t lo = node_ptr[na], hi = node_ptr[na + 1];
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (uniq[mid] < key)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    const int32_t off = adj_off[lo];
+    if (off > 65535) atomicExch(overflow, 1);
+    slot[i] = static_cast<uint16_t>(off);
+  }
+}
+
+unsigned grid_for(int64_t n, int threads = 256) {
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 65536)));
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count, int64_t* bytes) {
+  *bytes += static_cast<int64_t>(count * sizeof(T));
+  return cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T));
+}
+
+}  // namespace
+
+#define CXG_TRY(expr)                                  \
+  do {                                                 \
+    cudaError_t _e = (expr);                           \
+    if (_e != cudaSuccess) {                           \
+      *msg = cudaGetErrorString(_e);                   \
+      rc = _e == cudaErrorMemoryAllocation ? 3 : 2;    \
+      goto done;                                       \
+    }                                                  \
+  } while (0)
+
+int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t* d_conn,
+                  const int32_t* d_dof_eq, int32_t n_free, PatternOut* out, const char** msg,
+                  cudaStream_t s) {
+  const int npe = nodes_of(elem_type);
+  const uint64_t N = static_cast<uint64_t>(n_nodes);
+  const int64_t ndof = 3 * n_nodes;
+  const int64_t P = n_elems * npe * npe;
+  int rc = 0;
+  int64_t scratch = 0;
+  int* d_flag = nullptr;
+  unsigned long long* d_bad = nullptr;
+  int32_t* d_flags = nullptr;
+  int32_t* d_scan = nullptr;
+  uint64_t* d_keys = nullptr;
+  uint64_t* d_keys2 = nullptr;
+  void* d_temp = nullptr;
+  size_t temp_bytes = 0;
+  int64_t* d_M = nullptr;
+  int64_t* d_node_ptr = nullptr;
+  int32_t* d_adj_off = nullptr;
+  int64_t* d_node_nnz = nullptr;
+  int h_flag = 0;
+  int64_t M = 0;
+  uint64_t* uniq = nullptr;
+  unsigned long long h_bad = 0;
+  int end_bit = 1;
+
+  if (P >= (static_cast<int64_t>(1) << 31)) {
+    *msg = "mesh too large for one plan (n_elems * nodes^2 >= 2^31); split it into partitions";
+    return 5;
+  }
+  if (n_nodes >= (static_cast<int64_t>(1) << 31)) {
+    *msg = "node count exceeds int32 indexing";
+    return 5;
+  }
+  while (end_bit < 64 && (N * N) >> end_bit) ++end_bit;
+
+  CXG_TRY(cudaMalloc(&d_flag, sizeof(int)));
+  CXG_TRY(cudaMalloc(&d_bad, sizeof(unsigned long long)));
+  CXG_TRY(cudaMemsetAsync(d_flag, 0, sizeof(int), s));
+  CXG_TRY(cudaMemsetAsync(d_bad, 0xff, sizeof(unsigned long long), s));
+
+  // connectivity range check
+  check_conn_kernel<<<grid_for(n_elems * npe), 256, 0, s>>>(d_conn, n_elems * npe, n_nodes, d_flag, d_bad, npe);
+  CXG_TRY(cudaGetLastError());
+  CXG_TRY(cudaMemcpyAsync(&h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CXG_TRY(cudaMemcpyAsync(&h_bad, d_bad, sizeof(h_bad), cudaMemcpyDeviceToHost, s));
+  CXG_TRY(cudaStreamSynchronize(s));
+  if (h_flag) {
+    static thread_local char buf[160];
+    snprintf(buf, sizeof buf, "element references unknown node (element index %llu)", h_bad);
+    *msg = buf;
+    rc = 6;
+    goto done;
+  }
+
+  // free numbering must be ascending in g (SPC-only constraint transform)
+  CXG_TRY(cudaMalloc(&d_flags, sizeof(int32_t) * std::max<int64_t>(ndof, 1)));
+  CXG_TRY(cudaMalloc(&d_scan, sizeof(int32_t) * std::max<int64_t>(ndof, 1)));
+  free_flags_kernel<<<grid_for(ndof), 256, 0, s>>>(d_dof_eq, ndof, d_flags);
+  CXG_TRY(cudaGetLastError());
+  CXG_TRY(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, d_flags, d_scan, static_cast<int>(ndof), s));
+  CXG_TRY(cudaMalloc(&d_temp, temp_bytes));
+  CXG_TRY(cub::DeviceScan::ExclusiveSum(d_temp, temp_bytes, d_flags, d_scan, static_cast<int>(ndof), s));
+  check_numbering_kernel<<<grid_for(ndof), 256, 0, s>>>(d_dof_eq, d_scan, ndof, d_flag);
+  CXG_TRY(cudaGetLastError());
+  {
+    int32_t last_scan = 0, last_flag = 0;
+    if (ndof > 0) {
+      CXG_TRY(cudaMemcpyAsync(&last_scan, d_scan + ndof - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      CXG_TRY(cudaMemcpyAsync(&last_flag, d_flags + ndof - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    }
+    CXG_TRY(cudaMemcpyAsync(&h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CXG_TRY(cudaStreamSynchronize(s));
+    if (h_flag || last_scan + last_flag != n_free) {
+      *msg = "dof_eq must number the free DOFs 0..n_free-1 in increasing global DOF order "
+             "(SPC-only constraint transform)";
+      rc = 5;
+      goto done;
+    }
+  }
+  cudaFree(d_temp);
+  d_temp = nullptr;
+  cudaFree(d_flags);
+  d_flags = nullptr;
+  cudaFree(d_scan);
+  d_scan = nullptr;
+
+  CXG_TRY(dalloc(&out->node_mask, n_nodes, &out->device_bytes));
+  CXG_TRY(dalloc(&out->node_eq0, n_nodes, &out->device_bytes));
+  CXG_TRY(dalloc(&out->node_rowlen, n_nodes, &out->device_bytes));
+  CXG_TRY(dalloc(&out->node_base, n_nodes, &out->device_bytes));
+  node_info_kernel<<<grid_for(n_nodes), 256, 0, s>>>(d_dof_eq, n_nodes, out->node_mask, out->node_eq0);
+  CXG_TRY(cudaGetLastError());
+
+  // node adjacency by sort + unique of the element node-pair keys
+  CXG_TRY(dalloc(&d_keys, P, &scratch));
+  CXG_TRY(dalloc(&d_keys2, P, &scratch));
+  pair_keys_kernel<<<grid_for(P), 256, 0, s>>>(d_conn, n_elems, npe, N, d_keys);
+  CXG_TRY(cudaGetLastError());
+  {
+    cub::DoubleBuffer<uint64_t> db(d_keys, d_keys2);
+    temp_bytes = 0;
+    CXG_TRY(cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, db, static_cast<int>(P), 0, end_bit, s));
+    CXG_TRY(cudaMalloc(&d_temp, temp_bytes));
+    CXG_TRY(cub::DeviceRadixSort::SortKeys(d_temp, temp_bytes, db, static_cast<int>(P), 0, end_bit, s));
+    cudaFree(d_temp);
+    d_temp = nullptr;
+    uint64_t* sorted = db.Current();
+    uint64_t* other = db.Alternate();
+    CXG_TRY(cudaMalloc(&d_M, sizeof(int64_t)));
+    temp_bytes = 0;
+    CXG_TRY(cub::DeviceSelect::Unique(nullptr, temp_bytes, sorted, other, d_M, static_cast<int>(P), s));
+    CXG_TRY(cudaMalloc(&d_temp, temp_bytes));
+    CXG_TRY(cub::DeviceSelect::Unique(d_temp, temp_bytes, sorted, other, d_M, static_cast<int>(P), s));
+    CXG_TRY(cudaMemcpyAsync(&M, d_M, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CXG_TRY(cudaStreamSynchronize(s));
+    cudaFree(d_temp);
+    d_temp = nullptr;
+    uniq = other;
+  }
+
+  CXG_TRY(dalloc(&d_node_ptr, n_nodes + 1, &scratch));
+  CXG_TRY(dalloc(&d_adj_off, M, &scratch));
+  CXG_TRY(dalloc(&d_node_nnz, n_nodes, &scratch));
+  node_ptr_kernel<<<grid_for(n_nodes + 1), 256, 0, s>>>(uniq, M, n_nodes, N, d_node_ptr);
+  CXG_TRY(cudaGetLastError());
+  rowlen_kernel<<<grid_for(n_nodes), 256, 0, s>>>(uniq, d_node_ptr, n_nodes, N, out->node_mask,
+                                                  out->node_rowlen, d_adj_off, d_node_nnz);
+  CXG_TRY(cudaGetLastError());
+  temp_bytes = 0;
+  CXG_TRY(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, d_node_nnz, out->node_base, static_cast<int>(n_nodes), s));
+  CXG_TRY(cudaMalloc(&d_temp, temp_bytes));
+  CXG_TRY(cub::DeviceScan::ExclusiveSum(d_temp, temp_bytes, d_node_nnz, out->node_base, static_cast<int>(n_nodes), s));
+  {
+    int64_t last_base = 0, last_nnz = 0;
+    if (n_nodes > 0) {
+      CXG_TRY(cudaMemcpyAsync(&last_base, out->node_base + n_nodes - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      CXG_TRY(cudaMemcpyAsync(&last_nnz, d_node_nnz + n_nodes - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    }
+    CXG_TRY(cudaStreamSynchronize(s));
+    out->nnz = last_base + last_nnz;
+  }
+
+  CXG_TRY(dalloc(&out->row_ptr, static_cast<size_t>(n_free) + 1, &out->device_bytes));
+  CXG_TRY(dalloc(&out->col_idx, static_cast<size_t>(out->nnz), &out->device_bytes));
+  CXG_TRY(dalloc(&out->slot, static_cast<size_t>(P), &out->device_bytes));
+  row_ptr_kernel<<<grid_for(n_nodes), 256, 0, s>>>(n_nodes, out->node_mask, out->node_eq0, out->node_base,
+                                                   out->node_rowlen, out->row_ptr);
+  CXG_TRY(cudaGetLastError());
+  CXG_TRY(cudaMemcpyAsync(out->row_ptr + n_free, &out->nnz, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  col_idx_kernel<<<grid_for(M), 256, 0, s>>>(uniq, M, N, out->node_mask, out->node_eq0, out->node_base,
+                                             out->node_rowlen, d_adj_off, out->col_idx);
+  CXG_TRY(cudaGetLastError());
+  CXG_TRY(cudaMemsetAsync(d_flag, 0, sizeof(int), s));
+  slot_kernel<<<grid_for(P), 256, 0, s>>>(d_conn, n_elems, npe, N, uniq, d_node_ptr, d_adj_off, out->slot, d_flag);
+  CXG_TRY(cudaGetLastError());
+  CXG_TRY(cudaMemcpyAsync(&h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CXG_TRY(cudaStreamSynchronize(s));
+  if (h_flag) {
+    *msg = "a CSR row holds more than 65535 columns; not supported";
+    rc = 5;
+    goto done;
+  }
+
+done:
+  cudaFree(d_temp);
+  cudaFree(d_flag);
+  cudaFree(d_bad);
+  cudaFree(d_flags);
+  cudaFree(d_scan);
+  cudaFree(d_keys);
+  cudaFree(d_keys2);
+  cudaFree(d_M);
+  cudaFree(d_node_ptr);
+  cudaFree(d_adj_off);
+  cudaFree(d_node_nnz);
+  return rc;
+}
+
+}  // namespace cxg

@@ -1,0 +1,191 @@
+/* cxg — B200-native element integration and CSR assembly for CalculiX++.
+ *
+ * C ABI of libcxg.so (calculixpp_b200/_lib/libcxg.so). Plain pointers and sizes only.
+ * Every pointer argument may point to host or device memory; the library asks the
+ * CUDA driver which one it is and stages host buffers through device memory. Device
+ * pointers must belong to the current device. All entry points return a cxg_status;
+ * cxg_last_error() returns the thread's last error message.
+ *
+ * Conventions (identical to the reference, include/calculixpp/core/types.hpp:9-13 and
+ * include/calculixpp/fem/element.hpp:12-61):
+ *   - element type codes are the ordinals of cxpp::ElementType
+ *     (include/calculixpp/core/element.hpp:13-22): C3D8=2, C3D8R=3, C3D20=4,
+ *     C3D20R=5, C3D6=6, C3D15=7 (C3D4/C3D10 are not handled here);
+ *   - node indices are 0-based int32; DOF g = 3*node + component;
+ *   - element DOF order node-major [u1,v1,w1,u2,...]; Voigt xx,yy,zz,xy,xz,yz with
+ *     engineering shear;
+ *   - per-Gauss-point material history: 13 doubles {plastic strain[6], equivalent
+ *     plastic strain, back stress[6]} (include/calculixpp/fem/material_model.hpp:38-64),
+ *     Gauss points in element order then the element's Gauss-rule order.
+ *
+ * Reduced system: the free/free stiffness K_ff in CSR with int64 row_ptr and int32
+ * col_idx, rows and columns in free-equation order, columns ascending. It replaces
+ * the reference's COO LinearSystem (include/calculixpp/fem/assembly.hpp:18-38); the
+ * same triplets sorted by (row, col) give exactly this CSR.
+ */
+#ifndef CXG_H
+#define CXG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CXG_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define CXG_API __attribute__((visibility("default")))
+#else
+#define CXG_API
+#endif
+
+typedef enum {
+  CXG_OK = 0,
+  CXG_ERR_INVALID_ARGUMENT = 1,
+  CXG_ERR_CUDA = 2,
+  CXG_ERR_OUT_OF_MEMORY = 3,
+  /* det(J) <= 0 at a Gauss point: the reference throws
+   * "non-positive element Jacobian (bad connectivity?)" (src/fem/element.cpp:86-88). */
+  CXG_ERR_NEGATIVE_JACOBIAN = 4,
+  CXG_ERR_UNSUPPORTED = 5,
+  /* an element references a node index outside [0, n_nodes)
+   * (src/fem/assembly.cpp:53-54 "element references unknown node"). */
+  CXG_ERR_UNKNOWN_NODE = 6,
+  CXG_ERR_NO_GPU = 7
+} cxg_status;
+
+typedef enum { CXG_FP64 = 0, CXG_MIXED = 1 } cxg_precision;
+
+typedef enum { CXG_STATE_COMMITTED = 0, CXG_STATE_TRIAL = 1 } cxg_state_slot;
+
+/* Material of one element family. n_plastic == 0: linear isotropic elasticity
+ * (ElasticIsoMaterial, include/calculixpp/fem/material_model.hpp:84-93). Otherwise J2
+ * plasticity with a piecewise-linear *PLASTIC table (eqplastic[i], yield[i]) and
+ * hardening 0 = isotropic, 1 = kinematic, 2 = combined, kinematic modulus h_kin
+ * (J2PlasticMaterial, material_model.hpp:108-126). Table pointers are host memory. */
+typedef struct {
+  double E;
+  double nu;
+  int32_t n_plastic;
+  const double* eqplastic;
+  const double* yield;
+  int32_t hardening;
+  double h_kin;
+} cxg_material;
+
+/* One mesh of a single element type. young/poisson (per element) override the
+ * material's E and nu when non-NULL; elem_mat (per element) selects materials[],
+ * NULL means every element uses materials[0]. */
+typedef struct {
+  int64_t n_nodes;
+  int64_t n_elems;
+  int32_t elem_type;
+  const double* coords;   /* [3*n_nodes] */
+  const int32_t* conn;    /* [n_elems * nodes_per_element] */
+  const double* young;    /* [n_elems] or NULL */
+  const double* poisson;  /* [n_elems] or NULL */
+  const int32_t* elem_mat;  /* [n_elems] or NULL */
+  int32_t n_materials;
+  const cxg_material* materials; /* host array [n_materials] */
+} cxg_mesh_desc;
+
+/* Free-DOF map of an SPC-constrained model (ConstraintTransform::dof_eq and
+ * LinearSystem::prescribed, include/calculixpp/fem/constraint_transform.hpp:38-47):
+ * dof_eq[g] = free equation or -1; free equations numbered in increasing g.
+ * prescribed[g] = SPC value (0 for free DOFs). */
+typedef struct {
+  const int32_t* dof_eq;     /* [3*n_nodes] */
+  const double* prescribed;  /* [3*n_nodes] */
+  int32_t n_free;
+} cxg_dofmap_desc;
+
+typedef struct cxg_plan cxg_plan;
+
+typedef struct {
+  int64_t n_nodes;
+  int64_t n_elems;
+  int32_t elem_type;
+  int32_t n_free;
+  int64_t nnz;
+  int64_t n_gauss_points;
+  int32_t precision;
+  int32_t device;
+  int64_t device_bytes; /* device memory owned by the plan */
+} cxg_plan_info;
+
+CXG_API const char* cxg_last_error(void);
+CXG_API int cxg_abi_version(void);
+CXG_API int cxg_nodes_per_element(int32_t elem_type);
+CXG_API int cxg_gauss_points_per_element(int32_t elem_type);
+
+/* ---- plan: mesh + DOF map resident in device memory, CSR pattern built on device ---
+ * Replaces the per-call build_dof_map + hash-map scatter set-up of
+ * assemble_linear_static / assemble_material_tangent (src/fem/assembly.cpp:19-42,
+ * 76-110, 211-221): the pattern is built once and reused by every assembly. */
+CXG_API int cxg_plan_create(const cxg_mesh_desc* mesh, const cxg_dofmap_desc* dofs,
+                    int32_t precision, cxg_plan** out);
+CXG_API int cxg_plan_destroy(cxg_plan* plan);
+CXG_API int cxg_plan_get_info(const cxg_plan* plan, cxg_plan_info* info);
+CXG_API int cxg_plan_set_precision(cxg_plan* plan, int32_t precision);
+/* Copy the CSR pattern out (host or device destinations). */
+CXG_API int cxg_plan_get_pattern(const cxg_plan* plan, int64_t* row_ptr, int32_t* col_idx);
+/* Borrow the plan's device copies of the pattern (valid until destroy). */
+CXG_API int cxg_plan_pattern_device(const cxg_plan* plan, const int64_t** row_ptr,
+                            const int32_t** col_idx);
+/* Replace nodal coordinates [3*n_nodes] (same topology, e.g. design updates). */
+CXG_API int cxg_plan_update_coords(cxg_plan* plan, const double* coords);
+/* Replace per-element Young's moduli [n_elems]. */
+CXG_API int cxg_plan_update_young(cxg_plan* plan, const double* young);
+/* Synchronise the stream of the last launch and report the first in-kernel error
+ * (CXG_ERR_NEGATIVE_JACOBIAN, CXG_ERR_UNKNOWN_NODE) with the offending element. */
+CXG_API int cxg_plan_check(cxg_plan* plan, int64_t* bad_element);
+
+/* ---- assembly ------------------------------------------------------------------
+ * Linear static: vals[nnz] = K_ff; rhs[n_free] = T^T f_ext - K_fc u_c
+ * (assemble_linear_static, src/fem/assembly.cpp:225-257). f_ext[3*n_nodes] may be
+ * NULL. Asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream). */
+CXG_API int cxg_assemble_linear(cxg_plan* plan, double* vals, double* rhs, const double* f_ext,
+                        void* stream);
+
+/* Material-point tangent (assemble_material_tangent, src/fem/assembly.cpp:385-423):
+ * u[3*n_nodes] full displacement; vals = consistent tangent K_ff; f_int[3*n_nodes] =
+ * internal force; rhs = T^T f_ext - K_fc(tangent) u_c where u_c are the plan's
+ * prescribed values. Reads the committed state, writes the trial state. f_int, rhs
+ * and f_ext may be NULL. */
+CXG_API int cxg_assemble_tangent(cxg_plan* plan, const double* u, double* vals, double* f_int,
+                         double* rhs, const double* f_ext, void* stream);
+
+/* ---- per-Gauss-point history (MaterialPoints, include/calculixpp/fem/assembly.hpp:76-88)
+ * committed/trial buffers, 13 doubles per Gauss point. */
+CXG_API int cxg_state_get(const cxg_plan* plan, int32_t slot, double* out);
+CXG_API int cxg_state_set(cxg_plan* plan, int32_t slot, const double* in);
+/* trial -> committed (MaterialPoints::commit, assembly.hpp:84-87). */
+CXG_API int cxg_state_commit(cxg_plan* plan, void* stream);
+
+/* ---- element level (element_stiffness / element_tangent_force,
+ * include/calculixpp/fem/element.hpp:64-65, 156-164), batched over elements whose
+ * coordinates are given per element: coords[n_elems][n][3]. Dense outputs
+ * Ke[n_elems][3n][3n], fe[n_elems][3n]. */
+CXG_API int cxg_element_stiffness(int32_t elem_type, int64_t n_elems, const double* coords,
+                          const double* young, const double* poisson, int32_t precision,
+                          double* Ke, void* stream);
+CXG_API int cxg_element_tangent_force(int32_t elem_type, int64_t n_elems, const double* coords,
+                              const double* ue, const cxg_material* material,
+                              const double* state_committed, double* state_trial,
+                              int32_t precision, double* Ke, double* fe, void* stream);
+
+/* ---- adjoint of the compliance c = f^T u for K u = f with load independent of the
+ * design: dc/dE_e = -(1/E_e) u_e^T K_e u_e and dc/dX = -sum_e u_e^T dK_e/dX u_e,
+ * evaluated in closed form per Gauss point. Full-integration families (C3D8, C3D20,
+ * C3D20R, C3D6, C3D15) and linear elasticity. The reference computes the coordinate
+ * part by central differences of the reduced operator
+ * (src/numerics/sensitivity.cpp:77-108). dc_dE[n_elems], dc_dX[3*n_nodes]; either may
+ * be NULL. */
+CXG_API int cxg_adjoint_compliance(cxg_plan* plan, const double* u, double* dc_dE, double* dc_dX,
+                           void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CXG_H */

@@ -1,0 +1,156 @@
+"""Assembly parity of the CUDA path against the oracle's assemble_linear_static.
+
+Bars (FP64 path): CSR pattern (row_ptr, col_idx) bit-exact; values and rhs within
+1e-12 relative Frobenius; nodal displacements within 1e-10 relative L2 after the same
+sparse direct solve (scipy SuperLU on both operators). Mixed path: displacements within
+1e-6 relative L2 of the FP64 oracle."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from calculixpp_b200 import Plan, assemble_linear_static
+from calculixpp_b200 import meshgen as mg
+from calculixpp_b200.assembly import Material, Model
+from tests.helpers import ALL_TYPES, box_model, per_element_materials, rel_fro, to_np
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_system(port, model):
+    mats, em = per_element_materials(model)
+    dof_eq, pre, nf = model.dof_map()
+    return port.assemble_linear(model.mesh, mats, em, dof_eq, pre, nf, model.external_load_vector())
+
+
+def solve(n, rp, ci, v, rhs):
+    A = sp.csr_matrix((v, ci, rp), shape=(n, n))
+    return spla.spsolve(A.tocsc(), rhs)
+
+
+def compare_patterns(rp_g, ci_g, v_g, rp_o, ci_o, v_o, n):
+    """GPU pattern is topological; the oracle's skips exact-zero contributions. Equal
+    where the oracle has every topological entry; otherwise the extra GPU entries are
+    numerically zero and the shared ones agree."""
+    if np.array_equal(rp_g, rp_o) and np.array_equal(ci_g, ci_o):
+        return v_g, v_o, True
+    rows_g = np.repeat(np.arange(n), np.diff(rp_g))
+    rows_o = np.repeat(np.arange(n), np.diff(rp_o))
+    kg = rows_g.astype(np.int64) * n + ci_g
+    ko = rows_o.astype(np.int64) * n + ci_o
+    assert np.all(np.isin(ko, kg)), "oracle entry missing from the GPU pattern"
+    extra = ~np.isin(kg, ko)
+    assert np.abs(v_g[extra]).max() <= 1e-12 * np.abs(v_g).max()
+    return v_g[~extra], v_o, False
+
+
+def test_config1_cantilever_pattern_values_displacement(cuda, port):
+    cfg = mg.cantilever_c3d8_config1()
+    m = cfg["mesh"]
+    tip = cfg["tip"]
+    model = Model(m, [Material(210000.0, 0.3)], None, cfg["spc"],
+                  (tip, np.full(tip.size, 2), np.full(tip.size, -1000.0 / tip.size)))
+    sysg = assemble_linear_static(model)
+    rp, ci, v, rhs = oracle_system(port, model)
+    assert sysg.n_free == 1500 and v.size == 88218
+    assert np.array_equal(to_np(sysg.row_ptr), rp)
+    assert np.array_equal(to_np(sysg.col_idx), ci)
+    vg = to_np(sysg.vals)
+    assert rel_fro(vg, v) <= 1e-12
+    assert rel_fro(to_np(sysg.rhs), rhs) <= 1e-12
+    ug = solve(1500, rp, ci, vg, to_np(sysg.rhs))
+    uo = solve(1500, rp, ci, v, rhs)
+    assert rel_fro(ug, uo) <= 1e-10
+    # mixed precision: displacement within 1e-6 of the FP64 oracle
+    plan = sysg.extra["plan"]
+    plan.set_precision("mixed")
+    vm, rm = plan.assemble_linear(model.external_load_vector())
+    um = solve(1500, rp, ci, to_np(vm), to_np(rm))
+    assert rel_fro(um, uo) <= 1e-6
+
+
+@pytest.mark.parametrize("etype", ALL_TYPES)
+def test_all_families_small_box(cuda, port, etype):
+    quad = etype in (mg.C3D20, mg.C3D20R, mg.C3D15)
+    dims = (2, 2, 2) if quad else (3, 2, 2)
+    E = np.random.default_rng(etype).uniform(70e3, 210e3, size=mg.box_mesh(etype, *dims).n_elems)
+    model = box_model(etype, *dims, jitter=0.1, seed=etype, young=E)
+    sysg = assemble_linear_static(model)
+    rp, ci, v, rhs = oracle_system(port, model)
+    vg_cmp, vo_cmp, exact = compare_patterns(to_np(sysg.row_ptr), to_np(sysg.col_idx), to_np(sysg.vals),
+                                             rp, ci, v, sysg.n_free)
+    assert rel_fro(vg_cmp, vo_cmp) <= 1e-12
+    assert rel_fro(to_np(sysg.rhs), rhs) <= 1e-12
+    ug = solve(sysg.n_free, to_np(sysg.row_ptr), to_np(sysg.col_idx), to_np(sysg.vals), to_np(sysg.rhs))
+    uo = solve(sysg.n_free, rp, ci, v, rhs)
+    assert rel_fro(ug, uo) <= 1e-10
+    plan = sysg.extra["plan"]
+    plan.set_precision("mixed")
+    vm, rm = plan.assemble_linear(model.external_load_vector())
+    um = solve(sysg.n_free, to_np(sysg.row_ptr), to_np(sysg.col_idx), to_np(vm), to_np(rm))
+    assert rel_fro(um, uo) <= 1e-6
+
+
+def test_prescribed_displacement_rhs(cuda, port):
+    """Nonzero SPC values move -K_fc u_c into the rhs (src/fem/assembly.cpp:95-96)."""
+    model = box_model(mg.C3D20, 2, 2, 1, jitter=0.05, seed=9, prescribe=0.01)
+    sysg = assemble_linear_static(model)
+    rp, ci, v, rhs = oracle_system(port, model)
+    vgc, voc, _ = compare_patterns(to_np(sysg.row_ptr), to_np(sysg.col_idx), to_np(sysg.vals), rp, ci, v,
+                                   sysg.n_free)
+    assert rel_fro(vgc, voc) <= 1e-12
+    assert rel_fro(to_np(sysg.rhs), rhs) <= 1e-12
+    assert np.abs(rhs).max() > 0.0
+
+
+def test_c3d20_lognormal_block(cuda, port):
+    """Per-element lognormal E on a jittered C3D20 block (the 27-point benchmark case)."""
+    cfg = mg.c3d20_block(4, seed=2)
+    m = cfg["mesh"]
+    model = Model(m, [Material(200000.0, 0.3)], None, cfg["spc"], None)
+    f = cfg["f_ext"]
+    plan = Plan(model)
+    vg, rg = plan.assemble_linear(f)
+    mats, em = per_element_materials(model)
+    dof_eq, pre, nf = model.dof_map()
+    rp, ci, v, rhs = port.assemble_linear(m, mats, em, dof_eq, pre, nf, f)
+    rpg, cig = (to_np(t) for t in plan.pattern())
+    vgc, voc, _ = compare_patterns(rpg, cig, to_np(vg), rp, ci, v, nf)
+    assert rel_fro(vgc, voc) <= 1e-12
+    ug = solve(nf, rpg, cig, to_np(vg), to_np(rg))
+    uo = solve(nf, rp, ci, v, rhs)
+    assert rel_fro(ug, uo) <= 1e-10
+
+
+def test_repeat_assembly_bitwise_stable(cuda):
+    """Re-assembling into the same buffers gives the same operator to rounding (atomic
+    accumulation order may differ run to run; entries agree to 1e-15 relative)."""
+    model = box_model(mg.C3D8, 6, 4, 4, seed=5)
+    plan = Plan(model)
+    v1, r1 = (to_np(t).copy() for t in plan.assemble_linear(model.external_load_vector()))
+    v2, r2 = (to_np(t) for t in plan.assemble_linear(model.external_load_vector()))
+    assert rel_fro(v2, v1) <= 1e-15
+    assert np.array_equal(r1, r2)
+
+
+def test_unknown_node_rejected(cuda):
+    from calculixpp_b200 import CxgError
+    model = box_model(mg.C3D8, 2, 1, 1)
+    model.mesh.conn = model.mesh.conn.copy()
+    model.mesh.conn[1, 3] = model.mesh.n_nodes + 5
+    with pytest.raises(CxgError) as exc:
+        Plan(model)
+    assert exc.value.code == 6
+    assert "unknown node" in str(exc.value)
+
+
+def test_negative_jacobian_in_plan(cuda):
+    from calculixpp_b200 import CxgError
+    model = box_model(mg.C3D8, 2, 1, 1, jitter=0.0)
+    model.mesh.conn = model.mesh.conn.copy()
+    model.mesh.conn[1] = model.mesh.conn[1][[4, 5, 6, 7, 0, 1, 2, 3]]
+    plan = Plan(model)
+    with pytest.raises(CxgError) as exc:
+        plan.assemble_linear()
+    assert exc.value.code == 4
+    assert "non-positive element Jacobian" in str(exc.value)
