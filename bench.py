@@ -1,0 +1,416 @@
+"""Benchmark: element-integrations/s of the element-integration + CSR assembly path.
+
+Workload (default): the C3D20 full-integration (27-point) linear-elastic block, 64^3
+quadratic hexes of a unit cube (262,144 elements, 1,085,825 nodes, 3,257,475 DOF,
+557,286,921 CSR non-zeros), node jitter uniform +-0.05 h, per-element E lognormal
+(median 200000, sigma 0.3), nu 0.3, z=0 face clamped. Synthetic and seeded.
+
+One step = one assembly of K_ff and the rhs (vals zeroed, rhs from the load vector,
+every element integrated and scattered). `value` = mixed precision (FP32 integration,
+FP64 Jacobians and accumulation) element-integrations/s with all inputs resident in
+HBM; the FP64 path is measured in the same run ("fp64"). e2e = the same through the
+C ABI with host buffers: the load vector copied in and K_ff + rhs copied out each step.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--n 64]
+Multi-GPU (torchrun): every rank assembles its own block (weak scaling, no collective
+on the data path); timing is max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cxg", choices=["cxg", "reference"])
+    ap.add_argument("--n", type=int, default=64, help="cells per axis of the C3D20 block")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ---- distributed plumbing -------------------------------------------------------------
+def dist_init(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device(f"cuda:{local}"))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- clocks -------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        finally:
+            try:
+                os.remove(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded or sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ---- workload -----------------------------------------------------------------------------
+def c3d20_model(n, seed):
+    from calculixpp_b200 import meshgen as mg
+    from calculixpp_b200.assembly import Material, Model
+    cfg = mg.c3d20_block(n, seed=seed)
+    m = cfg["mesh"]
+    return Model(m, [Material(200000.0, 0.3)], None, cfg["spc"], None), cfg["f_ext"]
+
+
+def algorithmic_bytes(plan, model):
+    """Compulsory bytes of one linear assembly launch: connectivity, node coordinates,
+    per-element E and nu read once, every K_ff value written once."""
+    m = model.mesh
+    npe = m.conn.shape[1]
+    return 4 * npe * m.n_elems + 24 * m.n_nodes + 16 * m.n_elems + 8 * plan.nnz
+
+
+FLOPS_PER_ELEM_C3D20 = 27 * (2 * 9 * 20 + 60 + 2 * 9 * 20 + 45 * 20 * 21 // 2)
+
+
+def measure_peaks():
+    """cuBLAS DGEMM / SGEMM throughput (the FP64 / FP32 pipe references)."""
+    import torch
+    out = {}
+    for name, dt in (("fp64_tflops", torch.float64), ("fp32_tflops", torch.float32)):
+        torch.backends.cuda.matmul.allow_tf32 = False
+        n = 8192
+        a = torch.randn(n, n, dtype=dt, device="cuda")
+        b = torch.randn(n, n, dtype=dt, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            e.synchronize()
+            best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+        out[name] = best
+        del a, b
+    torch.cuda.empty_cache()
+    return out
+
+
+def time_steps(fn, steps, stream):
+    import torch
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(steps):
+        fn()
+    e.record(stream)
+    e.synchronize()
+    return s.elapsed_time(e) * 1e-3
+
+
+# ---- CPU baseline (the reference compiled from its sources, all host threads) ----------
+def cpu_baseline(seconds, seed=0):
+    from calculixpp_b200 import Plan
+    from oracle.oracle import Port, Ref
+    threads = len(os.sched_getaffinity(0))
+    n = 12
+    model, _ = c3d20_model(n, seed)
+    plan = Plan(model)
+    rp, ci = (t.cpu().numpy() for t in plan.pattern())
+    dof_eq, pre, _ = model.dof_map()
+    m = model.mesh
+    if Ref.available():
+        ref = Ref()
+        elems, t0 = 0, time.perf_counter()
+        while True:
+            ref.assemble_csr_threads(m, dof_eq, pre, rp, ci, threads)
+            elems += m.n_elems
+            if time.perf_counter() - t0 >= seconds:
+                break
+        dt = time.perf_counter() - t0
+        return {"value": elems / dt, "unit": "element-integrations/s", "cores": threads, "kind": "reference",
+                "sample": f"C3D20 {n}^3 block ({m.n_elems} elements) x {elems // m.n_elems} passes: reference "
+                          f"element_stiffness (src/fem/element.cpp) on {threads} threads + exact CSR scatter"}
+    port = Port()
+    from oracle.oracle import make_material
+    mats = [make_material(float(E), 0.3) for E in m.young]
+    em = np.arange(m.n_elems, dtype=np.int32)
+    nf = int((dof_eq >= 0).sum())
+    t0 = time.perf_counter()
+    elems = 0
+    while time.perf_counter() - t0 < seconds:
+        port.assemble_linear(m, mats, em, dof_eq, pre, nf)
+        elems += m.n_elems
+    dt = time.perf_counter() - t0
+    return {"value": elems / dt, "unit": "element-integrations/s", "cores": 1, "kind": "port",
+            "sample": f"C3D20 {n}^3 block x {elems // m.n_elems} passes through the oracle's C restatement"}
+
+
+def reference_arm(args, rank, world):
+    """--impl reference: the reference's own CPU implementation on the box's host cores."""
+    if rank != 0:
+        return
+    out = None
+    t_all = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(max(1.0, args.cpu_seconds / 4), seed=0)
+        if i >= args.warmup:
+            t_all.append(r["value"])
+        out = r
+    value = statistics.median(t_all)
+    line = {"impl": "reference", "metric": "element-integrations/s (K_e+f_int+J2), mixed vs FP64",
+            "value": value, "unit": "element-integrations/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"C3D20 27-point linear elastic block {args.n}^3 (sampled per step on the CPU)",
+                       "sample_per_step": out["sample"]},
+            "cpu_baseline": {"value": value, "unit": out["unit"], "cores": out["cores"], "kind": out["kind"],
+                             "sample": out["sample"]},
+            "e2e": {"value": value, "unit": "element-integrations/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args.gpus)
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    import torch
+
+    from calculixpp_b200 import Plan
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    model, f_ext = c3d20_model(args.n, seed=rank)
+    plan = Plan(model, "mixed")
+    m = model.mesh
+    d_f = torch.as_tensor(f_ext, device=dev)
+    vals = torch.empty(plan.nnz, dtype=torch.float64, device=dev)
+    rhs = torch.empty(plan.n_free, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        plan.assemble_linear(d_f, vals=vals, rhs=rhs, check=False)
+
+    def kernel_only():
+        plan.accumulate_linear(vals, None)
+
+    results = {}
+    clocks = None
+    for prec in ("fp64", "mixed"):
+        plan.set_precision(prec)
+        for _ in range(args.warmup):
+            step()
+        plan.check()
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        if prec == "mixed":
+            with ClockSampler(local) as cs:
+                t = time_steps(step, args.steps, stream)
+            clocks = cs.summary()
+        else:
+            t = time_steps(step, args.steps, stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        t = max_over_ranks(t, world)
+        tk = time_steps(kernel_only, args.steps, stream)
+        tk = max_over_ranks(tk, world)
+        plan.check()
+        results[prec] = {"t": t, "t_kernel": tk}
+
+    # e2e through the C ABI with host buffers (pinned): load vector in, K_ff + rhs out.
+    h_f = torch.as_tensor(f_ext).pin_memory()
+    h_vals = torch.empty(plan.nnz, dtype=torch.float64).pin_memory()
+    h_rhs = torch.empty(plan.n_free, dtype=torch.float64).pin_memory()
+    import ctypes as C
+
+    from calculixpp_b200 import _lib
+    lib = _lib.load()
+    e2e_steps = max(1, min(args.steps, 5))
+
+    def e2e_step():
+        _lib.check(lib.cxg_assemble_linear(plan.h, C.c_void_p(h_vals.data_ptr()), C.c_void_p(h_rhs.data_ptr()),
+                                           C.c_void_p(h_f.data_ptr()), C.c_void_p(stream.cuda_stream)))
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+
+    # accuracy of the mixed path against FP64 on a reduced block (host sparse solve)
+    acc = None
+    if rank == 0:
+        acc = mixed_accuracy(12)
+
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    pipe = measure_peaks() if rank == 0 else {}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_seconds)
+
+    if rank != 0:
+        return
+    E = m.n_elems
+    mix, f64 = results["mixed"], results["fp64"]
+    value = world * E * args.steps / mix["t"]
+    B = algorithmic_bytes(plan, model)
+    achieved = B / (mix["t_kernel"] / args.steps) / 1e9
+    traffic = None
+    if os.path.exists(TRAFFIC_FILE):
+        traffic = json.load(open(TRAFFIC_FILE)).get(f"c3d20_{args.n}_mixed_linear")
+    line = {
+        "metric": "element-integrations/s (K_e+f_int+J2), mixed vs FP64",
+        "value": value,
+        "unit": "element-integrations/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": mix["t"] / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic (seeded C3D20 block, lognormal E)",
+        "config": {"workload": f"C3D20 27-point linear elastic block {args.n}^3",
+                   "elements": E, "nodes": m.n_nodes, "n_free": plan.n_free, "nnz": plan.nnz,
+                   "precision": "mixed: FP32 gradients/Gram blocks, FP64 Jacobians, diagonal blocks and accumulation",
+                   "l2": "outputs (8*nnz bytes) far larger than L2; no flush needed",
+                   "parallelism": f"independent block per GPU x{world}"},
+        "fp64": {"value": world * E * args.steps / f64["t"], "ms_per_step": f64["t"] / args.steps * 1e3,
+                 "kernel_ms": f64["t_kernel"] / args.steps * 1e3,
+                 "fp64_pipe": {"achieved_tflops": FLOPS_PER_ELEM_C3D20 * E / (f64["t_kernel"] / args.steps) / 1e12,
+                               "peak_tflops": pipe.get("fp64_tflops"),
+                               "peak_kind": "cuBLAS DGEMM 8192^3 measured in this run"}},
+        "speedup_mixed_vs_fp64": f64["t"] / mix["t"],
+        "mixed_accuracy": acc,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": traffic,
+                     "kernel": "element_kernel<C3D20, linear, scatter, float>",
+                     "kernel_ms": mix["t_kernel"] / args.steps * 1e3,
+                     "algorithmic_bytes": B, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * E * e2e_steps / t_e2e, "unit": "element-integrations/s",
+                "h2d_bytes_per_step": int(h_f.numel() * 8),
+                "d2h_bytes_per_step": int((h_vals.numel() + h_rhs.numel()) * 8)},
+        "gpu_launches": args.steps * 3,
+        "clocks": clocks,
+        "measured_pipe_peaks": pipe,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def mixed_accuracy(n):
+    """Relative L2 displacement error of the mixed path against FP64 after the same
+    host sparse direct solve, on an n^3 block of the benchmark workload."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    import torch
+
+    from calculixpp_b200 import Plan
+    model, f = c3d20_model(n, seed=0)
+    plan = Plan(model)
+    rp, ci = (t.cpu().numpy() for t in plan.pattern())
+    out = {}
+    u = {}
+    for prec in ("fp64", "mixed"):
+        plan.set_precision(prec)
+        v, r = plan.assemble_linear(torch.as_tensor(f, device=plan.device))
+        A = sp.csr_matrix((v.cpu().numpy(), ci, rp), shape=(plan.n_free, plan.n_free))
+        u[prec] = spla.spsolve(A.tocsc(), r.cpu().numpy())
+        out[f"K_{prec}"] = v.cpu().numpy()
+    err_u = float(np.linalg.norm(u["mixed"] - u["fp64"]) / np.linalg.norm(u["fp64"]))
+    err_k = float(np.linalg.norm(out["K_mixed"] - out["K_fp64"]) / np.linalg.norm(out["K_fp64"]))
+    plan.close()
+    return {"block": f"{n}^3", "disp_rel_l2": err_u, "K_rel_fro": err_k, "bar": 1e-6, "pass": err_u <= 1e-6}
+
+
+if __name__ == "__main__":
+    main()

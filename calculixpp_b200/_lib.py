@@ -22,6 +22,7 @@ CXG_ERR_NO_GPU = 7
 
 FP64, MIXED = 0, 1
 COMMITTED, TRIAL = 0, 1
+ACCUMULATE = 1
 
 _vp = C.c_void_p
 
@@ -71,6 +72,7 @@ SIGNATURES = {
     "cxg_plan_update_young": (C.c_int, [_vp, _vp]),
     "cxg_plan_check": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
     "cxg_assemble_linear": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cxg_assemble_linear_ex": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int32, _vp]),
     "cxg_assemble_tangent": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cxg_state_get": (C.c_int, [_vp, C.c_int32, _vp]),
     "cxg_state_set": (C.c_int, [_vp, C.c_int32, _vp]),

@@ -197,6 +197,13 @@ class Plan:
                 self.check()
         return vals, rhs
 
+    def accumulate_linear(self, vals, rhs=None):
+        """Add this plan's element contributions to vals (and rhs) in place; the element
+        kernel alone, no zeroing and no load vector (cxg_assemble_linear_ex, CXG_ACCUMULATE)."""
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_assemble_linear_ex(self.h, _ptr(vals), _ptr(rhs), None, _lib.ACCUMULATE,
+                                                       _stream()))
+
     def assemble_tangent(self, u, f_ext=None, vals=None, f_int=None, rhs=None, check=True):
         dev = self.device
         vals = torch.empty(self.nnz, dtype=torch.float64, device=dev) if vals is None else vals
@@ -281,8 +288,8 @@ def element_stiffness(etype: int, coords, E, nu, precision: str = "fp64") -> tor
     single = x.dim() == 2
     x = x.reshape(-1, NODES[etype], 3)
     B = x.shape[0]
-    Ev = _dev(np.broadcast_to(np.asarray(E, dtype=np.float64), (B,)), torch.float64, dev)
-    nv = _dev(np.broadcast_to(np.asarray(nu, dtype=np.float64), (B,)), torch.float64, dev)
+    Ev = _dev(np.broadcast_to(np.asarray(E, dtype=np.float64), (B,)).copy(), torch.float64, dev)
+    nv = _dev(np.broadcast_to(np.asarray(nu, dtype=np.float64), (B,)).copy(), torch.float64, dev)
     nd = 3 * NODES[etype]
     Ke = torch.empty(B, nd, nd, dtype=torch.float64, device=dev)
     _lib.check(lib.cxg_element_stiffness(etype, B, _ptr(x), _ptr(Ev), _ptr(nv),

@@ -393,20 +393,28 @@ int cxg_plan_check(cxg_plan* p, int64_t* bad) {
 }
 
 int cxg_assemble_linear(cxg_plan* p, double* vals, double* rhs, const double* f_ext, void* stream) {
+  return cxg_assemble_linear_ex(p, vals, rhs, f_ext, 0, stream);
+}
+
+int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double* f_ext, int32_t flags,
+                           void* stream) {
   if (!p || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan and vals are required");
+  const bool accumulate = (flags & CXG_ACCUMULATE) != 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
   const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
   const size_t rb = sizeof(double) * static_cast<size_t>(p->n_free);
   const size_t fb = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
-  void *dv, *dr, *df;
-  int rc = staged(p, 0, vals, vb, false, s, &dv);
-  if (!rc) rc = staged(p, 1, rhs, rb, false, s, &dr);
-  if (!rc) rc = staged(p, 2, f_ext, fb, true, s, &df);
+  void *dv, *dr, *df = nullptr;
+  int rc = staged(p, 0, vals, vb, accumulate, s, &dv);
+  if (!rc) rc = staged(p, 1, rhs, rb, accumulate, s, &dr);
+  if (!rc && !accumulate) rc = staged(p, 2, f_ext, fb, true, s, &df);
   if (rc) return rc;
-  CHECK_CUDA(cudaMemsetAsync(dv, 0, vb, s), "zero vals");
-  if (dr) CHECK_CUDA(launch_rhs_init(p->dof_eq, static_cast<const double*>(df), 3 * p->n_nodes,
-                                     static_cast<double*>(dr), s), "rhs init");
+  if (!accumulate) {
+    CHECK_CUDA(cudaMemsetAsync(dv, 0, vb, s), "zero vals");
+    if (dr) CHECK_CUDA(launch_rhs_init(p->dof_eq, static_cast<const double*>(df), 3 * p->n_nodes,
+                                       static_cast<double*>(dr), s), "rhs init");
+  }
   ElemArgs a = base_args(p);
   a.vals = static_cast<double*>(dv);
   a.rhs = static_cast<double*>(dr);

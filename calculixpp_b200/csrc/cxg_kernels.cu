@@ -175,7 +175,14 @@ struct WarpSmem {
   static constexpr int nq = gauss_of(ET);
   static constexpr int GS = 3 * n + 1;
   static constexpr bool T = MODE == MODE_TANGENT;
+  static constexpr bool DF = sizeof(R) == 4;  // mixed precision: diagonal blocks from row sums
+  static constexpr int GD = T ? 27 : 9;
   double x[3 * n];
+  double gd[DF ? n * GD : 1];  // per-node FP64 sums of the off-diagonal Gram blocks
+  double gam[32];
+  double kappa;
+  double gc[3 * n];  // FP64 gradients at the last Gauss point (C3D8R: the centroid)
+  double vol;        // w det J there (C3D8R: 8 det J = element volume)
   double u[T ? 3 * n : 1];
   double presc[3 * n];
   double sig[T ? nq * 6 : 1];  // s_q * sigma_q (Voigt)
@@ -189,39 +196,179 @@ struct WarpSmem {
   R s[nq];                     // w_q det J_q
   R dp[T ? nq * 4 : 1];        // s*lam*, s*mu*, s*c per Gauss point
   R m[T ? nq * GS : 1];        // N_q g_k (plastic points)
-  R gam[32];
-  R kappa;
   double mu_hg;
 };
+
+// Gram blocks of node pair (a, b) over the Gauss points, in precision R:
+//   elastic points only : G1 = sum_q s_q g_a g_b^T
+//   with plastic points : G1 = sum_q (s lam*)_q g_a g_b^T, G2 = sum_q (s mu*)_q g_a g_b^T,
+//                         G3 = sum_q (s c)_q m_a m_b^T   (m = N g, N the return direction)
+template <int n, int nq, bool TAN, typename R, typename WS>
+__device__ __forceinline__ void gram(const WS& W, int a, int b, bool plastic, R (&G1)[3][3], R (&G2)[3][3],
+                                     R (&G3)[3][3]) {
+  constexpr int GS = 3 * n + 1;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) G1[i][j] = G2[i][j] = G3[i][j] = R(0);
+  if (!TAN || !plastic) {
+#pragma unroll 3
+    for (int q = 0; q < nq; ++q) {
+      const R* gq = W.g + q * GS;
+      const R s = W.s[q];
+      const R ga[3] = {s * gq[a], s * gq[n + a], s * gq[2 * n + a]};
+      const R gb[3] = {gq[b], gq[n + b], gq[2 * n + b]};
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) G1[i][j] += ga[i] * gb[j];
+    }
+    return;
+  }
+  if (TAN) {
+    for (int q = 0; q < nq; ++q) {
+      const R* gq = W.g + q * GS;
+      const R sl = W.dp[q * 4 + 0], sm = W.dp[q * 4 + 1], sc = W.dp[q * 4 + 2];
+      const R ga[3] = {gq[a], gq[n + a], gq[2 * n + a]};
+      const R gb[3] = {gq[b], gq[n + b], gq[2 * n + b]};
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          G1[i][j] += (sl * ga[i]) * gb[j];
+          G2[i][j] += (sm * ga[i]) * gb[j];
+        }
+      if (sc != R(0)) {
+        const R* mq = W.m + q * GS;
+        const R ma[3] = {sc * mq[a], sc * mq[n + a], sc * mq[2 * n + a]};
+        const R mb[3] = {mq[b], mq[n + b], mq[2 * n + b]};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) G3[i][j] += ma[i] * mb[j];
+      }
+    }
+  }
+}
+
+// K_ab from its Gram blocks, in FP64:
+//   elastic: lam G1 + mu (G1^T + tr(G1) I)        (= B_a^T D B_b summed over the points)
+//   plastic: G1 + G2^T + tr(G2) I - G3
+template <typename T>
+__device__ __forceinline__ void combine(const T (&G1)[3][3], const T (&G2)[3][3], const T (&G3)[3][3],
+                                        bool plastic, double lam, double mu, double (&K)[3][3]) {
+  if (!plastic) {
+    const double tr = static_cast<double>(G1[0][0]) + static_cast<double>(G1[1][1]) + static_cast<double>(G1[2][2]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        K[i][j] = lam * static_cast<double>(G1[i][j]) + mu * static_cast<double>(G1[j][i]) + (i == j ? mu * tr : 0.0);
+    return;
+  }
+  const double tr = static_cast<double>(G2[0][0]) + static_cast<double>(G2[1][1]) + static_cast<double>(G2[2][2]);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      K[i][j] = static_cast<double>(G1[i][j]) + static_cast<double>(G2[j][i]) + (i == j ? tr : 0.0) -
+                static_cast<double>(G3[i][j]);
+}
+
+// C3D8R hourglass stiffness kappa sum_alpha gamma_alpha,a gamma_alpha,b on the block
+// diagonal (src/fem/element.cpp:583-595).
+template <typename WS>
+__device__ __forceinline__ void add_hourglass(const WS& W, int a, int b, double (&K)[3][3]) {
+  double h = 0.0;
+  for (int al = 0; al < 4; ++al) h += W.gam[al * 8 + a] * W.gam[al * 8 + b];
+  h *= W.kappa;
+  K[0][0] += h;
+  K[1][1] += h;
+  K[2][2] += h;
+}
+
+// Dense element-matrix store, or CSR scatter with FP64 atomic adds: rows of node a /
+// columns of node b, and (a != b) the transposed block into rows of b. Prescribed
+// columns move -K_fc u_c into the rhs (src/fem/assembly.cpp:95-96).
+template <int n, bool DENSE, typename WS>
+__device__ __forceinline__ void write_pair(const ElemArgs& A, const WS& W, int64_t e, int a, int b,
+                                           const double (&K)[3][3]) {
+  constexpr int nd = 3 * n;
+  if (DENSE) {
+    double* Ke = A.Ke + e * nd * nd;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        Ke[(3 * a + i) * nd + 3 * b + j] = K[i][j];
+        Ke[(3 * b + j) * nd + 3 * a + i] = K[i][j];
+      }
+    return;
+  }
+  const unsigned short* sl = A.slot + e * n * n;
+  const int ma = W.mask[a], mb = W.mask[b];
+  {
+    const int64_t col0 = sl[a * n + b];
+    for (int i = 0; i < 3; ++i) {
+      if (!((ma >> i) & 1)) continue;
+      const int ri = __popc(ma & ((1 << i) - 1));
+      double* row = A.vals + W.base[a] + static_cast<int64_t>(ri) * W.rowlen[a] + col0;
+      double rr = 0.0;
+      for (int j = 0; j < 3; ++j) {
+        if ((mb >> j) & 1)
+          atomicAdd(row + __popc(mb & ((1 << j) - 1)), K[i][j]);
+        else
+          rr -= K[i][j] * W.presc[3 * b + j];
+      }
+      if (A.rhs && rr != 0.0) atomicAdd(A.rhs + W.eq0[a] + ri, rr);
+    }
+  }
+  if (a != b) {
+    const int64_t col0 = sl[b * n + a];
+    for (int j = 0; j < 3; ++j) {
+      if (!((mb >> j) & 1)) continue;
+      const int rj = __popc(mb & ((1 << j) - 1));
+      double* row = A.vals + W.base[b] + static_cast<int64_t>(rj) * W.rowlen[b] + col0;
+      double rr = 0.0;
+      for (int i = 0; i < 3; ++i) {
+        if ((ma >> i) & 1)
+          atomicAdd(row + __popc(ma & ((1 << i) - 1)), K[i][j]);
+        else
+          rr -= K[i][j] * W.presc[3 * a + i];
+      }
+      if (A.rhs && rr != 0.0) atomicAdd(A.rhs + W.eq0[b] + rj, rr);
+    }
+  }
+}
 
 template <int ET, int MODE, bool DENSE, typename R>
 __global__ void __launch_bounds__(kThreads) element_kernel(ElemArgs A) {
   constexpr int n = nodes_of(ET);
   constexpr int nq = gauss_of(ET);
   constexpr int nd = 3 * n;
-  constexpr int NP = n * (n + 1) / 2;
+  constexpr int NPO = n * (n - 1) / 2;  // off-diagonal node pairs
   constexpr int GS = 3 * n + 1;
   constexpr bool TAN = MODE == MODE_TANGENT;
   using WS = WarpSmem<ET, MODE, R>;
+  constexpr bool DIAGFIX = WS::DF;
+  constexpr int GD = WS::GD;
 
   extern __shared__ __align__(16) unsigned char smem[];
   double* sdN = reinterpret_cast<double*>(smem);  // [n*3*nq]
   double* sw = sdN + n * 3 * nq;                  // [nq]
   unsigned short* spair = reinterpret_cast<unsigned short*>(sw + nq);
-  constexpr size_t cta_bytes = ((sizeof(double) * (n * 3 * nq + nq) + 2 * NP) + 15) / 16 * 16;
+  constexpr size_t cta_bytes = ((sizeof(double) * (n * 3 * nq + nq) + 2 * NPO) + 15) / 16 * 16;
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   WS& W = *reinterpret_cast<WS*>(smem + cta_bytes + warp * ((sizeof(WS) + 15) / 16 * 16));
 
   for (int i = threadIdx.x; i < n * 3 * nq; i += blockDim.x) sdN[i] = c_dN[dn_offset(ET) + i];
   for (int i = threadIdx.x; i < nq; i += blockDim.x) sw[i] = c_w[ET][i];
-  for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+  for (int i = threadIdx.x; i < NPO; i += blockDim.x) {
     int a = 0, r = i;
-    while (r >= n - a) {
-      r -= n - a;
+    while (r >= n - 1 - a) {
+      r -= n - 1 - a;
       ++a;
     }
-    spair[i] = static_cast<unsigned short>(a | ((a + r) << 8));
+    spair[i] = static_cast<unsigned short>(a | ((a + 1 + r) << 8));
   }
   __syncthreads();
 
@@ -291,6 +438,7 @@ __global__ void __launch_bounds__(kThreads) element_kernel(ElemArgs A) {
            (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * inv}};
       const double sq = det * sw[q];
       W.s[q] = static_cast<R>(sq);
+      if (ET == C3D8R) W.vol = sq;
       double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
       for (int k = 0; k < n; ++k) {
         const double d0 = sdN[(3 * k + 0) * nq + q], d1 = sdN[(3 * k + 1) * nq + q],
@@ -299,6 +447,7 @@ __global__ void __launch_bounds__(kThreads) element_kernel(ElemArgs A) {
         for (int i = 0; i < 3; ++i) {
           gk[i] = it[i][0] * d0 + it[i][1] * d1 + it[i][2] * d2;
           W.g[q * GS + i * n + k] = static_cast<R>(gk[i]);
+          if (ET == C3D8R) W.gc[i * n + k] = gk[i];
         }
         if (TAN) {
           for (int i = 0; i < 3; ++i)
@@ -346,134 +495,77 @@ __global__ void __launch_bounds__(kThreads) element_kernel(ElemArgs A) {
           for (int d = 0; d < 3; ++d) gx[d] += c_hg[al][j] * W.x[3 * j + d];
         for (int j = 0; j < 8; ++j) {
           double corr = 0.0;
-          for (int d = 0; d < 3; ++d) corr += gx[d] * static_cast<double>(W.g[d * n + j]);
-          W.gam[al * 8 + j] = static_cast<R>(c_hg[al][j] - corr);
+          for (int d = 0; d < 3; ++d) corr += gx[d] * W.gc[d * n + j];
+          W.gam[al * 8 + j] = c_hg[al][j] - corr;
         }
       }
       if (lane == 0) {
         double b2 = 0.0;
         for (int j = 0; j < 8; ++j)
           for (int d = 0; d < 3; ++d) {
-            const double b = W.g[d * n + j];
+            const double b = W.gc[d * n + j];
             b2 += b * b;
           }
-        const double vol = static_cast<double>(W.s[0]);  // 8 det J at the centroid
+        const double vol = W.vol;  // 8 det J at the centroid
         const double mu_hg = TAN ? W.mu_hg : mu_j2;
-        W.kappa = static_cast<R>(0.05 * mu_hg * vol * b2);
+        W.kappa = 0.05 * mu_hg * vol * b2;
       }
       __syncwarp();
     }
 
-    // ---- phase C: symmetric node-pair blocks --------------------------------------
-    const R rlam = static_cast<R>(lam), rmu = static_cast<R>(mu_el);
-    for (int pi = lane; pi < NP; pi += 32) {
+    // ---- phase C: node-pair blocks -------------------------------------------------
+    // Off-diagonal pairs (a < b) first. In mixed precision their Gram blocks are also
+    // summed per node in FP64, and the diagonal blocks are then formed as the negative
+    // of those sums: every block row of the element matrix sums to zero in FP64, so the
+    // rigid translations stay in the null space exactly (sum_b g_b = 0), which FP32
+    // rounding of the individual products would otherwise break.
+    const bool plastic_elem = TAN && any_plastic;
+    if (DIAGFIX) {
+      for (int t = lane; t < n * GD; t += 32) W.gd[t] = 0.0;
+      __syncwarp();
+    }
+    for (int pi = lane; pi < NPO; pi += 32) {
       const int pr = spair[pi];
       const int a = pr & 0xff, b = pr >> 8;
-      R K[3][3];
-      if (!TAN || !any_plastic) {
-        R G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-#pragma unroll 3
-        for (int q = 0; q < nq; ++q) {
-          const R* gq = W.g + q * GS;
-          const R s = W.s[q];
-          const R ga[3] = {s * gq[a], s * gq[n + a], s * gq[2 * n + a]};
-          const R gb[3] = {gq[b], gq[n + b], gq[2 * n + b]};
-#pragma unroll
-          for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) G[i][j] += ga[i] * gb[j];
-        }
-        const R tr = G[0][0] + G[1][1] + G[2][2];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int j = 0; j < 3; ++j) K[i][j] = rlam * G[i][j] + rmu * G[j][i] + (i == j ? rmu * tr : R(0));
-      } else {
-        R G1[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        R G2[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        R G3[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        for (int q = 0; q < nq; ++q) {
-          const R* gq = W.g + q * GS;
-          const R sl = W.dp[q * 4 + 0], sm = W.dp[q * 4 + 1], sc = W.dp[q * 4 + 2];
-          const R ga[3] = {gq[a], gq[n + a], gq[2 * n + a]};
-          const R gb[3] = {gq[b], gq[n + b], gq[2 * n + b]};
-#pragma unroll
-          for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-              G1[i][j] += (sl * ga[i]) * gb[j];
-              G2[i][j] += (sm * ga[i]) * gb[j];
-            }
-          if (sc != R(0)) {
-            const R* mq = W.m + q * GS;
-            const R ma[3] = {sc * mq[a], sc * mq[n + a], sc * mq[2 * n + a]};
-            const R mb[3] = {mq[b], mq[n + b], mq[2 * n + b]};
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-              for (int j = 0; j < 3; ++j) G3[i][j] += ma[i] * mb[j];
-          }
-        }
-        const R tr = G2[0][0] + G2[1][1] + G2[2][2];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int j = 0; j < 3; ++j) K[i][j] = G1[i][j] + G2[j][i] + (i == j ? tr : R(0)) - G3[i][j];
-      }
-      if (ET == C3D8R) {
-        R h = 0;
-        for (int al = 0; al < 4; ++al) h += W.gam[al * 8 + a] * W.gam[al * 8 + b];
-        h *= W.kappa;
-        K[0][0] += h;
-        K[1][1] += h;
-        K[2][2] += h;
-      }
-      if (DENSE) {
-        double* Ke = A.Ke + e * nd * nd;
+      R G1[3][3], G2[3][3], G3[3][3];
+      gram<n, nq, TAN>(W, a, b, plastic_elem, G1, G2, G3);
+      if (DIAGFIX) {
         for (int i = 0; i < 3; ++i)
           for (int j = 0; j < 3; ++j) {
-            Ke[(3 * a + i) * nd + 3 * b + j] = static_cast<double>(K[i][j]);
-            Ke[(3 * b + j) * nd + 3 * a + i] = static_cast<double>(K[i][j]);
-          }
-      } else {
-        const int ma = W.mask[a], mb = W.mask[b];
-        const unsigned short* sl = A.slot + e * n * n;
-        // rows of node a, columns of node b
-        {
-          const int64_t col0 = sl[a * n + b];
-          double rr[3] = {0, 0, 0};
-          for (int i = 0; i < 3; ++i) {
-            if (!((ma >> i) & 1)) continue;
-            const int ri = __popc(ma & ((1 << i) - 1));
-            double* row = A.vals + W.base[a] + static_cast<int64_t>(ri) * W.rowlen[a] + col0;
-            for (int j = 0; j < 3; ++j) {
-              if ((mb >> j) & 1) {
-                atomicAdd(row + __popc(mb & ((1 << j) - 1)), static_cast<double>(K[i][j]));
-              } else {
-                rr[i] -= static_cast<double>(K[i][j]) * W.presc[3 * b + j];
-              }
+            atomicAdd(&W.gd[a * GD + 3 * i + j], static_cast<double>(G1[i][j]));
+            atomicAdd(&W.gd[b * GD + 3 * j + i], static_cast<double>(G1[i][j]));
+            if (plastic_elem) {
+              atomicAdd(&W.gd[a * GD + 9 + 3 * i + j], static_cast<double>(G2[i][j]));
+              atomicAdd(&W.gd[b * GD + 9 + 3 * j + i], static_cast<double>(G2[i][j]));
+              atomicAdd(&W.gd[a * GD + 18 + 3 * i + j], static_cast<double>(G3[i][j]));
+              atomicAdd(&W.gd[b * GD + 18 + 3 * j + i], static_cast<double>(G3[i][j]));
             }
-            if (A.rhs && rr[i] != 0.0) atomicAdd(A.rhs + W.eq0[a] + ri, rr[i]);
           }
-        }
-        if (a != b) {
-          const int64_t col0 = sl[b * n + a];
-          for (int j = 0; j < 3; ++j) {
-            if (!((mb >> j) & 1)) continue;
-            const int rj = __popc(mb & ((1 << j) - 1));
-            double* row = A.vals + W.base[b] + static_cast<int64_t>(rj) * W.rowlen[b] + col0;
-            double rr = 0.0;
-            for (int i = 0; i < 3; ++i) {
-              if ((ma >> i) & 1) {
-                atomicAdd(row + __popc(ma & ((1 << i) - 1)), static_cast<double>(K[i][j]));
-              } else {
-                rr -= static_cast<double>(K[i][j]) * W.presc[3 * a + i];
-              }
-            }
-            if (A.rhs && rr != 0.0) atomicAdd(A.rhs + W.eq0[b] + rj, rr);
-          }
-        }
       }
+      double K[3][3];
+      combine(G1, G2, G3, plastic_elem, lam, mu_el, K);
+      if (ET == C3D8R) add_hourglass(W, a, b, K);
+      write_pair<n, DENSE>(A, W, e, a, b, K);
+    }
+    __syncwarp();
+    for (int a = lane; a < n; a += 32) {
+      double K[3][3];
+      if (DIAGFIX) {
+        double G1[3][3], G2[3][3], G3[3][3];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            G1[i][j] = -W.gd[a * GD + 3 * i + j];
+            G2[i][j] = plastic_elem ? -W.gd[a * GD + 9 + 3 * i + j] : 0.0;
+            G3[i][j] = plastic_elem ? -W.gd[a * GD + 18 + 3 * i + j] : 0.0;
+          }
+        combine(G1, G2, G3, plastic_elem, lam, mu_el, K);
+      } else {
+        R G1[3][3], G2[3][3], G3[3][3];
+        gram<n, nq, TAN>(W, a, a, plastic_elem, G1, G2, G3);
+        combine(G1, G2, G3, plastic_elem, lam, mu_el, K);
+      }
+      if (ET == C3D8R) add_hourglass(W, a, a, K);
+      write_pair<n, DENSE>(A, W, e, a, a, K);
     }
 
     // ---- phase D: internal force (material-point mode) -----------------------------
@@ -491,8 +583,8 @@ __global__ void __launch_bounds__(kThreads) element_kernel(ElemArgs A) {
           for (int al = 0; al < 4; ++al) {
             double gu[3] = {0, 0, 0};
             for (int j = 0; j < 8; ++j)
-              for (int d = 0; d < 3; ++d) gu[d] += static_cast<double>(W.gam[al * 8 + j]) * W.u[3 * j + d];
-            const double ka = static_cast<double>(W.kappa) * static_cast<double>(W.gam[al * 8 + a]);
+              for (int d = 0; d < 3; ++d) gu[d] += W.gam[al * 8 + j] * W.u[3 * j + d];
+            const double ka = W.kappa * W.gam[al * 8 + a];
             for (int d = 0; d < 3; ++d) f[d] += ka * gu[d];
           }
         }
@@ -510,8 +602,8 @@ __global__ void __launch_bounds__(kThreads) element_kernel(ElemArgs A) {
 template <int ET, int MODE, bool DENSE, typename R>
 cudaError_t launch_t(const ElemArgs& a, cudaStream_t s) {
   using WS = WarpSmem<ET, MODE, R>;
-  constexpr int n = nodes_of(ET), nq = gauss_of(ET), NP = n * (n + 1) / 2;
-  constexpr size_t cta_bytes = ((sizeof(double) * (n * 3 * nq + nq) + 2 * NP) + 15) / 16 * 16;
+  constexpr int n = nodes_of(ET), nq = gauss_of(ET), NPO = n * (n - 1) / 2;
+  constexpr size_t cta_bytes = ((sizeof(double) * (n * 3 * nq + nq) + 2 * NPO) + 15) / 16 * 16;
   constexpr size_t smem = cta_bytes + kWarps * ((sizeof(WS) + 15) / 16 * 16);
   auto kern = element_kernel<ET, MODE, DENSE, R>;
   static thread_local int configured_device = -1;

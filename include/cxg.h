@@ -148,6 +148,13 @@ CXG_API int cxg_plan_check(cxg_plan* plan, int64_t* bad_element);
 CXG_API int cxg_assemble_linear(cxg_plan* plan, double* vals, double* rhs, const double* f_ext,
                         void* stream);
 
+/* Flags of the _ex variants. CXG_ACCUMULATE adds this plan's element contributions
+ * to the values already in vals (and rhs, f_int) instead of overwriting them, e.g. to
+ * sum several meshes that share one DOF numbering and pattern; f_ext is then ignored. */
+#define CXG_ACCUMULATE 1
+CXG_API int cxg_assemble_linear_ex(cxg_plan* plan, double* vals, double* rhs, const double* f_ext,
+                                   int32_t flags, void* stream);
+
 /* Material-point tangent (assemble_material_tangent, src/fem/assembly.cpp:385-423):
  * u[3*n_nodes] full displacement; vals = consistent tangent K_ff; f_int[3*n_nodes] =
  * internal force; rhs = T^T f_ext - K_fc(tangent) u_c where u_c are the plan's

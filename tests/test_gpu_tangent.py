@@ -39,7 +39,7 @@ def test_tangent_increments(cuda, port, etype):
     committed = np.zeros(plan.n_gauss * 13)
     yielded = 0.0
     for k in range(1, 4):
-        u = displacement_field(model, 0.002 * k, seed=k)
+        u = displacement_field(model, 0.0006 * k, seed=k)
         vg, fg, rg = plan.assemble_tangent(u)
         rp, ci, v, rhs, fo, so = port.assemble_tangent(model.mesh, mats, em, dof_eq, pre, nf, u, committed)
         rpg, cig = (to_np(t) for t in plan.pattern())
