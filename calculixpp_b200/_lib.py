@@ -81,6 +81,8 @@ SIGNATURES = {
     "cxg_element_tangent_force": (C.c_int, [C.c_int32, C.c_int64, _vp, _vp, C.POINTER(CxgMaterial),
                                             _vp, _vp, C.c_int32, _vp, _vp, _vp]),
     "cxg_adjoint_compliance": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cxg_element_tangent_force_noalloc": (C.c_int, [C.c_int32, C.c_int64, _vp, _vp, C.POINTER(CxgMaterial),
+                                                    _vp, _vp, C.c_int32, _vp, _vp, _vp]),
 }
 
 _LIB = None

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -669,3 +670,112 @@ int cxg_adjoint_compliance(cxg_plan* p, const double* u, double* dc_dE, double* 
 }
 
 }  // extern "C"
+
+// ---- element_tangent_force without device allocation -------------------------------
+// The scratch of cxg_element_tangent_force (J2 history in the kernel's point-major
+// layout, per-element elastic constants, the material record and the error word)
+// lives in this file-scope device buffer instead of cudaMalloc'ed memory. Host code
+// never dereferences the symbol: its device address is looked up once per device
+// with cudaGetSymbolAddress and passed to the kernels.
+namespace {
+
+constexpr int64_t kNoallocPoints = CXG_NOALLOC_MAX_GAUSS_POINTS;
+constexpr size_t kNoallocStateBytes = sizeof(double) * kStateDoubles * kNoallocPoints;
+constexpr size_t kNoallocPropBytes = sizeof(double) * kNoallocPoints;
+constexpr size_t kNoallocMatOffset = 2 * kNoallocStateBytes + 2 * kNoallocPropBytes;
+constexpr size_t kNoallocStatusOffset = kNoallocMatOffset + ((sizeof(J2Mat) + 255) / 256) * 256;
+static_assert(kNoallocStatusOffset + sizeof(DevStatus) <= CXG_NOALLOC_SCRATCH_BYTES, "scratch layout");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CXG_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+__global__ void fill_pair_kernel(double* a, double va, double* b, double vb, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    a[i] = va;
+    b[i] = vb;
+  }
+}
+
+}  // namespace
+
+extern "C" int cxg_element_tangent_force_noalloc(int32_t t, int64_t n_elems, const double* coords, const double* ue,
+                                                 const cxg_material* material, const double* sc, double* st,
+                                                 int32_t precision, double* Ke, double* fe, void* stream) {
+  if (!supported(t)) return set_err(CXG_ERR_UNSUPPORTED, "unsupported element type");
+  if (n_elems < 0 || !coords || !ue || !material || !Ke || !fe)
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "coords, ue, material, Ke and fe are required");
+  if (precision != 0 && precision != 1) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad precision");
+  const int64_t G = n_elems * gauss_of(t);
+  if (G > kNoallocPoints)
+    return set_err(CXG_ERR_INVALID_ARGUMENT,
+                   "batch of " + std::to_string(G) + " Gauss points exceeds the no-allocation limit of " +
+                       std::to_string(kNoallocPoints) + " (CXG_NOALLOC_MAX_GAUSS_POINTS); split the batch");
+  const void* arrays[] = {coords, ue, Ke, fe, sc, st};
+  for (const void* ptr : arrays)
+    if (ptr && !on_device(ptr))
+      return set_err(CXG_ERR_INVALID_ARGUMENT, "every array argument must be device memory");
+  std::vector<J2Mat> mats;
+  bool plastic = false;
+  int rc = build_mats(1, material, mats, &plastic);
+  if (rc) return rc;
+  int dev = 0;
+  CHECK_CUDA(cudaGetDevice(&dev), "device");
+  if (dev < 0 || dev >= 64) return set_err(CXG_ERR_UNSUPPORTED, "device ordinal above 63");
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* addr = nullptr;
+      CHECK_CUDA(cudaGetSymbolAddress(&addr, g_noalloc_scratch), "scratch address");
+      g_noalloc_addr[dev] = addr;
+    }
+    base = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+  }
+  CHECK_CUDA(ensure_tables(), "constant tables");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* d_sc = reinterpret_cast<double*>(base);
+  double* d_st = reinterpret_cast<double*>(base + kNoallocStateBytes);
+  double* d_E = reinterpret_cast<double*>(base + 2 * kNoallocStateBytes);
+  double* d_nu = reinterpret_cast<double*>(base + 2 * kNoallocStateBytes + kNoallocPropBytes);
+  J2Mat* d_mat = reinterpret_cast<J2Mat*>(base + kNoallocMatOffset);
+  DevStatus* d_status = reinterpret_cast<DevStatus*>(base + kNoallocStatusOffset);
+  if (n_elems == 0) return CXG_OK;
+  const DevStatus clear{0, 0, ~0ull};
+  CHECK_CUDA(cudaMemcpyAsync(d_mat, mats.data(), sizeof(J2Mat), cudaMemcpyHostToDevice, s), "material");
+  CHECK_CUDA(cudaMemcpyAsync(d_status, &clear, sizeof clear, cudaMemcpyHostToDevice, s), "status");
+  const unsigned grid = static_cast<unsigned>(std::min<int64_t>((n_elems + 255) / 256, 1024));
+  fill_pair_kernel<<<grid, 256, 0, s>>>(d_E, material->E, d_nu, material->nu, n_elems);
+  CHECK_CUDA(cudaGetLastError(), "constants");
+  if (sc)
+    CHECK_CUDA(launch_state_transpose(sc, d_sc, G, true, s), "state in");
+  else
+    CHECK_CUDA(cudaMemsetAsync(d_sc, 0, sizeof(double) * kStateDoubles * G, s), "state in");
+  ElemArgs a{};
+  a.n_elems = n_elems;
+  a.elem_coords = coords;
+  a.u = ue;
+  a.young = d_E;
+  a.poisson = d_nu;
+  a.mats = d_mat;
+  a.state_c = d_sc;
+  a.state_t = d_st;
+  a.n_gauss = G;
+  a.Ke = Ke;
+  a.fe = fe;
+  a.status = d_status;
+  CHECK_CUDA(launch_element_kernel(t, MODE_TANGENT, true, precision, a, s), "element kernel");
+  if (st) CHECK_CUDA(launch_state_transpose(d_st, st, G, false, s), "state out");
+  DevStatus hs{};
+  CHECK_CUDA(cudaMemcpyAsync(&hs, d_status, sizeof hs, cudaMemcpyDeviceToHost, s), "status read");
+  CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
+  if (hs.code) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "non-positive element Jacobian (bad connectivity?) at element index %llu", hs.bad_elem);
+    return set_err(hs.code, buf);
+  }
+  return CXG_OK;
+}
+

@@ -182,6 +182,28 @@ CXG_API int cxg_element_tangent_force(int32_t elem_type, int64_t n_elems, const 
                               const double* state_committed, double* state_trial,
                               int32_t precision, double* Ke, double* fe, void* stream);
 
+/* ---- element_tangent_force for callers that cannot allocate device memory --------
+ * No counterpart in the reference. Same computation and argument meaning as
+ * cxg_element_tangent_force, but the library allocates nothing: code that runs inside
+ * another framework's memory pool, a real-time loop or a caller-managed arena may not
+ * call cudaMalloc/cudaFree (or any allocating routine). Every array argument must be a
+ * device pointer the caller owns; the material table is read from host memory.
+ * The J2 history staging, per-element constants and the error word live in one
+ * statically sized device buffer of this library (CXG_NOALLOC_SCRATCH_BYTES, held by
+ * every GPU that loads the library until the process exits), so one call handles at
+ * most CXG_NOALLOC_MAX_GAUSS_POINTS Gauss points (n_elems x points per element);
+ * larger batches are rejected with CXG_ERR_INVALID_ARGUMENT. All calls share that
+ * buffer: calls whose work overlaps on the GPU (different streams, or different host
+ * threads on one device) race with each other and must be serialised by the caller.
+ * The first call on each device looks up the buffer's device address; make that first
+ * call before any stream capture. The call synchronises `stream` before returning. */
+#define CXG_NOALLOC_MAX_GAUSS_POINTS 8192
+#define CXG_NOALLOC_SCRATCH_BYTES (2 * 13 * 8 * CXG_NOALLOC_MAX_GAUSS_POINTS + 2 * 8 * CXG_NOALLOC_MAX_GAUSS_POINTS + 4096)
+CXG_API int cxg_element_tangent_force_noalloc(int32_t elem_type, int64_t n_elems, const double* coords,
+                                              const double* ue, const cxg_material* material,
+                                              const double* state_committed, double* state_trial,
+                                              int32_t precision, double* Ke, double* fe, void* stream);
+
 /* ---- adjoint of the compliance c = f^T u for K u = f with load independent of the
  * design: dc/dE_e = -(1/E_e) u_e^T K_e u_e and dc/dX = -sum_e u_e^T dK_e/dX u_e,
  * evaluated in closed form per Gauss point. Full-integration families (C3D8, C3D20,
