@@ -37,6 +37,9 @@ struct cxg_plan {
   PatternOut pat;
   double* state[2] = {nullptr, nullptr};  // SoA [13][G]: committed, trial
   DevStatus* status = nullptr;
+  void* edata = nullptr;      // per-element K blocks of the two-pass assembly
+  size_t edata_bytes = 0;
+  double* fdata = nullptr;    // per-element internal force (material-point mode)
   cudaStream_t last_stream = nullptr;
   int64_t device_bytes = 0;
   // staging buffers for host pointers, grown on demand and reused
@@ -187,6 +190,37 @@ int ensure_state(cxg_plan* p, cudaStream_t s) {
   return CXG_OK;
 }
 
+int ensure_v2(cxg_plan* p, bool tangent) {
+  const size_t need = v2_edata_bytes(p->type, p->n_elems, p->precision);
+  if (p->edata_bytes < need) {
+    cudaFree(p->edata);
+    p->edata = nullptr;
+    p->device_bytes -= static_cast<int64_t>(p->edata_bytes);
+    p->edata_bytes = 0;
+    CHECK_CUDA(cudaMalloc(&p->edata, std::max<size_t>(need, 16)), "element buffer");
+    p->edata_bytes = need;
+    p->device_bytes += static_cast<int64_t>(need);
+  }
+  if (tangent && !p->fdata) {
+    const size_t fb = sizeof(double) * 3 * nodes_of(p->type) * static_cast<size_t>(std::max<int64_t>(p->n_elems, 1));
+    CHECK_CUDA(cudaMalloc(&p->fdata, fb), "force buffer");
+    p->device_bytes += static_cast<int64_t>(fb);
+  }
+  return CXG_OK;
+}
+
+V2Args v2_args(cxg_plan* p, const double* f_ext, bool accumulate) {
+  V2Args v{};
+  v.edata = p->edata;
+  v.fdata = p->fdata;
+  v.inc_ptr = p->pat.inc_ptr;
+  v.inc_code = p->pat.inc_code;
+  v.f_ext = f_ext;
+  v.max_row = p->pat.max_row;
+  v.accumulate = accumulate ? 1 : 0;
+  return v;
+}
+
 ElemArgs base_args(cxg_plan* p) {
   ElemArgs a{};
   a.n_elems = p->n_elems;
@@ -328,7 +362,8 @@ int cxg_plan_destroy(cxg_plan* p) {
   if (p->last_stream) cudaStreamSynchronize(p->last_stream);
   void* bufs[] = {p->coords, p->conn, p->young, p->poisson, p->elem_mat, p->mats, p->dof_eq, p->prescribed,
                   p->pat.row_ptr, p->pat.col_idx, p->pat.node_base, p->pat.node_rowlen, p->pat.node_mask,
-                  p->pat.node_eq0, p->pat.slot, p->state[0], p->state[1], p->status};
+                  p->pat.node_eq0, p->pat.slot, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
+                  p->status, p->edata, p->fdata};
   for (void* b : bufs) cudaFree(b);
   for (void* b : p->stage) cudaFree(b);
   delete p;
@@ -411,15 +446,12 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
   if (!rc) rc = staged(p, 1, rhs, rb, accumulate, s, &dr);
   if (!rc && !accumulate) rc = staged(p, 2, f_ext, fb, true, s, &df);
   if (rc) return rc;
-  if (!accumulate) {
-    CHECK_CUDA(cudaMemsetAsync(dv, 0, vb, s), "zero vals");
-    if (dr) CHECK_CUDA(launch_rhs_init(p->dof_eq, static_cast<const double*>(df), 3 * p->n_nodes,
-                                       static_cast<double*>(dr), s), "rhs init");
-  }
+  if ((rc = ensure_v2(p, false))) return rc;
   ElemArgs a = base_args(p);
   a.vals = static_cast<double*>(dv);
   a.rhs = static_cast<double*>(dr);
-  CHECK_CUDA(launch_element_kernel(p->type, MODE_LINEAR, false, p->precision, a, s), "element kernel");
+  CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, p->precision, a, v2_args(p, static_cast<const double*>(df), accumulate), s),
+             "assembly kernels");
   if ((rc = copy_out(vals, dv, vb, s))) return rc;
   if ((rc = copy_out(rhs, dr, rb, s))) return rc;
   if (dv != vals || (rhs && dr != rhs)) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
@@ -443,10 +475,7 @@ int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_i
   if (!rc) rc = staged(p, 3, u, fb, true, s, &du);
   if (!rc) rc = staged(p, 4, f_int, fb, false, s, &dfi);
   if (rc) return rc;
-  CHECK_CUDA(cudaMemsetAsync(dv, 0, vb, s), "zero vals");
-  if (dfi) CHECK_CUDA(cudaMemsetAsync(dfi, 0, fb, s), "zero f_int");
-  if (dr) CHECK_CUDA(launch_rhs_init(p->dof_eq, static_cast<const double*>(df), 3 * p->n_nodes,
-                                     static_cast<double*>(dr), s), "rhs init");
+  if ((rc = ensure_v2(p, true))) return rc;
   ElemArgs a = base_args(p);
   a.vals = static_cast<double*>(dv);
   a.rhs = static_cast<double*>(dr);
@@ -454,7 +483,8 @@ int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_i
   a.u = static_cast<const double*>(du);
   a.state_c = p->state[0];
   a.state_t = p->state[1];
-  CHECK_CUDA(launch_element_kernel(p->type, MODE_TANGENT, false, p->precision, a, s), "element kernel");
+  CHECK_CUDA(launch_v2(p->type, MODE_TANGENT, p->precision, a, v2_args(p, static_cast<const double*>(df), false), s),
+             "assembly kernels");
   if ((rc = copy_out(vals, dv, vb, s))) return rc;
   if ((rc = copy_out(rhs, dr, rb, s))) return rc;
   if ((rc = copy_out(f_int, dfi, fb, s))) return rc;

@@ -32,6 +32,18 @@ struct DevStatus {
 
 enum KernelMode : int { MODE_LINEAR = 0, MODE_TANGENT = 1 };
 
+// Constant tables (defined in cxg_kernels.cu, filled by ensure_tables): natural
+// derivatives dN[k][d][q] (Gauss point fastest) and weights of every family.
+constexpr int dn_size(int t) { return nodes_of(t) * 3 * gauss_of(t); }
+constexpr int dn_offset(int t) {
+  int off = 0;
+  for (int u = C3D8; u < t; ++u) off += dn_size(u);
+  return off;
+}
+constexpr int kDnTotal = dn_offset(C3D15) + dn_size(C3D15);
+extern __constant__ double c_dN[kDnTotal];
+extern __constant__ double c_w[8][kMaxGauss];
+
 // Everything an element-integration launch reads or writes. Pointers are device
 // pointers; optional ones may be null.
 struct ElemArgs {
@@ -67,6 +79,20 @@ struct ElemArgs {
   DevStatus* status;
 };
 
+// Extra arguments of the two-pass assembly (cxg_v2.cu).
+struct V2Args {
+  void* edata;              // per-element upper 3x3 blocks, FP32 (mixed) or FP64
+  double* fdata;            // per-element internal force [E*3n] (material-point mode)
+  const int64_t* inc_ptr;   // node -> incident elements
+  const int32_t* inc_code;
+  const double* f_ext;      // [3N] load vector for the rhs, or null
+  int64_t max_row;          // largest (free rows x row length) of any node
+  int64_t row_stride;       // set by the launcher
+  int accumulate;           // add into vals / rhs / f_int instead of overwriting
+};
+size_t v2_edata_bytes(int elem_type, int64_t n_elems, int precision);
+cudaError_t launch_v2(int elem_type, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s);
+
 // Launchers (cxg_kernels.cu). `precision` 0 = FP64, 1 = mixed.
 cudaError_t launch_element_kernel(int elem_type, int mode, bool dense, int precision,
                                   const ElemArgs& a, cudaStream_t s);
@@ -89,6 +115,10 @@ struct PatternOut {
   uint8_t* node_mask = nullptr;
   int32_t* node_eq0 = nullptr;
   uint16_t* slot = nullptr;     // [E*n*n]
+  // node -> incident elements, ascending element order: codes e*n + local node index
+  int64_t* inc_ptr = nullptr;   // [N+1]
+  int32_t* inc_code = nullptr;  // [E*n]
+  int64_t max_row = 0;          // max over nodes of (free rows) x (row length)
   int64_t device_bytes = 0;
 };
 // Returns a cxg_status code; on error *msg is set.

@@ -30,22 +30,14 @@
 
 namespace cxg {
 
+__constant__ double c_dN[kDnTotal];
+__constant__ double c_w[8][kMaxGauss];
+
 namespace {
 
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
 
-// Constant tables: natural derivatives dN[k][d][q] (q fastest) and weights per family.
-constexpr int dn_size(int t) { return nodes_of(t) * 3 * gauss_of(t); }
-constexpr int dn_offset(int t) {
-  int off = 0;
-  for (int u = C3D8; u < t; ++u) off += dn_size(u);
-  return off;
-}
-constexpr int kDnTotal = dn_offset(C3D15) + dn_size(C3D15);
-
-__constant__ double c_dN[kDnTotal];
-__constant__ double c_w[8][kMaxGauss];
 
 // sqrt(3/2) with the literal the reference uses (src/fem/plasticity.cpp:24), so the
 // yield-function value agrees with it bit for bit.

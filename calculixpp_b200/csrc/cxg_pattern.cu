@@ -167,6 +167,27 @@ __global__ void slot_kernel(const int32_t* conn, int64_t n_elems, int npe, uint6
   }
 }
 
+__global__ void iota_kernel(int32_t* v, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    v[i] = static_cast<int32_t>(i);
+}
+
+__global__ void inc_ptr_kernel(const int32_t* sorted_nodes, int64_t m, int64_t n_nodes, int64_t* ptr) {
+  for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a <= n_nodes;
+       a += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int64_t lo = 0, hi = m;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (sorted_nodes[mid] < a)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    ptr[a] = lo;
+  }
+}
+
 unsigned grid_for(int64_t n, int threads = 256) {
   return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 65536)));
 }
@@ -352,6 +373,46 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
     *msg = "a CSR row holds more than 65535 columns; not supported";
     rc = 5;
     goto done;
+  }
+
+  // largest per-node row block (free rows x row length): sizes the gather's buffers
+  {
+    int64_t* d_max = nullptr;
+    CXG_TRY(cudaMalloc(&d_max, sizeof(int64_t)));
+    temp_bytes = 0;
+    CXG_TRY(cub::DeviceReduce::Max(nullptr, temp_bytes, d_node_nnz, d_max, static_cast<int>(n_nodes), s));
+    CXG_TRY(cudaMalloc(&d_temp, temp_bytes));
+    CXG_TRY(cub::DeviceReduce::Max(d_temp, temp_bytes, d_node_nnz, d_max, static_cast<int>(n_nodes), s));
+    CXG_TRY(cudaMemcpyAsync(&out->max_row, d_max, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CXG_TRY(cudaStreamSynchronize(s));
+    cudaFree(d_max);
+    cudaFree(d_temp);
+    d_temp = nullptr;
+  }
+
+  // node -> element incidence: stable sort of (node, e*n + local) by node
+  {
+    const int64_t m = n_elems * npe;
+    int32_t *d_codes = nullptr, *d_nodes_sorted = nullptr;
+    CXG_TRY(dalloc(&out->inc_ptr, n_nodes + 1, &out->device_bytes));
+    CXG_TRY(dalloc(&out->inc_code, m, &out->device_bytes));
+    CXG_TRY(cudaMalloc(&d_codes, sizeof(int32_t) * std::max<int64_t>(m, 1)));
+    CXG_TRY(cudaMalloc(&d_nodes_sorted, sizeof(int32_t) * std::max<int64_t>(m, 1)));
+    iota_kernel<<<grid_for(m), 256, 0, s>>>(d_codes, m);
+    CXG_TRY(cudaGetLastError());
+    int node_bits = 1;
+    while (node_bits < 31 && (n_nodes >> node_bits) != 0) ++node_bits;
+    temp_bytes = 0;
+    CXG_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, d_conn, d_nodes_sorted, d_codes, out->inc_code,
+                                            static_cast<int>(m), 0, node_bits, s));
+    CXG_TRY(cudaMalloc(&d_temp, temp_bytes));
+    CXG_TRY(cub::DeviceRadixSort::SortPairs(d_temp, temp_bytes, d_conn, d_nodes_sorted, d_codes, out->inc_code,
+                                            static_cast<int>(m), 0, node_bits, s));
+    inc_ptr_kernel<<<grid_for(n_nodes + 1), 256, 0, s>>>(d_nodes_sorted, m, n_nodes, out->inc_ptr);
+    CXG_TRY(cudaGetLastError());
+    CXG_TRY(cudaStreamSynchronize(s));
+    cudaFree(d_codes);
+    cudaFree(d_nodes_sorted);
   }
 
 done:

@@ -1,0 +1,669 @@
+// Assembly in two passes, with no atomics and every CSR value written exactly once.
+//
+// P1 (element pass): each warp integrates EPW elements at once. Lanes first handle
+// (element, Gauss point) tasks: Jacobian, its inverse and the physical gradients in
+// FP64 (plus the J2 return in material-point mode, whose trial history is written
+// here, once per Gauss point). Then every lane owns a 2x4 tile of node pairs of one
+// element and accumulates the 8 corresponding 3x3 blocks of K_e in registers over the
+// Gauss points from float4/double4 gradient loads; elastic points use the Gram form
+// K_ab = lam G + mu (G^T + tr(G) I) with G = sum_q s_q g_a g_b^T, plastic elements the
+// full tangent sum_q s [lam* g_a g_b^T + mu* (g_b g_a^T + (g_a.g_b) I) - c m_a m_b^T]
+// (m = N g, N the return direction). The upper blocks (a <= b) go to a per-element
+// buffer, FP32 in mixed precision, FP64 otherwise; the internal force goes beside them.
+//
+// P2 (row gather): one warp per node. It walks the node's incident elements in
+// element order, adds their block rows into the node's CSR rows held in shared memory
+// (plain read-modify-write: within one element every target is distinct), moves
+// prescribed columns into the rhs (-K_fc u_c, src/fem/assembly.cpp:95-96), adds the
+// load vector, and stores its rows once with coalesced writes. In mixed precision the
+// diagonal block of each element row is formed here in FP64 as minus the sum of that
+// row's off-diagonal FP32 blocks, so rigid translations stay in the null space exactly.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "cxg_internal.cuh"
+
+namespace cxg {
+
+namespace {
+
+constexpr int kT1 = 128;          // P1 threads per block
+constexpr int kW1 = kT1 / 32;
+constexpr double kSqrt3_2v2 = 1.224744871391589;
+
+struct TileList {
+  int count;
+  unsigned char r[64];
+  unsigned char c[64];
+};
+
+constexpr TileList make_tiles(int n) {
+  TileList t{};
+  const int npad = (n + 3) / 4 * 4;
+  for (int r = 0; r < npad / 2; ++r)
+    for (int c = 0; c < npad / 4; ++c) {
+      bool any = false;
+      for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 4; ++j) {
+          const int a = 2 * r + i, b = 4 * c + j;
+          if (a < n && b < n && a <= b) any = true;
+        }
+      if (any) {
+        t.r[t.count] = static_cast<unsigned char>(r);
+        t.c[t.count] = static_cast<unsigned char>(c);
+        ++t.count;
+      }
+    }
+  return t;
+}
+
+template <int ET>
+struct Geo {
+  static constexpr int n = nodes_of(ET);
+  static constexpr int nq = gauss_of(ET);
+  static constexpr int npad = (n + 3) / 4 * 4;
+  static constexpr int NB = n * (n + 1) / 2;
+  static constexpr TileList tiles = make_tiles(n);
+  static constexpr int NT = tiles.count;
+  static constexpr int EPW = NT >= 32 ? 1 : 32 / NT;
+};
+
+__host__ __device__ constexpr int blk_index(int n, int a, int b) { return a * n - a * (a - 1) / 2 + (b - a); }
+
+__device__ __forceinline__ void hardening2(const J2Mat& M, double ep, double& sy, double& h) {
+  const int n = M.n;
+  if (n == 1 || ep <= M.ep[0]) {
+    sy = M.sy[0];
+    h = 0.0;
+    return;
+  }
+  if (ep >= M.ep[n - 1]) {
+    sy = M.sy[n - 1];
+    h = 0.0;
+    return;
+  }
+  for (int i = 0; i + 1 < n; ++i) {
+    if (ep >= M.ep[i] && ep <= M.ep[i + 1]) {
+      h = (M.sy[i + 1] - M.sy[i]) / (M.ep[i + 1] - M.ep[i]);
+      sy = M.sy[i] + h * (ep - M.ep[i]);
+      return;
+    }
+  }
+  sy = M.sy[n - 1];
+  h = 0.0;
+}
+
+// J2 radial return + consistent tangent (restating src/fem/plasticity.cpp:90-236), FP64.
+// Returns true on the plastic branch; lam_s/mu_s/c: tangent parameters, nv: direction.
+__device__ bool j2_point(const J2Mat& M, double lam, double mu_el, double mu, const double* eps, const double* cs,
+                         double* ts, double* sig, double& lam_t, double& mu_t, double& c_t, double* nv,
+                         double& mu_hg) {
+  const double lam2mu = lam + 2.0 * mu_el;
+  double el[6];
+  for (int i = 0; i < 6; ++i) el[i] = eps[i] - cs[i];
+  double st[6];
+  st[0] = lam2mu * el[0] + lam * el[1] + lam * el[2];
+  st[1] = lam * el[0] + lam2mu * el[1] + lam * el[2];
+  st[2] = lam * el[0] + lam * el[1] + lam2mu * el[2];
+  st[3] = mu_el * el[3];
+  st[4] = mu_el * el[4];
+  st[5] = mu_el * el[5];
+  const double p = (st[0] + st[1] + st[2]) / 3.0;
+  const double s_tr[6] = {st[0] - p, st[1] - p, st[2] - p, st[3], st[4], st[5]};
+  double xi[6];
+  for (int i = 0; i < 6; ++i) xi[i] = s_tr[i] - cs[7 + i];
+  const double xi_norm = sqrt(xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2] +
+                              2.0 * (xi[3] * xi[3] + xi[4] * xi[4] + xi[5] * xi[5]));
+  const double q_tr = kSqrt3_2v2 * xi_norm;
+  double sy0 = 0.0, h0 = 0.0;
+  if (M.plastic) hardening2(M, cs[6], sy0, h0);
+  if (!M.plastic || q_tr - sy0 <= 0.0 || xi_norm == 0.0) {
+    for (int i = 0; i < 6; ++i) sig[i] = st[i];
+    for (int i = 0; i < kStateDoubles; ++i) ts[i] = cs[i];
+    lam_t = lam;
+    mu_t = mu_el;
+    c_t = 0.0;
+    mu_hg = mu_el;
+    return false;
+  }
+  const double ep0 = cs[6];
+  double dgamma = 0.0;
+  for (int it = 0; it < 50; ++it) {
+    double sy, h_iso;
+    hardening2(M, ep0 + dgamma, sy, h_iso);
+    const double g = q_tr - 3.0 * mu * dgamma - M.h_kin * dgamma - sy;
+    const double dg = -(3.0 * mu + M.h_kin + h_iso);
+    const double step = -g / dg;
+    dgamma += step;
+    if (dgamma < 0.0) dgamma = 0.0;
+    if (fabs(step) <= 1e-14 * (1.0 + fabs(dgamma))) break;
+  }
+  for (int i = 0; i < 6; ++i) nv[i] = xi[i] / xi_norm;
+  const double dev_scale = 2.0 * mu * dgamma * kSqrt3_2v2;
+  const double alpha_scale = (2.0 / 3.0) * M.h_kin * dgamma * kSqrt3_2v2;
+  const double dep_scale = dgamma * kSqrt3_2v2;
+  for (int i = 0; i < 6; ++i) {
+    sig[i] = (s_tr[i] - dev_scale * nv[i]) + (i < 3 ? p : 0.0);
+    ts[i] = cs[i] + dep_scale * nv[i] * (i < 3 ? 1.0 : 2.0);
+    ts[7 + i] = cs[7 + i] + alpha_scale * nv[i];
+  }
+  ts[6] = ep0 + dgamma;
+  double sy, h_iso;
+  hardening2(M, ep0 + dgamma, sy, h_iso);
+  const double theta = 1.0 - (2.0 * mu * dgamma * kSqrt3_2v2) / xi_norm;
+  const double denom = 1.0 + (h_iso + M.h_kin) / (3.0 * mu);
+  const double theta_bar = 1.0 / denom - (1.0 - theta);
+  lam_t = lam + (2.0 / 3.0) * (1.0 - theta) * mu;
+  mu_t = mu_el - (1.0 - theta) * mu;
+  c_t = 2.0 * mu * theta_bar;
+  mu_hg = mu_t - c_t * nv[3] * nv[3];
+  return true;
+}
+
+__constant__ double c_hg2[4][8] = {
+    {1, 1, -1, -1, -1, -1, 1, 1},
+    {1, -1, -1, 1, -1, 1, 1, -1},
+    {1, -1, 1, -1, 1, -1, 1, -1},
+    {-1, 1, -1, 1, 1, -1, 1, -1},
+};
+
+template <typename R>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  using T = float4;
+};
+template <>
+struct Vec4<double> {
+  using T = double4;
+};
+
+template <typename R>
+__device__ __forceinline__ void ld3(const R* p, R& x, R& y, R& z) {
+  const typename Vec4<R>::T v = *reinterpret_cast<const typename Vec4<R>::T*>(p);
+  x = v.x;
+  y = v.y;
+  z = v.z;
+}
+
+template <int ET, int MODE, typename R>
+struct P1Smem {
+  using G = Geo<ET>;
+  static constexpr int n = G::n, nq = G::nq, npad = G::npad, EPW = G::EPW;
+  static constexpr bool T = MODE == MODE_TANGENT;
+  R g[EPW][nq][npad][4];
+  R m[T ? EPW : 1][T ? nq : 1][T ? npad : 1][4];
+  R s[EPW][nq];
+  R dp[T ? EPW : 1][T ? nq : 1][4];
+  double x[EPW][3 * n];
+  double u[T ? EPW : 1][T ? 3 * n : 1];
+  double sig[T ? EPW : 1][T ? nq : 1][6];
+  double lam[EPW], mu[EPW], mu_j2[EPW];
+  double gam[EPW][32];
+  double kappa[EPW];
+  double gc[EPW][3 * n];
+  double vol[EPW];
+  double mu_hg[EPW];
+  int plastic[EPW];
+};
+
+template <int ET, int MODE, typename R>
+__global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
+  using G = Geo<ET>;
+  constexpr int n = G::n, nq = G::nq, npad = G::npad, EPW = G::EPW, NT = G::NT, NB = G::NB;
+  constexpr bool TAN = MODE == MODE_TANGENT;
+  using WS = P1Smem<ET, MODE, R>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* sdN = reinterpret_cast<double*>(smem);  // [n][3][nq]
+  double* sw = sdN + n * 3 * nq;
+  constexpr size_t cta_bytes = (sizeof(double) * (n * 3 * nq + nq) + 15) / 16 * 16;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WS& W = *reinterpret_cast<WS*>(smem + cta_bytes + warp * ((sizeof(WS) + 15) / 16 * 16));
+  __shared__ unsigned char s_tr[64], s_tc[64];
+  for (int i = threadIdx.x; i < n * 3 * nq; i += blockDim.x) sdN[i] = c_dN[dn_offset(ET) + i];
+  for (int i = threadIdx.x; i < nq; i += blockDim.x) sw[i] = c_w[ET][i];
+  if (threadIdx.x == 0) {
+    constexpr TileList tl = make_tiles(n);
+    for (int i = 0; i < NT; ++i) {
+      s_tr[i] = tl.r[i];
+      s_tc[i] = tl.c[i];
+    }
+  }
+  // zero the padded gradient slots once; they are never written afterwards
+  for (int t = lane; t < EPW * nq * npad * 4; t += 32) {
+    (&W.g[0][0][0][0])[t] = R(0);
+    if (TAN) (&W.m[0][0][0][0])[t % (sizeof(W.m) / sizeof(R))] = R(0);
+  }
+  __syncthreads();
+
+  const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * kW1 + warp;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kW1;
+  for (int64_t e0 = gwarp * EPW; e0 < A.n_elems; e0 += nwarps * EPW) {
+    // ---- phase A ---------------------------------------------------------------
+    for (int t = lane; t < EPW * n; t += 32) {
+      const int ei = t / n, k = t % n;
+      const int64_t e = e0 + ei;
+      if (e < A.n_elems) {
+        const int node = A.conn[e * n + k];
+        for (int d = 0; d < 3; ++d) {
+          W.x[ei][3 * k + d] = A.coords[3 * static_cast<int64_t>(node) + d];
+          if (TAN) W.u[ei][3 * k + d] = A.u[3 * static_cast<int64_t>(node) + d];
+        }
+      }
+    }
+    if (lane < EPW) {
+      const int64_t e = e0 + lane;
+      const double E = e < A.n_elems ? A.young[e] : 1.0, nu = e < A.n_elems ? A.poisson[e] : 0.0;
+      const double um2 = E / (1.0 + nu);
+      W.lam[lane] = nu * um2 / (1.0 - 2.0 * nu);
+      W.mu[lane] = um2 / 2.0;
+      W.mu_j2[lane] = E / (2.0 * (1.0 + nu));
+      W.plastic[lane] = 0;
+    }
+    __syncwarp();
+    // ---- phase B: (element, Gauss point) tasks ----------------------------------------
+    for (int t = lane; t < EPW * nq; t += 32) {
+      const int ei = t / nq, q = t % nq;
+      const int64_t e = e0 + ei;
+      if (e >= A.n_elems) continue;
+      double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int k = 0; k < n; ++k) {
+        const double d0 = sdN[(3 * k) * nq + q], d1 = sdN[(3 * k + 1) * nq + q], d2 = sdN[(3 * k + 2) * nq + q];
+        for (int i = 0; i < 3; ++i) {
+          const double xk = W.x[ei][3 * k + i];
+          J[i][0] = fma(xk, d0, J[i][0]);
+          J[i][1] = fma(xk, d1, J[i][1]);
+          J[i][2] = fma(xk, d2, J[i][2]);
+        }
+      }
+      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+      const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+      const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+      const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      if (!(det > 0.0)) {
+        atomicCAS(&A.status->code, 0, 4);
+        atomicMin(&A.status->bad_elem, static_cast<unsigned long long>(e));
+      }
+      const double inv = 1.0 / det;
+      const double it[3][3] = {
+          {c00 * inv, c01 * inv, c02 * inv},
+          {(J[0][2] * J[2][1] - J[0][1] * J[2][2]) * inv, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * inv,
+           (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * inv},
+          {(J[0][1] * J[1][2] - J[0][2] * J[1][1]) * inv, (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * inv,
+           (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * inv}};
+      const double sq = det * sw[q];
+      W.s[ei][q] = static_cast<R>(sq);
+      if (ET == C3D8R) W.vol[ei] = sq;
+      double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int k = 0; k < n; ++k) {
+        const double d0 = sdN[(3 * k) * nq + q], d1 = sdN[(3 * k + 1) * nq + q], d2 = sdN[(3 * k + 2) * nq + q];
+        double gk[3];
+        for (int i = 0; i < 3; ++i) {
+          gk[i] = it[i][0] * d0 + it[i][1] * d1 + it[i][2] * d2;
+          W.g[ei][q][k][i] = static_cast<R>(gk[i]);
+          if (ET == C3D8R) W.gc[ei][i * n + k] = gk[i];
+        }
+        if (TAN)
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) H[i][j] = fma(W.u[ei][3 * k + i], gk[j], H[i][j]);
+      }
+      if (TAN) {
+        const double eps[6] = {H[0][0], H[1][1], H[2][2], H[0][1] + H[1][0], H[0][2] + H[2][0], H[1][2] + H[2][1]};
+        const int mat = A.elem_mat ? A.elem_mat[e] : 0;
+        const int64_t gidx = e * nq + q;
+        double cs[kStateDoubles], ts[kStateDoubles], sig[6], nv[6] = {0, 0, 0, 0, 0, 0};
+        for (int c = 0; c < kStateDoubles; ++c) cs[c] = A.state_c[c * A.n_gauss + gidx];
+        double lt, mt, ct, mhg;
+        const bool pl = j2_point(A.mats[mat], W.lam[ei], W.mu[ei], W.mu_j2[ei], eps, cs, ts, sig, lt, mt, ct, nv, mhg);
+        for (int c = 0; c < kStateDoubles; ++c) A.state_t[c * A.n_gauss + gidx] = ts[c];
+        for (int c = 0; c < 6; ++c) W.sig[ei][q][c] = sq * sig[c];
+        W.dp[ei][q][0] = static_cast<R>(sq * lt);
+        W.dp[ei][q][1] = static_cast<R>(sq * mt);
+        W.dp[ei][q][2] = static_cast<R>(sq * ct);
+        if (pl) {
+          W.plastic[ei] = 1;
+          for (int k = 0; k < n; ++k) {
+            const double gx = W.g[ei][q][k][0], gy = W.g[ei][q][k][1], gz = W.g[ei][q][k][2];
+            W.m[ei][q][k][0] = static_cast<R>(nv[0] * gx + nv[3] * gy + nv[4] * gz);
+            W.m[ei][q][k][1] = static_cast<R>(nv[3] * gx + nv[1] * gy + nv[5] * gz);
+            W.m[ei][q][k][2] = static_cast<R>(nv[4] * gx + nv[5] * gy + nv[2] * gz);
+          }
+        }
+        if (q == nq - 1) W.mu_hg[ei] = mhg;
+      }
+    }
+    __syncwarp();
+    // ---- C3D8R hourglass vectors (src/fem/element.cpp:545-579) ------------------------
+    if (ET == C3D8R) {
+      for (int t = lane; t < EPW * 4; t += 32) {
+        const int ei = t / 4, al = t % 4;
+        double gx[3] = {0, 0, 0};
+        for (int j = 0; j < 8; ++j)
+          for (int d = 0; d < 3; ++d) gx[d] += c_hg2[al][j] * W.x[ei][3 * j + d];
+        for (int j = 0; j < 8; ++j) {
+          double corr = 0.0;
+          for (int d = 0; d < 3; ++d) corr += gx[d] * W.gc[ei][d * n + j];
+          W.gam[ei][al * 8 + j] = c_hg2[al][j] - corr;
+        }
+      }
+      if (lane < EPW) {
+        double b2 = 0.0;
+        for (int t = 0; t < 3 * n; ++t) b2 += W.gc[lane][t] * W.gc[lane][t];
+        W.kappa[lane] = 0.05 * (TAN ? W.mu_hg[lane] : W.mu_j2[lane]) * W.vol[lane] * b2;
+      }
+      __syncwarp();
+    }
+    // ---- phase C: 2x4 node-pair tiles -------------------------------------------------
+    if (lane < EPW * NT) {
+      const int ei = lane / NT, ti = lane % NT;
+      const int64_t e = e0 + ei;
+      if (e < A.n_elems) {
+        const int a0 = 2 * s_tr[ti], b0 = 4 * s_tc[ti];
+        R acc[2][4][9];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) acc[i][j][k] = R(0);
+        const bool pl = TAN && W.plastic[ei];
+        if (!pl) {
+#pragma unroll 3
+          for (int q = 0; q < nq; ++q) {
+            const R s = W.s[ei][q];
+            R ga[2][3], gb[4][3];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              ld3(&W.g[ei][q][a0 + i][0], ga[i][0], ga[i][1], ga[i][2]);
+              ga[i][0] *= s;
+              ga[i][1] *= s;
+              ga[i][2] *= s;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ld3(&W.g[ei][q][b0 + j][0], gb[j][0], gb[j][1], gb[j][2]);
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+              for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int x = 0; x < 3; ++x)
+#pragma unroll
+                  for (int y = 0; y < 3; ++y) acc[i][j][3 * x + y] += ga[i][x] * gb[j][y];
+          }
+          const R lam = static_cast<R>(W.lam[ei]), mu = static_cast<R>(W.mu[ei]);
+#pragma unroll
+          for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              R Gm[9];
+#pragma unroll
+              for (int k = 0; k < 9; ++k) Gm[k] = acc[i][j][k];
+              const R tr = Gm[0] + Gm[4] + Gm[8];
+#pragma unroll
+              for (int x = 0; x < 3; ++x)
+#pragma unroll
+                for (int y = 0; y < 3; ++y)
+                  acc[i][j][3 * x + y] = lam * Gm[3 * x + y] + mu * Gm[3 * y + x] + (x == y ? mu * tr : R(0));
+            }
+        } else if (TAN) {
+          for (int q = 0; q < nq; ++q) {
+            const R sl = W.dp[ei][q][0], sm = W.dp[ei][q][1], sc = W.dp[ei][q][2];
+            R ga[2][3], gb[4][3];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) ld3(&W.g[ei][q][a0 + i][0], ga[i][0], ga[i][1], ga[i][2]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ld3(&W.g[ei][q][b0 + j][0], gb[j][0], gb[j][1], gb[j][2]);
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                const R dot = sm * (ga[i][0] * gb[j][0] + ga[i][1] * gb[j][1] + ga[i][2] * gb[j][2]);
+#pragma unroll
+                for (int x = 0; x < 3; ++x)
+#pragma unroll
+                  for (int y = 0; y < 3; ++y)
+                    acc[i][j][3 * x + y] += (sl * ga[i][x]) * gb[j][y] + (sm * gb[j][x]) * ga[i][y] + (x == y ? dot : R(0));
+              }
+            if (sc != R(0)) {
+              R ma[2][3], mb[4][3];
+#pragma unroll
+              for (int i = 0; i < 2; ++i) ld3(&W.m[ei][q][a0 + i][0], ma[i][0], ma[i][1], ma[i][2]);
+#pragma unroll
+              for (int j = 0; j < 4; ++j) ld3(&W.m[ei][q][b0 + j][0], mb[j][0], mb[j][1], mb[j][2]);
+#pragma unroll
+              for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                  for (int x = 0; x < 3; ++x)
+#pragma unroll
+                    for (int y = 0; y < 3; ++y) acc[i][j][3 * x + y] -= (sc * ma[i][x]) * mb[j][y];
+            }
+          }
+        }
+        R* out = reinterpret_cast<R*>(V.edata) + e * (NB * 9);
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int a = a0 + i, b = b0 + j;
+            if (a < n && b < n && a <= b) {
+              R h = R(0);
+              if (ET == C3D8R) {
+                double hd = 0.0;
+                for (int al = 0; al < 4; ++al) hd += W.gam[ei][al * 8 + a] * W.gam[ei][al * 8 + b];
+                h = static_cast<R>(hd * W.kappa[ei]);
+              }
+              R* blk = out + blk_index(n, a, b) * 9;
+#pragma unroll
+              for (int k = 0; k < 9; ++k) blk[k] = acc[i][j][k] + ((k % 4 == 0) ? h : R(0));
+            }
+          }
+      }
+    }
+    // ---- phase D: internal force per element (material-point mode) --------------------
+    if (TAN) {
+      for (int t = lane; t < EPW * n; t += 32) {
+        const int ei = t / n, a = t % n;
+        const int64_t e = e0 + ei;
+        if (e >= A.n_elems) continue;
+        double f[3] = {0, 0, 0};
+        for (int q = 0; q < nq; ++q) {
+          const double* S = W.sig[ei][q];
+          const double gx = W.g[ei][q][a][0], gy = W.g[ei][q][a][1], gz = W.g[ei][q][a][2];
+          f[0] += S[0] * gx + S[3] * gy + S[4] * gz;
+          f[1] += S[3] * gx + S[1] * gy + S[5] * gz;
+          f[2] += S[4] * gx + S[5] * gy + S[2] * gz;
+        }
+        if (ET == C3D8R) {
+          for (int al = 0; al < 4; ++al) {
+            double gu[3] = {0, 0, 0};
+            for (int j = 0; j < 8; ++j)
+              for (int d = 0; d < 3; ++d) gu[d] += W.gam[ei][al * 8 + j] * W.u[ei][3 * j + d];
+            const double ka = W.kappa[ei] * W.gam[ei][al * 8 + a];
+            for (int d = 0; d < 3; ++d) f[d] += ka * gu[d];
+          }
+        }
+        for (int d = 0; d < 3; ++d) V.fdata[e * (3 * n) + 3 * a + d] = f[d];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---- P2: row gather ------------------------------------------------------------------
+template <int ET, bool TAN, typename R, bool DIAGFIX>
+__global__ void p2_kernel(ElemArgs A, V2Args V) {
+  using G = Geo<ET>;
+  constexpr int n = G::n, NB = G::NB;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* buf = reinterpret_cast<double*>(smem) + static_cast<int64_t>(warp) * V.row_stride;
+  const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  const R* ed = reinterpret_cast<const R*>(V.edata);
+  const int ij = lane % 9, grp = lane / 9;
+  const int i = ij / 3, j = ij % 3;
+  for (int64_t a = gwarp; a < A.n_nodes; a += nwarps) {
+    const int ma = A.node_mask[a];
+    const int nf = __popc(ma);
+    const int64_t L = A.node_rowlen[a];
+    const int64_t total = nf * L;
+    const int64_t base = A.node_base[a];
+    if (V.accumulate) {
+      for (int64_t t = lane; t < total; t += 32) buf[t] = A.vals[base + t];
+    } else {
+      for (int64_t t = lane; t < total; t += 32) buf[t] = 0.0;
+    }
+    __syncwarp();
+    const bool fi = (ma >> i) & 1;
+    const int ri = __popc(ma & ((1 << i) - 1));
+    double rr = 0.0;    // rhs contribution of row (a, i), spread over 9 lanes
+    double fsum = 0.0;  // internal force component (lanes 27..29)
+    const int64_t i0 = V.inc_ptr[a], i1 = V.inc_ptr[a + 1];
+    for (int64_t inc = i0; inc < i1; ++inc) {
+      const int code = V.inc_code[inc];
+      const int64_t e = code / n;
+      const int la = code % n;
+      const R* eblk = ed + e * (NB * 9);
+      const unsigned short* sl = A.slot + e * n * n + la * n;
+      const int32_t* cn = A.conn + e * n;
+      if (lane < 27) {
+        double dsum = 0.0;
+        for (int lb = grp; lb < n; lb += 3) {
+          if (DIAGFIX && lb == la) continue;
+          const double v = lb >= la ? static_cast<double>(eblk[blk_index(n, la, lb) * 9 + ij])
+                                    : static_cast<double>(eblk[blk_index(n, lb, la) * 9 + 3 * j + i]);
+          if (DIAGFIX) dsum += v;
+          if (!fi) continue;
+          const int nb = cn[lb];
+          const int mb = A.node_mask[nb];
+          if ((mb >> j) & 1) {
+            buf[ri * L + sl[lb] + __popc(mb & ((1 << j) - 1))] += v;
+          } else {
+            const double pv = A.prescribed[3 * static_cast<int64_t>(nb) + j];
+            if (pv != 0.0) rr -= v * pv;
+          }
+        }
+        if (DIAGFIX) {
+          const double d1 = __shfl_down_sync(0x07ffffffu, dsum, 9);
+          const double d2 = __shfl_down_sync(0x07ffffffu, dsum, 18);
+          if (lane < 9 && fi) {
+            const double diag = -(dsum + d1 + d2);
+            if ((ma >> j) & 1)
+              buf[ri * L + sl[la] + __popc(ma & ((1 << j) - 1))] += diag;
+            else {
+              const double pv = A.prescribed[3 * a + j];
+              if (pv != 0.0) rr -= diag * pv;
+            }
+          }
+        }
+      } else if (TAN && lane < 30) {
+        fsum += V.fdata[e * (3 * n) + 3 * la + (lane - 27)];
+      }
+      __syncwarp();
+    }
+    // rhs: sum the 9 lanes of each row i and add the load vector
+    if (A.rhs) {
+      for (int r = 0; r < 3; ++r) {
+        double v = (lane < 27 && i == r) ? rr : 0.0;
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0 && ((ma >> r) & 1)) {
+          const int64_t eq = A.node_eq0[a] + __popc(ma & ((1 << r) - 1));
+          const double prev = V.accumulate ? A.rhs[eq] : (V.f_ext ? V.f_ext[3 * a + r] : 0.0);
+          A.rhs[eq] = prev + v;
+        }
+      }
+    }
+    if (TAN && A.f_int && lane >= 27 && lane < 30) {
+      const int64_t gi = 3 * a + (lane - 27);
+      A.f_int[gi] = (V.accumulate ? A.f_int[gi] : 0.0) + fsum;
+    }
+    for (int64_t t = lane; t < total; t += 32) A.vals[base + t] = buf[t];
+    __syncwarp();
+  }
+}
+
+int sm_count() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+template <int ET, int MODE, typename R>
+cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, cudaStream_t s) {
+  using WS = P1Smem<ET, MODE, R>;
+  constexpr int n = nodes_of(ET), nq = gauss_of(ET);
+  constexpr size_t cta_bytes = (sizeof(double) * (n * 3 * nq + nq) + 15) / 16 * 16;
+  constexpr size_t smem = cta_bytes + kW1 * ((sizeof(WS) + 15) / 16 * 16);
+  auto kern = p1_kernel<ET, MODE, R>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  int per_sm = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT1, smem);
+  if (err != cudaSuccess) return err;
+  constexpr int EPW = Geo<ET>::EPW;
+  const int64_t need = (a.n_elems + kW1 * EPW - 1) / (kW1 * EPW);
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, static_cast<int64_t>(std::max(per_sm, 1)) * sm_count()));
+  if (a.n_elems == 0) return cudaSuccess;
+  kern<<<static_cast<unsigned>(grid), kT1, smem, s>>>(a, v);
+  return cudaGetLastError();
+}
+
+template <int ET, bool TAN, typename R, bool DF>
+cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, cudaStream_t s) {
+  auto kern = p2_kernel<ET, TAN, R, DF>;
+  // warps per block: as many as fit in ~160 KB of row buffers, up to 8
+  const int64_t stride = std::max<int64_t>(1, (v.max_row + 1) / 2 * 2);
+  int warps = 8;
+  while (warps > 1 && warps * stride * 8 > 160 * 1024) warps /= 2;
+  const size_t smem = static_cast<size_t>(warps) * stride * 8;
+  if (smem > 220 * 1024) return cudaErrorInvalidConfiguration;
+  v.row_stride = stride;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  int per_sm = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
+  if (err != cudaSuccess) return err;
+  const int64_t need = (a.n_nodes + warps - 1) / warps;
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, static_cast<int64_t>(std::max(per_sm, 1)) * sm_count()));
+  kern<<<static_cast<unsigned>(grid), warps * 32, smem, s>>>(a, v);
+  return cudaGetLastError();
+}
+
+template <int ET>
+cudaError_t launch_v2_type(int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s) {
+  cudaError_t err;
+  if (mode == MODE_LINEAR) {
+    err = precision ? launch_p1_t<ET, MODE_LINEAR, float>(a, v, s) : launch_p1_t<ET, MODE_LINEAR, double>(a, v, s);
+    if (err != cudaSuccess) return err;
+    return precision ? launch_p2_t<ET, false, float, true>(a, v, s) : launch_p2_t<ET, false, double, false>(a, v, s);
+  }
+  err = precision ? launch_p1_t<ET, MODE_TANGENT, float>(a, v, s) : launch_p1_t<ET, MODE_TANGENT, double>(a, v, s);
+  if (err != cudaSuccess) return err;
+  return precision ? launch_p2_t<ET, true, float, true>(a, v, s) : launch_p2_t<ET, true, double, false>(a, v, s);
+}
+
+}  // namespace
+
+size_t v2_edata_bytes(int t, int64_t n_elems, int precision) {
+  const int n = nodes_of(t);
+  return static_cast<size_t>(n_elems) * (n * (n + 1) / 2) * 9 * (precision ? 4 : 8);
+}
+
+cudaError_t launch_v2(int t, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s) {
+  switch (t) {
+    case C3D8: return launch_v2_type<C3D8>(mode, precision, a, v, s);
+    case C3D8R: return launch_v2_type<C3D8R>(mode, precision, a, v, s);
+    case C3D20: return launch_v2_type<C3D20>(mode, precision, a, v, s);
+    case C3D20R: return launch_v2_type<C3D20R>(mode, precision, a, v, s);
+    case C3D6: return launch_v2_type<C3D6>(mode, precision, a, v, s);
+    case C3D15: return launch_v2_type<C3D15>(mode, precision, a, v, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace cxg
