@@ -19,6 +19,7 @@ CXG_ERR_NEGATIVE_JACOBIAN = 4
 CXG_ERR_UNSUPPORTED = 5
 CXG_ERR_UNKNOWN_NODE = 6
 CXG_ERR_NO_GPU = 7
+CXG_ERR_NOT_CONVERGED = 8
 
 FP64, MIXED = 0, 1
 COMMITTED, TRIAL = 0, 1
@@ -81,6 +82,9 @@ SIGNATURES = {
     "cxg_element_tangent_force": (C.c_int, [C.c_int32, C.c_int64, _vp, _vp, C.POINTER(CxgMaterial),
                                             _vp, _vp, C.c_int32, _vp, _vp, _vp]),
     "cxg_adjoint_compliance": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cxg_spmv": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cxg_solve_cg": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_int32, C.POINTER(C.c_int32),
+                               C.POINTER(C.c_double), _vp]),
     "cxg_element_tangent_force_noalloc": (C.c_int, [C.c_int32, C.c_int64, _vp, _vp, C.POINTER(CxgMaterial),
                                                     _vp, _vp, C.c_int32, _vp, _vp, _vp]),
 }

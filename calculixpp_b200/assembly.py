@@ -234,6 +234,45 @@ class Plan:
         with torch.cuda.device(self.device):
             _lib.check(self.lib.cxg_state_commit(self.h, _stream()))
 
+    # -- reduced-system products, solve and adjoint ------------------------------------------
+    def spmv(self, vals, x):
+        y = torch.empty(self.n_free, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_spmv(self.h, _ptr(vals), _ptr(_dev(x, torch.float64, self.device)), _ptr(y),
+                                         _stream()))
+        return y
+
+    def solve_cg(self, vals, rhs, x=None, rtol=1e-10, max_iter=20000):
+        """K_ff x = rhs by Jacobi-preconditioned CG on the device (cxg_solve_cg)."""
+        x = torch.zeros(self.n_free, dtype=torch.float64, device=self.device) if x is None else x
+        it = C.c_int32()
+        rel = C.c_double()
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_solve_cg(self.h, _ptr(vals), _ptr(_dev(rhs, torch.float64, self.device)), _ptr(x),
+                                             float(rtol), int(max_iter), C.byref(it), C.byref(rel), _stream()))
+        return x, int(it.value), float(rel.value)
+
+    def expand(self, x):
+        """Full nodal displacement [3N] from the free solution: free DOFs from x, SPC
+        DOFs at their prescribed value (linear_static.cpp:42-47 for SPC-only models)."""
+        if not hasattr(self, "_free_idx"):
+            self._free_idx = torch.as_tensor(np.nonzero(self.dof_eq >= 0)[0], device=self.device)
+            self._pre = torch.as_tensor(self.prescribed, device=self.device)
+        u = self._pre.clone()
+        u[self._free_idx] = x
+        return u
+
+    def adjoint_compliance(self, u):
+        """(dc/dE per element, dc/dX per node (N,3)) for c = f^T u (cxg_adjoint_compliance)."""
+        m = self.model.mesh
+        dE = torch.empty(m.n_elems, dtype=torch.float64, device=self.device)
+        dX = torch.empty(3 * m.n_nodes, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_adjoint_compliance(self.h, _ptr(_dev(u, torch.float64, self.device)), _ptr(dE),
+                                                       _ptr(dX), _stream()))
+            self.check()
+        return dE, dX.view(-1, 3)
+
     def update_coords(self, coords):
         c = _dev(coords, torch.float64, self.device)
         _lib.check(self.lib.cxg_plan_update_coords(self.h, _ptr(c)))

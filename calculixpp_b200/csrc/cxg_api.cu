@@ -691,12 +691,82 @@ int cxg_element_tangent_force(int32_t t, int64_t n_elems, const double* coords, 
 }
 
 int cxg_adjoint_compliance(cxg_plan* p, const double* u, double* dc_dE, double* dc_dX, void* stream) {
-  (void)p;
-  (void)u;
-  (void)dc_dE;
-  (void)dc_dX;
-  (void)stream;
-  return set_err(CXG_ERR_UNSUPPORTED, "adjoint not built yet");
+  if (!p || !u) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan and u are required");
+  if (p->type == C3D8R)
+    return set_err(CXG_ERR_UNSUPPORTED, "compliance adjoint of the hourglass-stabilised C3D8R is not provided");
+  if (p->has_plastic) return set_err(CXG_ERR_UNSUPPORTED, "compliance adjoint is for linear elasticity");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  const size_t ub = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
+  const size_t eb = sizeof(double) * static_cast<size_t>(p->n_elems);
+  void *du, *dE, *dX;
+  int rc = staged(p, 3, u, ub, true, s, &du);
+  if (!rc) rc = staged(p, 1, dc_dE, eb, false, s, &dE);
+  if (!rc) rc = staged(p, 4, dc_dX, ub, false, s, &dX);
+  if (rc) return rc;
+  if (dX) CHECK_CUDA(cudaMemsetAsync(dX, 0, ub, s), "zero dc_dX");
+  ElemArgs a = base_args(p);
+  a.u = static_cast<const double*>(du);
+  CHECK_CUDA(launch_adjoint(p->type, a, static_cast<double*>(dE), static_cast<double*>(dX), s), "adjoint kernel");
+  if ((rc = copy_out(dc_dE, dE, eb, s))) return rc;
+  if ((rc = copy_out(dc_dX, dX, ub, s))) return rc;
+  if ((dc_dE && dE != dc_dE) || (dc_dX && dX != dc_dX)) CHECK_CUDA(cudaStreamSynchronize(s), "sync");
+  return CXG_OK;
+}
+
+int cxg_spmv(cxg_plan* p, const double* vals, const double* x, double* y, void* stream) {
+  if (!p || !vals || !x || !y) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, vals, x, y are required");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
+  const size_t nb = sizeof(double) * static_cast<size_t>(p->n_free);
+  void *dv, *dx, *dy;
+  int rc = staged(p, 0, vals, vb, true, s, &dv);
+  if (!rc) rc = staged(p, 2, x, nb, true, s, &dx);
+  if (!rc) rc = staged(p, 1, y, nb, false, s, &dy);
+  if (rc) return rc;
+  CHECK_CUDA(launch_spmv(p->n_free, p->pat.row_ptr, p->pat.col_idx, static_cast<const double*>(dv),
+                         static_cast<const double*>(dx), static_cast<double*>(dy), s), "spmv");
+  if ((rc = copy_out(y, dy, nb, s))) return rc;
+  if (dy != y) CHECK_CUDA(cudaStreamSynchronize(s), "sync");
+  return CXG_OK;
+}
+
+int cxg_solve_cg(cxg_plan* p, const double* vals, const double* rhs, double* x, double rtol, int32_t max_iter,
+                 int32_t* iterations, double* rel_residual, void* stream) {
+  if (!p || !vals || !rhs || !x || max_iter < 0) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
+  const size_t nb = sizeof(double) * static_cast<size_t>(p->n_free);
+  void *dv, *db, *dx;
+  int rc = staged(p, 0, vals, vb, true, s, &dv);
+  if (!rc) rc = staged(p, 1, rhs, nb, true, s, &db);
+  if (!rc) rc = staged(p, 2, x, nb, true, s, &dx);
+  if (rc) return rc;
+  const size_t wb = sizeof(double) * (5 * static_cast<size_t>(p->n_free) + 2056);
+  if (p->stage_bytes[5] < wb) {
+    cudaFree(p->stage[5]);
+    p->stage[5] = nullptr;
+    p->stage_bytes[5] = 0;
+    CHECK_CUDA(cudaMalloc(&p->stage[5], wb), "solver work");
+    p->stage_bytes[5] = wb;
+  }
+  int it = 0;
+  double rel = 0.0;
+  CHECK_CUDA(cg_solve(p->n_free, p->pat.row_ptr, p->pat.col_idx, static_cast<const double*>(dv),
+                      static_cast<const double*>(db), static_cast<double*>(dx), rtol, max_iter,
+                      static_cast<double*>(p->stage[5]), &it, &rel, s), "cg");
+  if ((rc = copy_out(x, dx, nb, s))) return rc;
+  CHECK_CUDA(cudaStreamSynchronize(s), "sync");
+  if (iterations) *iterations = it;
+  if (rel_residual) *rel_residual = rel;
+  if (!(rel <= rtol)) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "CG did not converge (relative residual %.3e after %d iterations)", rel, it);
+    return set_err(CXG_ERR_NOT_CONVERGED, buf);
+  }
+  return CXG_OK;
 }
 
 }  // extern "C"

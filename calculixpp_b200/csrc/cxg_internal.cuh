@@ -102,6 +102,11 @@ cudaError_t launch_state_transpose(const double* src, double* dst, int64_t G, bo
                                    cudaStream_t s);
 cudaError_t launch_adjoint(int elem_type, const ElemArgs& a, double* dc_dE, double* dc_dX,
                            cudaStream_t s);
+cudaError_t launch_spmv(int32_t nrows, const int64_t* rp, const int32_t* ci, const double* v, const double* x,
+                        double* y, cudaStream_t s);
+// Jacobi-preconditioned CG on CSR; work holds 5*n + 2056 doubles.
+cudaError_t cg_solve(int32_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* b, double* x,
+                     double rtol, int max_iter, double* work, int* iters_out, double* rel_out, cudaStream_t s);
 // Element tables (constant memory) are uploaded once per device.
 cudaError_t ensure_tables();
 

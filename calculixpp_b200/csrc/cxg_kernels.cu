@@ -711,8 +711,4 @@ cudaError_t launch_state_transpose(const double* src, double* dst, int64_t G, bo
   return cudaGetLastError();
 }
 
-cudaError_t launch_adjoint(int, const ElemArgs&, double*, double*, cudaStream_t) {
-  return cudaErrorNotSupported;
-}
-
 }  // namespace cxg

@@ -180,12 +180,36 @@ struct Vec4<double> {
   using T = double4;
 };
 
-template <typename R>
-__device__ __forceinline__ void ld3(const R* p, R& x, R& y, R& z) {
-  const typename Vec4<R>::T v = *reinterpret_cast<const typename Vec4<R>::T*>(p);
-  x = v.x;
-  y = v.y;
-  z = v.z;
+// Shared-memory layout of per-(element, Gauss point) node vectors: node k lives in
+// slot(k) = k/2 for even k and npad/2 + k/2 for odd k, so the row nodes 2r + i of the
+// lanes' tiles occupy consecutive slots. FP32 vectors are float4 per slot; FP64 vectors
+// are split in two half planes of double2 (x,y | z,0) so consecutive slots are 16 bytes
+// apart. Either way one warp-wide vector load touches distinct banks.
+__host__ __device__ constexpr int node_slot(int k, int npad) { return (k & 1) ? npad / 2 + (k >> 1) : (k >> 1); }
+
+template <typename R, int NPAD>
+struct VecIdx {
+  // flat index of component c of the vector in `slot` of plane block b (b = element*nq + q)
+  __device__ __forceinline__ static int at(int b, int slot, int c) {
+    if (sizeof(R) == 4) return (b * NPAD + slot) * 4 + c;
+    return ((b * 2 + (c >> 1)) * NPAD + slot) * 2 + (c & 1);
+  }
+};
+
+template <typename R, int NPAD>
+__device__ __forceinline__ void ld3(const R* base, int b, int slot, R& x, R& y, R& z) {
+  if (sizeof(R) == 4) {
+    const float4 v = *reinterpret_cast<const float4*>(base + VecIdx<R, NPAD>::at(b, slot, 0));
+    x = v.x;
+    y = v.y;
+    z = v.z;
+  } else {
+    const double2 v = *reinterpret_cast<const double2*>(base + VecIdx<R, NPAD>::at(b, slot, 0));
+    const double2 w = *reinterpret_cast<const double2*>(base + VecIdx<R, NPAD>::at(b, slot, 2));
+    x = v.x;
+    y = v.y;
+    z = w.x;
+  }
 }
 
 template <int ET, int MODE, typename R>
@@ -193,8 +217,8 @@ struct P1Smem {
   using G = Geo<ET>;
   static constexpr int n = G::n, nq = G::nq, npad = G::npad, EPW = G::EPW;
   static constexpr bool T = MODE == MODE_TANGENT;
-  R g[EPW][nq][npad][4];
-  R m[T ? EPW : 1][T ? nq : 1][T ? npad : 1][4];
+  R g[EPW * nq * npad * 4];                       // node vectors, see VecIdx
+  R m[T ? EPW * nq * npad * 4 : 4];
   R s[EPW][nq];
   R dp[T ? EPW : 1][T ? nq : 1][4];
   double x[EPW][3 * n];
@@ -233,8 +257,8 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
   }
   // zero the padded gradient slots once; they are never written afterwards
   for (int t = lane; t < EPW * nq * npad * 4; t += 32) {
-    (&W.g[0][0][0][0])[t] = R(0);
-    if (TAN) (&W.m[0][0][0][0])[t % (sizeof(W.m) / sizeof(R))] = R(0);
+    W.g[t] = R(0);
+    if (TAN) W.m[t % (sizeof(W.m) / sizeof(R))] = R(0);
   }
   __syncthreads();
 
@@ -302,7 +326,7 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
         double gk[3];
         for (int i = 0; i < 3; ++i) {
           gk[i] = it[i][0] * d0 + it[i][1] * d1 + it[i][2] * d2;
-          W.g[ei][q][k][i] = static_cast<R>(gk[i]);
+          W.g[VecIdx<R, npad>::at(ei * nq + q, node_slot(k, npad), i)] = static_cast<R>(gk[i]);
           if (ET == C3D8R) W.gc[ei][i * n + k] = gk[i];
         }
         if (TAN)
@@ -325,10 +349,12 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
         if (pl) {
           W.plastic[ei] = 1;
           for (int k = 0; k < n; ++k) {
-            const double gx = W.g[ei][q][k][0], gy = W.g[ei][q][k][1], gz = W.g[ei][q][k][2];
-            W.m[ei][q][k][0] = static_cast<R>(nv[0] * gx + nv[3] * gy + nv[4] * gz);
-            W.m[ei][q][k][1] = static_cast<R>(nv[3] * gx + nv[1] * gy + nv[5] * gz);
-            W.m[ei][q][k][2] = static_cast<R>(nv[4] * gx + nv[5] * gy + nv[2] * gz);
+            const int b = ei * nq + q, sl = node_slot(k, npad);
+            const double gx = W.g[VecIdx<R, npad>::at(b, sl, 0)], gy = W.g[VecIdx<R, npad>::at(b, sl, 1)],
+                         gz = W.g[VecIdx<R, npad>::at(b, sl, 2)];
+            W.m[VecIdx<R, npad>::at(b, sl, 0)] = static_cast<R>(nv[0] * gx + nv[3] * gy + nv[4] * gz);
+            W.m[VecIdx<R, npad>::at(b, sl, 1)] = static_cast<R>(nv[3] * gx + nv[1] * gy + nv[5] * gz);
+            W.m[VecIdx<R, npad>::at(b, sl, 2)] = static_cast<R>(nv[4] * gx + nv[5] * gy + nv[2] * gz);
           }
         }
         if (q == nq - 1) W.mu_hg[ei] = mhg;
@@ -376,13 +402,14 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
             R ga[2][3], gb[4][3];
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
-              ld3(&W.g[ei][q][a0 + i][0], ga[i][0], ga[i][1], ga[i][2]);
+              ld3<R, npad>(W.g, ei * nq + q, node_slot(a0 + i, npad), ga[i][0], ga[i][1], ga[i][2]);
               ga[i][0] *= s;
               ga[i][1] *= s;
               ga[i][2] *= s;
             }
 #pragma unroll
-            for (int j = 0; j < 4; ++j) ld3(&W.g[ei][q][b0 + j][0], gb[j][0], gb[j][1], gb[j][2]);
+            for (int j = 0; j < 4; ++j)
+              ld3<R, npad>(W.g, ei * nq + q, node_slot(b0 + j, npad), gb[j][0], gb[j][1], gb[j][2]);
 #pragma unroll
             for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -412,9 +439,11 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
             const R sl = W.dp[ei][q][0], sm = W.dp[ei][q][1], sc = W.dp[ei][q][2];
             R ga[2][3], gb[4][3];
 #pragma unroll
-            for (int i = 0; i < 2; ++i) ld3(&W.g[ei][q][a0 + i][0], ga[i][0], ga[i][1], ga[i][2]);
+            for (int i = 0; i < 2; ++i)
+              ld3<R, npad>(W.g, ei * nq + q, node_slot(a0 + i, npad), ga[i][0], ga[i][1], ga[i][2]);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) ld3(&W.g[ei][q][b0 + j][0], gb[j][0], gb[j][1], gb[j][2]);
+            for (int j = 0; j < 4; ++j)
+              ld3<R, npad>(W.g, ei * nq + q, node_slot(b0 + j, npad), gb[j][0], gb[j][1], gb[j][2]);
 #pragma unroll
             for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -429,9 +458,11 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
             if (sc != R(0)) {
               R ma[2][3], mb[4][3];
 #pragma unroll
-              for (int i = 0; i < 2; ++i) ld3(&W.m[ei][q][a0 + i][0], ma[i][0], ma[i][1], ma[i][2]);
+              for (int i = 0; i < 2; ++i)
+                ld3<R, npad>(W.m, ei * nq + q, node_slot(a0 + i, npad), ma[i][0], ma[i][1], ma[i][2]);
 #pragma unroll
-              for (int j = 0; j < 4; ++j) ld3(&W.m[ei][q][b0 + j][0], mb[j][0], mb[j][1], mb[j][2]);
+              for (int j = 0; j < 4; ++j)
+                ld3<R, npad>(W.m, ei * nq + q, node_slot(b0 + j, npad), mb[j][0], mb[j][1], mb[j][2]);
 #pragma unroll
               for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -472,7 +503,9 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
         double f[3] = {0, 0, 0};
         for (int q = 0; q < nq; ++q) {
           const double* S = W.sig[ei][q];
-          const double gx = W.g[ei][q][a][0], gy = W.g[ei][q][a][1], gz = W.g[ei][q][a][2];
+          const int gb_ = ei * nq + q, sl = node_slot(a, npad);
+          const double gx = W.g[VecIdx<R, npad>::at(gb_, sl, 0)], gy = W.g[VecIdx<R, npad>::at(gb_, sl, 1)],
+                       gz = W.g[VecIdx<R, npad>::at(gb_, sl, 2)];
           f[0] += S[0] * gx + S[3] * gy + S[4] * gz;
           f[1] += S[3] * gx + S[1] * gy + S[5] * gz;
           f[2] += S[4] * gx + S[5] * gy + S[2] * gz;
@@ -494,18 +527,31 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
 }
 
 // ---- P2: row gather ------------------------------------------------------------------
+// Lanes map to (incident element in flight, column node lb of that element); EG
+// elements are in flight per pass (EG = 1 for 15/20-node families, 32/n otherwise).
+// Every lane issues its loads (connectivity, node mask, slot, the 9 block values)
+// independently, so a pass costs one round of memory latency, not a chain per column.
+template <int ET>
+struct P2Geo {
+  static constexpr int n = nodes_of(ET);
+  static constexpr int EG = n >= 16 ? 1 : 32 / n;
+};
+
 template <int ET, bool TAN, typename R, bool DIAGFIX>
 __global__ void p2_kernel(ElemArgs A, V2Args V) {
   using G = Geo<ET>;
   constexpr int n = G::n, NB = G::NB;
+  constexpr int EG = P2Geo<ET>::EG;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* buf = reinterpret_cast<double*>(smem) + static_cast<int64_t>(warp) * V.row_stride;
+  const int64_t wstride = V.row_stride + (DIAGFIX ? 32 * 9 : 0);
+  double* buf = reinterpret_cast<double*>(smem) + static_cast<int64_t>(warp) * wstride;
+  double* part = buf + V.row_stride;  // [32][9] diagonal partials (mixed precision)
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   const R* ed = reinterpret_cast<const R*>(V.edata);
-  const int ij = lane % 9, grp = lane / 9;
-  const int i = ij / 3, j = ij % 3;
+  const int sub = lane / n, lb = lane % n;
+  const bool lane_ok = sub < EG;
   for (int64_t a = gwarp; a < A.n_nodes; a += nwarps) {
     const int ma = A.node_mask[a];
     const int nf = __popc(ma);
@@ -518,57 +564,84 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
       for (int64_t t = lane; t < total; t += 32) buf[t] = 0.0;
     }
     __syncwarp();
-    const bool fi = (ma >> i) & 1;
-    const int ri = __popc(ma & ((1 << i) - 1));
-    double rr = 0.0;    // rhs contribution of row (a, i), spread over 9 lanes
-    double fsum = 0.0;  // internal force component (lanes 27..29)
+    double rr[3] = {0.0, 0.0, 0.0};
+    double fs[3] = {0.0, 0.0, 0.0};
     const int64_t i0 = V.inc_ptr[a], i1 = V.inc_ptr[a + 1];
-    for (int64_t inc = i0; inc < i1; ++inc) {
-      const int code = V.inc_code[inc];
-      const int64_t e = code / n;
-      const int la = code % n;
-      const R* eblk = ed + e * (NB * 9);
-      const unsigned short* sl = A.slot + e * n * n + la * n;
-      const int32_t* cn = A.conn + e * n;
-      if (lane < 27) {
-        double dsum = 0.0;
-        for (int lb = grp; lb < n; lb += 3) {
-          if (DIAGFIX && lb == la) continue;
-          const double v = lb >= la ? static_cast<double>(eblk[blk_index(n, la, lb) * 9 + ij])
-                                    : static_cast<double>(eblk[blk_index(n, lb, la) * 9 + 3 * j + i]);
-          if (DIAGFIX) dsum += v;
-          if (!fi) continue;
-          const int nb = cn[lb];
-          const int mb = A.node_mask[nb];
-          if ((mb >> j) & 1) {
-            buf[ri * L + sl[lb] + __popc(mb & ((1 << j) - 1))] += v;
-          } else {
-            const double pv = A.prescribed[3 * static_cast<int64_t>(nb) + j];
-            if (pv != 0.0) rr -= v * pv;
-          }
-        }
+    for (int64_t inc0 = i0; inc0 < i1; inc0 += EG) {
+      const int64_t inc = inc0 + sub;
+      const bool active = lane_ok && inc < i1;
+      if (active) {
+        const int code = V.inc_code[inc];
+        const int64_t e = code / n;
+        const int la = code % n;
+        const int64_t nb = A.conn[e * n + lb];
+        const int mb = A.node_mask[nb];
+        const int slotv = A.slot[(e * n + la) * n + lb];
+        const bool tr = lb < la;
+        const R* blk = ed + e * (NB * 9) + (tr ? blk_index(n, lb, la) : blk_index(n, la, lb)) * 9;
+        double v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = static_cast<double>(blk[tr ? 3 * (k % 3) + k / 3 : k]);
         if (DIAGFIX) {
-          const double d1 = __shfl_down_sync(0x07ffffffu, dsum, 9);
-          const double d2 = __shfl_down_sync(0x07ffffffu, dsum, 18);
-          if (lane < 9 && fi) {
-            const double diag = -(dsum + d1 + d2);
-            if ((ma >> j) & 1)
-              buf[ri * L + sl[la] + __popc(ma & ((1 << j) - 1))] += diag;
-            else {
-              const double pv = A.prescribed[3 * a + j];
-              if (pv != 0.0) rr -= diag * pv;
+#pragma unroll
+          for (int k = 0; k < 9; ++k) part[lane * 9 + k] = lb == la ? 0.0 : v[k];
+        }
+        if (!DIAGFIX || lb != la) {
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            if (!((ma >> i) & 1)) continue;
+            const int64_t row = __popc(ma & ((1 << i) - 1)) * L + slotv;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              if ((mb >> j) & 1) {
+                double* t = buf + row + __popc(mb & ((1 << j) - 1));
+                if (EG > 1)
+                  atomicAdd(t, v[3 * i + j]);
+                else
+                  *t += v[3 * i + j];
+              } else {
+                const double pv = A.prescribed[3 * nb + j];
+                if (pv != 0.0) rr[i] -= v[3 * i + j] * pv;
+              }
             }
           }
         }
-      } else if (TAN && lane < 30) {
-        fsum += V.fdata[e * (3 * n) + 3 * la + (lane - 27)];
+        if (TAN && lb == la) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) fs[d] += V.fdata[e * (3 * n) + 3 * la + d];
+        }
+      }
+      if (DIAGFIX) {
+        __syncwarp();
+        for (int t = lane; t < EG * 9; t += 32) {
+          const int s = t / 9, ij = t % 9, i = ij / 3, j = ij % 3;
+          const int64_t incs = inc0 + s;
+          if (incs >= i1 || !((ma >> i) & 1)) continue;
+          double sum = 0.0;
+          for (int k = 0; k < n; ++k) sum += part[(s * n + k) * 9 + ij];
+          const int code = V.inc_code[incs];
+          const int64_t e = code / n;
+          const int la = code % n;
+          const double diag = -sum;
+          if ((ma >> j) & 1) {
+            double* tp = buf + __popc(ma & ((1 << i) - 1)) * L + A.slot[(e * n + la) * n + la] +
+                         __popc(ma & ((1 << j) - 1));
+            if (EG > 1)
+              atomicAdd(tp, diag);
+            else
+              *tp += diag;
+          } else {
+            const double pv = A.prescribed[3 * a + j];
+            if (pv != 0.0) rr[i] -= diag * pv;
+          }
+        }
       }
       __syncwarp();
     }
-    // rhs: sum the 9 lanes of each row i and add the load vector
     if (A.rhs) {
+#pragma unroll
       for (int r = 0; r < 3; ++r) {
-        double v = (lane < 27 && i == r) ? rr : 0.0;
+        double v = rr[r];
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
         if (lane == 0 && ((ma >> r) & 1)) {
           const int64_t eq = A.node_eq0[a] + __popc(ma & ((1 << r) - 1));
@@ -577,9 +650,13 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
         }
       }
     }
-    if (TAN && A.f_int && lane >= 27 && lane < 30) {
-      const int64_t gi = 3 * a + (lane - 27);
-      A.f_int[gi] = (V.accumulate ? A.f_int[gi] : 0.0) + fsum;
+    if (TAN && A.f_int) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double v = fs[d];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) A.f_int[3 * a + d] = (V.accumulate ? A.f_int[3 * a + d] : 0.0) + v;
+      }
     }
     for (int64_t t = lane; t < total; t += 32) A.vals[base + t] = buf[t];
     __syncwarp();
@@ -617,10 +694,11 @@ template <int ET, bool TAN, typename R, bool DF>
 cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, cudaStream_t s) {
   auto kern = p2_kernel<ET, TAN, R, DF>;
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8
-  const int64_t stride = std::max<int64_t>(1, (v.max_row + 1) / 2 * 2);
+  const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
+  const int64_t wbytes = (stride + (DF ? 32 * 9 : 0)) * 8;
   int warps = 8;
-  while (warps > 1 && warps * stride * 8 > 160 * 1024) warps /= 2;
-  const size_t smem = static_cast<size_t>(warps) * stride * 8;
+  while (warps > 1 && warps * wbytes > 160 * 1024) warps /= 2;
+  const size_t smem = static_cast<size_t>(warps) * wbytes;
   if (smem > 220 * 1024) return cudaErrorInvalidConfiguration;
   v.row_stride = stride;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));

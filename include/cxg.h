@@ -52,7 +52,10 @@ typedef enum {
   /* an element references a node index outside [0, n_nodes)
    * (src/fem/assembly.cpp:53-54 "element references unknown node"). */
   CXG_ERR_UNKNOWN_NODE = 6,
-  CXG_ERR_NO_GPU = 7
+  CXG_ERR_NO_GPU = 7,
+  /* cxg_solve_cg stopped at max_iter above the tolerance (the reference's CG path
+   * throws "CG did not converge", src/compute/cpu_backend.cpp:57-62). */
+  CXG_ERR_NOT_CONVERGED = 8
 } cxg_status;
 
 typedef enum { CXG_FP64 = 0, CXG_MIXED = 1 } cxg_precision;
@@ -181,6 +184,17 @@ CXG_API int cxg_element_tangent_force(int32_t elem_type, int64_t n_elems, const 
                               const double* ue, const cxg_material* material,
                               const double* state_committed, double* state_trial,
                               int32_t precision, double* Ke, double* fe, void* stream);
+
+/* ---- reduced-system products and solve on the device ------------------------------
+ * The device counterpart of ComputeBackend::solve_sparse (include/calculixpp/compute/
+ * backend.hpp:51-56; CPU: SciPP spsolve / IC0-CG, src/compute/cpu_backend.cpp:24-72),
+ * on the plan's CSR pattern: y = K_ff x, and Jacobi-preconditioned conjugate gradients
+ * for K_ff x = rhs from the initial guess in x, stopping at ||r|| <= rtol ||rhs|| or
+ * max_iter. Returns CXG_ERR_NOT_CONVERGED (with the reached residual) when the
+ * tolerance is not met, as the reference's CG path throws (cpu_backend.cpp:57-62). */
+CXG_API int cxg_spmv(cxg_plan* plan, const double* vals, const double* x, double* y, void* stream);
+CXG_API int cxg_solve_cg(cxg_plan* plan, const double* vals, const double* rhs, double* x, double rtol,
+                         int32_t max_iter, int32_t* iterations, double* rel_residual, void* stream);
 
 /* ---- element_tangent_force for callers that cannot allocate device memory --------
  * No counterpart in the reference. Same computation and argument meaning as
