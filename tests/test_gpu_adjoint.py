@@ -122,8 +122,8 @@ def test_device_cg_matches_direct_solve(cuda):
     xd, _ = host_solution(plan, model.external_load_vector())
     assert rel <= 1e-13 and iters > 0
     assert rel_fro(to_np(x), xd) <= 1e-9
-    y = plan.spmv(vals, x)
-    assert rel_fro(to_np(y), to_np(rhs)) <= 1e-12
+    y = plan.spmv(vals, x)  # true residual; CG's recurrence residual drifts from it
+    assert rel_fro(to_np(y), to_np(rhs)) <= 1e-9
     with pytest.raises(CxgError) as exc:
         plan.solve_cg(vals, rhs, rtol=1e-14, max_iter=5)
     assert exc.value.code == 8 and "did not converge" in str(exc.value)
