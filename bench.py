@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--n", type=int, default=64, help="cells per axis of the C3D20 block")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--j2-n", type=int, default=128, help="cells per axis of the C3D8 J2 block (0: skip)")
     return ap.parse_args()
 
 
@@ -139,6 +140,90 @@ def c3d20_model(n, seed):
     cfg = mg.c3d20_block(n, seed=seed)
     m = cfg["mesh"]
     return Model(m, [Material(200000.0, 0.3)], None, cfg["spc"], None), cfg["f_ext"]
+
+
+def j2_model(n, k, seed=0):
+    """The J2 Newton workload (C3D8 n^3, graded uniaxial ramp) at increment k."""
+    from calculixpp_b200 import meshgen as mg
+    from calculixpp_b200.assembly import Material, Model
+    cfg = mg.c3d8_j2_block(n, seed)
+    u, spc = mg.j2_increment(cfg, k)
+    return Model(cfg["mesh"], [Material(mg.J2_E, mg.J2_NU, cfg["table"])], None, spc, None), cfg, u
+
+
+def j2_algorithmic_bytes(plan, model):
+    """Compulsory bytes of one residual + consistent-tangent pass: connectivity, node
+    coordinates and displacements read, E and nu per element, the isotropic-hardening
+    state (plastic strain 6 + equivalent plastic strain 1 doubles per Gauss point) read
+    and written, f_int and rhs written, every K_ff value written once."""
+    m = model.mesh
+    npe = m.conn.shape[1]
+    G = m.n_elems * npe  # 2x2x2 rule: 8 points per C3D8
+    return (4 * npe * m.n_elems + 24 * m.n_nodes * 3 + 16 * m.n_elems + 2 * 56 * G + 8 * plan.n_free
+            + 8 * plan.nnz)
+
+
+def j2_newton(args, world, dev, stream):
+    """Residual + consistent tangent of one Newton iteration of the last ramp increment,
+    FP64 and mixed, on the C3D8 J2 block. The committed state is that of increment 9
+    (assembled and committed before timing); every timed step re-integrates all
+    elements from it."""
+    import torch
+
+    from calculixpp_b200 import Plan
+    model, cfg, u10 = j2_model(args.j2_n, 10)
+    from calculixpp_b200 import meshgen as mg
+    u9, _ = mg.j2_increment(cfg, 9)
+    plan = Plan(model, "fp64")
+    m = model.mesh
+    vals = torch.empty(plan.nnz, dtype=torch.float64, device=dev)
+    f_int = torch.empty(3 * m.n_nodes, dtype=torch.float64, device=dev)
+    rhs = torch.empty(plan.n_free, dtype=torch.float64, device=dev)
+    d_u9 = torch.as_tensor(u9, device=dev)
+    d_u = torch.as_tensor(u10, device=dev)
+    plan.assemble_tangent(d_u9, vals=vals, f_int=f_int, rhs=rhs)
+    plan.commit()
+
+    def step():
+        plan.assemble_tangent(d_u, vals=vals, f_int=f_int, rhs=rhs, check=False)
+
+    out = {}
+    keep = {}
+    for prec in ("fp64", "mixed"):
+        plan.set_precision(prec)
+        for _ in range(args.warmup):
+            step()
+        plan.check()
+        torch.cuda.synchronize()
+        barrier(world)
+        t = max_over_ranks(time_steps(step, args.steps, stream), world)
+        plan.check()
+        keep[prec] = (vals.clone(), f_int.clone(), plan.state(committed=False).clone())
+        out[prec] = {"value": world * m.n_elems * args.steps / t, "ms_per_step": t / args.steps * 1e3}
+    (v64, f64, s64), (vm, fm, sm) = keep["fp64"], keep["mixed"]
+    yielded = float((s64[:, 6] > 0).double().mean())
+    B = j2_algorithmic_bytes(plan, model)
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    ach = B / (out["fp64"]["ms_per_step"] * 1e-3) / 1e9
+    res = {
+        "workload": f"C3D8 J2 block {args.j2_n}^3, graded uniaxial ramp, increment 10 of 10, "
+                    "Newton residual + consistent tangent",
+        "elements": m.n_elems, "gauss_points": 8 * m.n_elems, "nnz": plan.nnz,
+        "yielded_fraction": yielded,
+        "fp64": out["fp64"], "mixed": out["mixed"],
+        "speedup_mixed_vs_fp64": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+        "mixed_error": {"K_rel_fro": float(torch.linalg.norm(vm - v64) / torch.linalg.norm(v64)),
+                        "f_int_rel_l2": float(torch.linalg.norm(fm - f64) / torch.linalg.norm(f64)),
+                        "state_max_abs": float((sm - s64).abs().max())},
+        "roofline_fp64": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                          "algorithmic_bytes": B, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "gpu_launches_per_step": 2,
+    }
+    del keep, v64, vm, f64, fm, s64, sm, vals, f_int, rhs
+    plan.close()
+    torch.cuda.empty_cache()
+    return res
 
 
 def algorithmic_bytes(plan, model):
@@ -324,6 +409,8 @@ def main():
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(time.perf_counter() - t0, world)
 
+    j2 = j2_newton(args, world, dev, stream) if args.j2_n > 0 else None
+
     # accuracy of the mixed path against FP64 on a reduced block (host sparse solve)
     acc = None
     if rank == 0:
@@ -376,6 +463,7 @@ def main():
                      "kernel": "element_kernel<C3D20, linear, scatter, float>",
                      "kernel_ms": mix["t_kernel"] / args.steps * 1e3,
                      "algorithmic_bytes": B, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "j2_newton": j2,
         "cpu_baseline": cpu,
         "e2e": {"value": world * E * e2e_steps / t_e2e, "unit": "element-integrations/s",
                 "h2d_bytes_per_step": int(h_f.numel() * 8),

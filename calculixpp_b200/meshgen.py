@@ -196,3 +196,53 @@ def c3d20_block(n=64, seed=0) -> dict:
     f_ext = np.zeros(3 * m.n_nodes)
     f_ext[3 * top + 0] = 1.0 / top.size
     return {"mesh": m, "spc": spc, "f_ext": f_ext}
+
+
+J2_E, J2_NU, J2_SY, J2_H = 210000.0, 0.3, 250.0, 1000.0
+
+
+def j2_table(h=J2_H, sy=J2_SY, ep_max=1.0):
+    """*PLASTIC table of linear isotropic hardening: {0: sy, ep_max: sy + h*ep_max}. The
+    reference extrapolates the table flat beyond its last point (plasticity.cpp:74-78),
+    so ep_max is set far above any reachable equivalent plastic strain."""
+    return (np.array([0.0, ep_max]), np.array([sy, sy + h * ep_max]))
+
+
+def graded_uniaxial_field(coords, eps_max, p=3.0, nu=J2_NU):
+    """Displacement of a bar under a graded uniaxial ramp: axial strain
+    eps(x) = eps_max * x^p along the unit cube's x axis, lateral contraction -nu*eps(x)
+    about the cross-section centre. With p = 3 and eps_max = 0.5 % the points with
+    x > (sigma_y/(E*eps_max))^(1/3) ~ 0.62 yield, i.e. ~40 % of the Gauss points."""
+    x, y, z = coords[:, 0], coords[:, 1], coords[:, 2]
+    eps = eps_max * x ** p
+    u = np.empty_like(coords)
+    u[:, 0] = eps_max * x ** (p + 1) / (p + 1)
+    u[:, 1] = -nu * eps * (y - 0.5)
+    u[:, 2] = -nu * eps * (z - 0.5)
+    return u.reshape(-1)
+
+
+def c3d8_j2_block(n=128, seed=0) -> dict:
+    """J2 Newton workload: n^3 C3D8 cube (unit edge), E=210000, nu=0.3, sigma_y=250,
+    linear isotropic hardening H=1000. Constraints: u_x = 0 on x=0, u_y = u_z = 0 at the
+    origin, u_z = 0 at (0,1,0); u_x on x=1 follows the ramp (filled in per increment by
+    `j2_increment`)."""
+    m = box_mesh(C3D8, n, n, n, 1.0, 1.0, 1.0, jitter=0.0, seed=seed)
+    m.young = np.full(m.n_elems, J2_E)
+    m.poisson = np.full(m.n_elems, J2_NU)
+    x0 = face_nodes(m, 0, 0.0)
+    x1 = face_nodes(m, 0, 1.0)
+    origin = int(np.argmin(np.abs(m.coords).sum(1)))
+    corner = int(np.argmin(np.abs(m.coords - np.array([0.0, 1.0, 0.0])).sum(1)))
+    sn = np.concatenate([x0, x1, [origin, origin, corner]]).astype(np.int32)
+    sc = np.concatenate([np.zeros(x0.size + x1.size, np.int32), np.array([1, 2, 2], np.int32)])
+    return {"mesh": m, "spc_node": sn, "spc_comp": sc, "x1": x1, "table": j2_table()}
+
+
+def j2_increment(cfg, k, n_inc=10, eps_final=0.005):
+    """(u, spc) of increment k of the ramp: the graded field at eps_max = eps_final*k/n_inc
+    and the matching prescribed values."""
+    m = cfg["mesh"]
+    u = graded_uniaxial_field(m.coords, eps_final * k / n_inc)
+    sn, sc = cfg["spc_node"], cfg["spc_comp"]
+    return u, (sn, sc, u[3 * sn.astype(np.int64) + sc])
