@@ -11,7 +11,8 @@ from ._lib import CxgError, load as load_library
 from .assembly import (LinearSystem, Material, MaterialPoints, Model, Plan, assemble_linear_static,
                        assemble_material_tangent, element_stiffness, element_tangent_force,
                        make_material_points)
+from .batch import Batch
 
-__all__ = ["meshgen", "CxgError", "load_library", "LinearSystem", "Material", "MaterialPoints", "Model",
+__all__ = ["meshgen", "Batch", "CxgError", "load_library", "LinearSystem", "Material", "MaterialPoints", "Model",
            "Plan", "assemble_linear_static", "assemble_material_tangent", "element_stiffness",
            "element_tangent_force", "make_material_points"]

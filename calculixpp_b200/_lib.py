@@ -56,6 +56,17 @@ class CxgPlanInfo(C.Structure):
                 ("precision", C.c_int32), ("device", C.c_int32), ("device_bytes", C.c_int64)]
 
 
+class CxgBatchModelInfo(C.Structure):
+    _fields_ = [("elem_type", C.c_int32), ("group", C.c_int32), ("n_nodes", C.c_int64), ("n_elems", C.c_int64),
+                ("n_free", C.c_int32), ("nnz", C.c_int64), ("vals_offset", C.c_int64), ("rhs_offset", C.c_int64),
+                ("node_offset", C.c_int64)]
+
+
+class CxgBatchInfo(C.Structure):
+    _fields_ = [("n_models", C.c_int32), ("n_groups", C.c_int32), ("n_nodes", C.c_int64), ("n_elems", C.c_int64),
+                ("n_free", C.c_int64), ("nnz", C.c_int64), ("device_bytes", C.c_int64)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "cxg_last_error": (C.c_char_p, []),
@@ -87,6 +98,20 @@ SIGNATURES = {
                                C.POINTER(C.c_double), _vp]),
     "cxg_element_tangent_force_noalloc": (C.c_int, [C.c_int32, C.c_int64, _vp, _vp, C.POINTER(CxgMaterial),
                                                     _vp, _vp, C.c_int32, _vp, _vp, _vp]),
+    "cxg_batch_create": (C.c_int, [C.c_int32, C.POINTER(CxgMeshDesc), C.POINTER(CxgDofmapDesc), C.c_int32,
+                                   C.POINTER(_vp)]),
+    "cxg_batch_destroy": (C.c_int, [_vp]),
+    "cxg_batch_get_info": (C.c_int, [_vp, C.POINTER(CxgBatchInfo)]),
+    "cxg_batch_get_model_info": (C.c_int, [_vp, C.c_int32, C.POINTER(CxgBatchModelInfo)]),
+    "cxg_batch_get_pattern": (C.c_int, [_vp, C.c_int32, _vp, _vp]),
+    "cxg_batch_set_precision": (C.c_int, [_vp, C.c_int32]),
+    "cxg_batch_assemble": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cxg_batch_graph_launch": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cxg_batch_check": (C.c_int, [_vp]),
+    "cxg_batch_tune": (C.c_int, [_vp, _vp, _vp, _vp, C.c_char_p, _vp]),
+    "cxg_batch_group_config": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "cxg_batch_set_group_config": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
 }
 
 _LIB = None

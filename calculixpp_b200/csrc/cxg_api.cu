@@ -15,41 +15,17 @@
 #include <string>
 #include <vector>
 
-#include "../../include/cxg.h"
-#include "cxg_internal.cuh"
+#include "cxg_plan.hpp"
 
 using namespace cxg;
-
-struct cxg_plan {
-  int device = 0;
-  int64_t n_nodes = 0, n_elems = 0, n_gauss = 0;
-  int32_t type = 0, n_free = 0, precision = 0;
-  double* coords = nullptr;
-  int32_t* conn = nullptr;
-  double* young = nullptr;
-  double* poisson = nullptr;
-  int32_t* elem_mat = nullptr;
-  J2Mat* mats = nullptr;
-  int32_t n_mats = 0;
-  bool has_plastic = false;
-  int32_t* dof_eq = nullptr;
-  double* prescribed = nullptr;
-  PatternOut pat;
-  double* state[2] = {nullptr, nullptr};  // SoA [13][G]: committed, trial
-  DevStatus* status = nullptr;
-  void* edata = nullptr;      // per-element K blocks of the two-pass assembly
-  size_t edata_bytes = 0;
-  double* fdata = nullptr;    // per-element internal force (material-point mode)
-  cudaStream_t last_stream = nullptr;
-  int64_t device_bytes = 0;
-  // staging buffers for host pointers, grown on demand and reused
-  void* stage[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-  size_t stage_bytes[6] = {0, 0, 0, 0, 0, 0};
-};
+using namespace cxg::api;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
+
+namespace cxg {
+namespace api {
 
 int set_err(int code, const std::string& msg) {
   g_err = msg;
@@ -64,12 +40,6 @@ int cuda_err(cudaError_t e, const char* where) {
   return set_err(CXG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-#define CHECK_CUDA(expr, where)                 \
-  do {                                          \
-    cudaError_t _e = (expr);                    \
-    if (_e != cudaSuccess) return cuda_err(_e, where); \
-  } while (0)
-
 bool on_device(const void* p) {
   if (!p) return false;
   cudaPointerAttributes at;
@@ -79,6 +49,11 @@ bool on_device(const void* p) {
   }
   return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
+
+}  // namespace api
+}  // namespace cxg
+
+namespace {
 
 template <typename T>
 cudaError_t alloc_copy(T** dst, const T* src, size_t count, cudaStream_t s, int64_t* bytes) {
@@ -160,6 +135,10 @@ __global__ void fill_props_kernel(const int32_t* elem_mat, const double* E, cons
   }
 }
 
+}  // namespace
+
+namespace cxg {
+namespace api {
 int plan_status(cxg_plan* p, int64_t* bad) {
   CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");
   DevStatus st;
@@ -178,6 +157,10 @@ int plan_status(cxg_plan* p, int64_t* bad) {
   }
   return CXG_OK;
 }
+}  // namespace api
+}  // namespace cxg
+
+namespace {
 
 int ensure_state(cxg_plan* p, cudaStream_t s) {
   if (p->state[0]) return CXG_OK;
@@ -190,6 +173,10 @@ int ensure_state(cxg_plan* p, cudaStream_t s) {
   return CXG_OK;
 }
 
+}  // namespace
+
+namespace cxg {
+namespace api {
 int ensure_v2(cxg_plan* p, bool tangent) {
   const size_t need = v2_edata_bytes(p->type, p->n_elems, p->precision);
   if (p->edata_bytes < need) {
@@ -241,6 +228,11 @@ ElemArgs base_args(cxg_plan* p) {
   a.status = p->status;
   return a;
 }
+
+}  // namespace api
+}  // namespace cxg
+
+namespace {
 
 int copy_out(void* dst, const void* dev, size_t bytes, cudaStream_t s) {
   if (!dst || dst == dev) return CXG_OK;
@@ -450,7 +442,8 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
   ElemArgs a = base_args(p);
   a.vals = static_cast<double*>(dv);
   a.rhs = static_cast<double*>(dr);
-  CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, p->precision, a, v2_args(p, static_cast<const double*>(df), accumulate), s),
+  CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, p->precision, a, v2_args(p, static_cast<const double*>(df), accumulate), s,
+                       p->cfg[p->precision]),
              "assembly kernels");
   if ((rc = copy_out(vals, dv, vb, s))) return rc;
   if ((rc = copy_out(rhs, dr, rb, s))) return rc;

@@ -90,8 +90,21 @@ struct V2Args {
   int64_t row_stride;       // set by the launcher
   int accumulate;           // add into vals / rhs / f_int instead of overwriting
 };
+// Launch shape of the two passes. tile: element-pass node-pair tile (0 = 2x4, 1 = 2x2,
+// 2 = 4x4; 1 and 2 in the linear pass only, 2 with FP32 accumulators only);
+// *_blocks_per_sm: persistent grid per SM (0 = as many as are resident); p2_warps:
+// warps per row-gather block (0 = up to 8 as shared memory allows); passes: bit 0 the
+// element pass, bit 1 the row gather.
+struct LaunchCfg {
+  int tile = 0;
+  int p1_blocks_per_sm = 0;
+  int p2_warps = 0;
+  int p2_blocks_per_sm = 0;
+  int passes = 3;
+};
 size_t v2_edata_bytes(int elem_type, int64_t n_elems, int precision);
-cudaError_t launch_v2(int elem_type, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s);
+cudaError_t launch_v2(int elem_type, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s,
+                      const LaunchCfg& cfg = LaunchCfg{});
 
 // Launchers (cxg_kernels.cu). `precision` 0 = FP64, 1 = mixed.
 cudaError_t launch_element_kernel(int elem_type, int mode, bool dense, int precision,

@@ -39,15 +39,16 @@ struct TileList {
   unsigned char c[64];
 };
 
-constexpr TileList make_tiles(int n) {
+// Node-pair tiles of TR rows x TC columns covering the upper triangle (a <= b).
+constexpr TileList make_tiles(int n, int TR, int TC) {
   TileList t{};
   const int npad = (n + 3) / 4 * 4;
-  for (int r = 0; r < npad / 2; ++r)
-    for (int c = 0; c < npad / 4; ++c) {
+  for (int r = 0; r < npad / TR; ++r)
+    for (int c = 0; c < npad / TC; ++c) {
       bool any = false;
-      for (int i = 0; i < 2; ++i)
-        for (int j = 0; j < 4; ++j) {
-          const int a = 2 * r + i, b = 4 * c + j;
+      for (int i = 0; i < TR; ++i)
+        for (int j = 0; j < TC; ++j) {
+          const int a = TR * r + i, b = TC * c + j;
           if (a < n && b < n && a <= b) any = true;
         }
       if (any) {
@@ -59,13 +60,18 @@ constexpr TileList make_tiles(int n) {
   return t;
 }
 
-template <int ET>
+// Tile shapes of the element pass (TILE codes): 0 = 2x4 (default), 1 = 2x2, 2 = 4x4.
+constexpr int tile_rows(int tile) { return tile == 2 ? 4 : 2; }
+constexpr int tile_cols(int tile) { return tile == 1 ? 2 : 4; }
+
+template <int ET, int TILE = 0>
 struct Geo {
   static constexpr int n = nodes_of(ET);
   static constexpr int nq = gauss_of(ET);
   static constexpr int npad = (n + 3) / 4 * 4;
   static constexpr int NB = n * (n + 1) / 2;
-  static constexpr TileList tiles = make_tiles(n);
+  static constexpr int TR = tile_rows(TILE), TC = tile_cols(TILE);
+  static constexpr TileList tiles = make_tiles(n, TR, TC);
   static constexpr int NT = tiles.count;
   static constexpr int EPW = NT >= 32 ? 1 : 32 / NT;
 };
@@ -212,9 +218,9 @@ __device__ __forceinline__ void ld3(const R* base, int b, int slot, R& x, R& y, 
   }
 }
 
-template <int ET, int MODE, typename R>
+template <int ET, int MODE, typename R, int TILE>
 struct P1Smem {
-  using G = Geo<ET>;
+  using G = Geo<ET, TILE>;
   static constexpr int n = G::n, nq = G::nq, npad = G::npad, EPW = G::EPW;
   static constexpr bool T = MODE == MODE_TANGENT;
   R g[EPW * nq * npad * 4];                       // node vectors, see VecIdx
@@ -233,12 +239,13 @@ struct P1Smem {
   int plastic[EPW];
 };
 
-template <int ET, int MODE, typename R>
+template <int ET, int MODE, typename R, int TILE>
 __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
-  using G = Geo<ET>;
+  using G = Geo<ET, TILE>;
   constexpr int n = G::n, nq = G::nq, npad = G::npad, EPW = G::EPW, NT = G::NT, NB = G::NB;
+  constexpr int TR = G::TR, TC = G::TC;
   constexpr bool TAN = MODE == MODE_TANGENT;
-  using WS = P1Smem<ET, MODE, R>;
+  using WS = P1Smem<ET, MODE, R, TILE>;
   extern __shared__ __align__(16) unsigned char smem[];
   double* sdN = reinterpret_cast<double*>(smem);  // [n][3][nq]
   double* sw = sdN + n * 3 * nq;
@@ -249,7 +256,7 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
   for (int i = threadIdx.x; i < n * 3 * nq; i += blockDim.x) sdN[i] = c_dN[dn_offset(ET) + i];
   for (int i = threadIdx.x; i < nq; i += blockDim.x) sw[i] = c_w[ET][i];
   if (threadIdx.x == 0) {
-    constexpr TileList tl = make_tiles(n);
+    constexpr TileList tl = make_tiles(n, TR, TC);
     for (int i = 0; i < NT; ++i) {
       s_tr[i] = tl.r[i];
       s_tc[i] = tl.c[i];
@@ -381,17 +388,17 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
       }
       __syncwarp();
     }
-    // ---- phase C: 2x4 node-pair tiles -------------------------------------------------
-    if (lane < EPW * NT) {
-      const int ei = lane / NT, ti = lane % NT;
+    // ---- phase C: TR x TC node-pair tiles ---------------------------------------------
+    for (int task = lane; task < EPW * NT; task += 32) {
+      const int ei = task / NT, ti = task % NT;
       const int64_t e = e0 + ei;
       if (e < A.n_elems) {
-        const int a0 = 2 * s_tr[ti], b0 = 4 * s_tc[ti];
-        R acc[2][4][9];
+        const int a0 = TR * s_tr[ti], b0 = TC * s_tc[ti];
+        R acc[TR][TC][9];
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < TR; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
+          for (int j = 0; j < TC; ++j)
 #pragma unroll
             for (int k = 0; k < 9; ++k) acc[i][j][k] = R(0);
         const bool pl = TAN && W.plastic[ei];
@@ -399,21 +406,21 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
 #pragma unroll 3
           for (int q = 0; q < nq; ++q) {
             const R s = W.s[ei][q];
-            R ga[2][3], gb[4][3];
+            R ga[TR][3], gb[TC][3];
 #pragma unroll
-            for (int i = 0; i < 2; ++i) {
+            for (int i = 0; i < TR; ++i) {
               ld3<R, npad>(W.g, ei * nq + q, node_slot(a0 + i, npad), ga[i][0], ga[i][1], ga[i][2]);
               ga[i][0] *= s;
               ga[i][1] *= s;
               ga[i][2] *= s;
             }
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < TC; ++j)
               ld3<R, npad>(W.g, ei * nq + q, node_slot(b0 + j, npad), gb[j][0], gb[j][1], gb[j][2]);
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
+            for (int i = 0; i < TR; ++i)
 #pragma unroll
-              for (int j = 0; j < 4; ++j)
+              for (int j = 0; j < TC; ++j)
 #pragma unroll
                 for (int x = 0; x < 3; ++x)
 #pragma unroll
@@ -421,9 +428,9 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
           }
           const R lam = static_cast<R>(W.lam[ei]), mu = static_cast<R>(W.mu[ei]);
 #pragma unroll
-          for (int i = 0; i < 2; ++i)
+          for (int i = 0; i < TR; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
+            for (int j = 0; j < TC; ++j) {
               R Gm[9];
 #pragma unroll
               for (int k = 0; k < 9; ++k) Gm[k] = acc[i][j][k];
@@ -437,17 +444,17 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
         } else if (TAN) {
           for (int q = 0; q < nq; ++q) {
             const R sl = W.dp[ei][q][0], sm = W.dp[ei][q][1], sc = W.dp[ei][q][2];
-            R ga[2][3], gb[4][3];
+            R ga[TR][3], gb[TC][3];
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
+            for (int i = 0; i < TR; ++i)
               ld3<R, npad>(W.g, ei * nq + q, node_slot(a0 + i, npad), ga[i][0], ga[i][1], ga[i][2]);
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < TC; ++j)
               ld3<R, npad>(W.g, ei * nq + q, node_slot(b0 + j, npad), gb[j][0], gb[j][1], gb[j][2]);
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
+            for (int i = 0; i < TR; ++i)
 #pragma unroll
-              for (int j = 0; j < 4; ++j) {
+              for (int j = 0; j < TC; ++j) {
                 const R dot = sm * (ga[i][0] * gb[j][0] + ga[i][1] * gb[j][1] + ga[i][2] * gb[j][2]);
 #pragma unroll
                 for (int x = 0; x < 3; ++x)
@@ -456,17 +463,17 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
                     acc[i][j][3 * x + y] += (sl * ga[i][x]) * gb[j][y] + (sm * gb[j][x]) * ga[i][y] + (x == y ? dot : R(0));
               }
             if (sc != R(0)) {
-              R ma[2][3], mb[4][3];
+              R ma[TR][3], mb[TC][3];
 #pragma unroll
-              for (int i = 0; i < 2; ++i)
+              for (int i = 0; i < TR; ++i)
                 ld3<R, npad>(W.m, ei * nq + q, node_slot(a0 + i, npad), ma[i][0], ma[i][1], ma[i][2]);
 #pragma unroll
-              for (int j = 0; j < 4; ++j)
+              for (int j = 0; j < TC; ++j)
                 ld3<R, npad>(W.m, ei * nq + q, node_slot(b0 + j, npad), mb[j][0], mb[j][1], mb[j][2]);
 #pragma unroll
-              for (int i = 0; i < 2; ++i)
+              for (int i = 0; i < TR; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
+                for (int j = 0; j < TC; ++j)
 #pragma unroll
                   for (int x = 0; x < 3; ++x)
 #pragma unroll
@@ -476,9 +483,9 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
         }
         R* out = reinterpret_cast<R*>(V.edata) + e * (NB * 9);
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < TR; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
+          for (int j = 0; j < TC; ++j) {
             const int a = a0 + i, b = b0 + j;
             if (a < n && b < n && a <= b) {
               R h = R(0);
@@ -670,33 +677,56 @@ int sm_count() {
   return sms;
 }
 
-template <int ET, int MODE, typename R>
-cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, cudaStream_t s) {
-  using WS = P1Smem<ET, MODE, R>;
+// Persistent grid: blocks_per_sm (0 = as many as are resident) blocks on every SM,
+// capped by the work available.
+int64_t persistent_grid(int64_t need, int resident, int blocks_per_sm) {
+  const int per_sm = blocks_per_sm > 0 ? std::min(blocks_per_sm, std::max(resident, 1)) : std::max(resident, 1);
+  return std::max<int64_t>(1, std::min<int64_t>(need, static_cast<int64_t>(per_sm) * sm_count()));
+}
+
+template <int ET, int MODE, typename R, int TILE>
+cudaError_t launch_p1_tile(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg, cudaStream_t s) {
+  using WS = P1Smem<ET, MODE, R, TILE>;
   constexpr int n = nodes_of(ET), nq = gauss_of(ET);
   constexpr size_t cta_bytes = (sizeof(double) * (n * 3 * nq + nq) + 15) / 16 * 16;
   constexpr size_t smem = cta_bytes + kW1 * ((sizeof(WS) + 15) / 16 * 16);
-  auto kern = p1_kernel<ET, MODE, R>;
+  static_assert(smem <= 227 * 1024, "element pass shared memory");
+  auto kern = p1_kernel<ET, MODE, R, TILE>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (err != cudaSuccess) return err;
   int per_sm = 0;
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT1, smem);
   if (err != cudaSuccess) return err;
-  constexpr int EPW = Geo<ET>::EPW;
+  constexpr int EPW = Geo<ET, TILE>::EPW;
   const int64_t need = (a.n_elems + kW1 * EPW - 1) / (kW1 * EPW);
-  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, static_cast<int64_t>(std::max(per_sm, 1)) * sm_count()));
+  const int64_t grid = persistent_grid(need, per_sm, cfg.p1_blocks_per_sm);
   if (a.n_elems == 0) return cudaSuccess;
   kern<<<static_cast<unsigned>(grid), kT1, smem, s>>>(a, v);
   return cudaGetLastError();
 }
 
+// Tile shapes instantiated: 2x4 everywhere; 2x2 and (FP32 accumulators only) 4x4 in
+// the linear pass, where the batched autotuner chooses among them.
+template <int ET, int MODE, typename R>
+cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg, cudaStream_t s) {
+  if constexpr (MODE == MODE_LINEAR) {
+    if (cfg.tile == 1) return launch_p1_tile<ET, MODE, R, 1>(a, v, cfg, s);
+    if constexpr (sizeof(R) == 4) {
+      if (cfg.tile == 2) return launch_p1_tile<ET, MODE, R, 2>(a, v, cfg, s);
+    }
+  }
+  if (cfg.tile != 0) return cudaErrorInvalidValue;
+  return launch_p1_tile<ET, MODE, R, 0>(a, v, cfg, s);
+}
+
 template <int ET, bool TAN, typename R, bool DF>
-cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, cudaStream_t s) {
+cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaStream_t s) {
   auto kern = p2_kernel<ET, TAN, R, DF>;
-  // warps per block: as many as fit in ~160 KB of row buffers, up to 8
+  // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
+  // configured count when it fits)
   const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
   const int64_t wbytes = (stride + (DF ? 32 * 9 : 0)) * 8;
-  int warps = 8;
+  int warps = cfg.p2_warps > 0 ? std::min(cfg.p2_warps, 32) : 8;
   while (warps > 1 && warps * wbytes > 160 * 1024) warps /= 2;
   const size_t smem = static_cast<size_t>(warps) * wbytes;
   if (smem > 220 * 1024) return cudaErrorInvalidConfiguration;
@@ -707,22 +737,25 @@ cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, cudaStream_t s) {
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
   if (err != cudaSuccess) return err;
   const int64_t need = (a.n_nodes + warps - 1) / warps;
-  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, static_cast<int64_t>(std::max(per_sm, 1)) * sm_count()));
+  const int64_t grid = persistent_grid(need, per_sm, cfg.p2_blocks_per_sm);
   kern<<<static_cast<unsigned>(grid), warps * 32, smem, s>>>(a, v);
   return cudaGetLastError();
 }
 
 template <int ET>
-cudaError_t launch_v2_type(int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s) {
-  cudaError_t err;
+cudaError_t launch_v2_type(int mode, int precision, const ElemArgs& a, const V2Args& v, const LaunchCfg& c,
+                           cudaStream_t s) {
+  cudaError_t err = cudaSuccess;
   if (mode == MODE_LINEAR) {
-    err = precision ? launch_p1_t<ET, MODE_LINEAR, float>(a, v, s) : launch_p1_t<ET, MODE_LINEAR, double>(a, v, s);
-    if (err != cudaSuccess) return err;
-    return precision ? launch_p2_t<ET, false, float, true>(a, v, s) : launch_p2_t<ET, false, double, false>(a, v, s);
+    if (c.passes & 1)
+      err = precision ? launch_p1_t<ET, MODE_LINEAR, float>(a, v, c, s) : launch_p1_t<ET, MODE_LINEAR, double>(a, v, c, s);
+    if (err != cudaSuccess || !(c.passes & 2)) return err;
+    return precision ? launch_p2_t<ET, false, float, true>(a, v, c, s) : launch_p2_t<ET, false, double, false>(a, v, c, s);
   }
-  err = precision ? launch_p1_t<ET, MODE_TANGENT, float>(a, v, s) : launch_p1_t<ET, MODE_TANGENT, double>(a, v, s);
-  if (err != cudaSuccess) return err;
-  return precision ? launch_p2_t<ET, true, float, true>(a, v, s) : launch_p2_t<ET, true, double, false>(a, v, s);
+  if (c.passes & 1)
+    err = precision ? launch_p1_t<ET, MODE_TANGENT, float>(a, v, c, s) : launch_p1_t<ET, MODE_TANGENT, double>(a, v, c, s);
+  if (err != cudaSuccess || !(c.passes & 2)) return err;
+  return precision ? launch_p2_t<ET, true, float, true>(a, v, c, s) : launch_p2_t<ET, true, double, false>(a, v, c, s);
 }
 
 }  // namespace
@@ -732,14 +765,15 @@ size_t v2_edata_bytes(int t, int64_t n_elems, int precision) {
   return static_cast<size_t>(n_elems) * (n * (n + 1) / 2) * 9 * (precision ? 4 : 8);
 }
 
-cudaError_t launch_v2(int t, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s) {
+cudaError_t launch_v2(int t, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s,
+                      const LaunchCfg& c) {
   switch (t) {
-    case C3D8: return launch_v2_type<C3D8>(mode, precision, a, v, s);
-    case C3D8R: return launch_v2_type<C3D8R>(mode, precision, a, v, s);
-    case C3D20: return launch_v2_type<C3D20>(mode, precision, a, v, s);
-    case C3D20R: return launch_v2_type<C3D20R>(mode, precision, a, v, s);
-    case C3D6: return launch_v2_type<C3D6>(mode, precision, a, v, s);
-    case C3D15: return launch_v2_type<C3D15>(mode, precision, a, v, s);
+    case C3D8: return launch_v2_type<C3D8>(mode, precision, a, v, c, s);
+    case C3D8R: return launch_v2_type<C3D8R>(mode, precision, a, v, c, s);
+    case C3D20: return launch_v2_type<C3D20>(mode, precision, a, v, c, s);
+    case C3D20R: return launch_v2_type<C3D20R>(mode, precision, a, v, c, s);
+    case C3D6: return launch_v2_type<C3D6>(mode, precision, a, v, c, s);
+    case C3D15: return launch_v2_type<C3D15>(mode, precision, a, v, c, s);
     default: return cudaErrorInvalidValue;
   }
 }

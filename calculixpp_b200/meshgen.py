@@ -22,6 +22,7 @@ import numpy as np
 C3D8, C3D8R, C3D20, C3D20R, C3D6, C3D15 = 2, 3, 4, 5, 6, 7
 NODES = {C3D8: 8, C3D8R: 8, C3D20: 20, C3D20R: 20, C3D6: 6, C3D15: 15}
 NGP = {C3D8: 8, C3D8R: 1, C3D20: 27, C3D20R: 8, C3D6: 2, C3D15: 6}
+TYPE_NAMES = {C3D8: "C3D8", C3D8R: "C3D8R", C3D20: "C3D20", C3D20R: "C3D20R", C3D6: "C3D6", C3D15: "C3D15"}
 NAMES = {C3D8: "C3D8", C3D8R: "C3D8R", C3D20: "C3D20", C3D20R: "C3D20R",
          C3D6: "C3D6", C3D15: "C3D15"}
 BY_NAME = {v: k for k, v in NAMES.items()}
@@ -71,12 +72,15 @@ def _lattice_nodes(n2, mask_fn):
 
 
 def box_mesh(etype: int, nx: int, ny: int, nz: int, lx=1.0, ly=1.0, lz=1.0,
-             jitter=0.0, seed=0) -> Mesh:
+             jitter=0.0, seed=0, straight_edges=False) -> Mesh:
     """Structured box [0,lx]x[0,ly]x[0,lz] of nx*ny*nz hex cells.
 
     Hex types give one element per cell, wedge types two. Interior nodes (not on
     the box faces) move by uniform(-jitter*h, +jitter*h) per axis, h the cell size
-    on that axis, drawn from numpy's default_rng(seed).
+    on that axis, drawn from numpy's default_rng(seed). With straight_edges, quadratic
+    elements keep straight edges: the jittered corner nodes define the geometry and
+    every midside node sits at the midpoint of its edge, so each quadratic element is
+    exactly as regular as the linear cell under it.
     """
     if etype not in NODES:
         raise ValueError(f"unsupported element type {etype}")
@@ -133,6 +137,13 @@ def box_mesh(etype: int, nx: int, ny: int, nz: int, lx=1.0, ly=1.0, lz=1.0,
         interior = np.all((coords > lo + eps) & (coords < hi - eps), axis=1)
         d = rng.uniform(-1.0, 1.0, size=coords.shape) * (jitter * h)
         coords = coords + d * interior[:, None]
+        if straight_edges and quadratic:
+            if etype == C3D15:
+                nc_, edges = 6, _W15_EDGES
+            else:
+                nc_, edges = 8, _HEX_EDGES
+            for i, (a, b) in enumerate(edges):
+                coords[conn[:, nc_ + i]] = 0.5 * (coords[conn[:, a]] + coords[conn[:, b]])
     return Mesh(coords=np.ascontiguousarray(coords), conn=conn, etype=etype,
                 shape=(nx, ny, nz))
 
@@ -246,3 +257,40 @@ def j2_increment(cfg, k, n_inc=10, eps_final=0.005):
     u = graded_uniaxial_field(m.coords, eps_final * k / n_inc)
     sn, sc = cfg["spc_node"], cfg["spc_comp"]
     return u, (sn, sc, u[3 * sn.astype(np.int64) + sc])
+
+
+BATCH_TYPES = (C3D8, C3D8R, C3D20R, C3D6, C3D15)
+
+
+def batch_box(etype, n_elems, jitter=0.1, seed=0, E=210000.0, nu=0.3):
+    """One model of the batched workload: a box of about n_elems elements of etype
+    (wedges: two per hex cell), cells h = 1 per axis, node jitter +-jitter*h (corner nodes;
+    quadratic midside nodes at their edge midpoints), z=0 clamped, unit total load in +x
+    on the top face."""
+    cells = max(1, int(round(n_elems / (2 if etype in (C3D6, C3D15) else 1))))
+    nx = max(1, int(round(cells ** (1.0 / 3.0))))
+    ny = nx
+    nz = max(1, int(round(cells / (nx * ny))))
+    m = box_mesh(etype, nx, ny, nz, float(nx), float(ny), float(nz), jitter=jitter, seed=seed, straight_edges=True)
+    m.young = np.full(m.n_elems, float(E))
+    m.poisson = np.full(m.n_elems, float(nu))
+    spc = clamp_face_spc(m, 2, 0.0)
+    top = face_nodes(m, 2, float(nz))
+    return m, spc, top
+
+
+def batched_workload(n_models=256, min_elems=1000, max_elems=200000, seed=0, types=BATCH_TYPES):
+    """The batched mixed-element workload: n_models independent boxes with element counts
+    log-uniform in [min_elems, max_elems], element type drawn from `types`, node jitter
+    +-0.1 h, E ~ U[70000, 210000] and nu ~ U[0.25, 0.35] per model. Returns a list of
+    (mesh, spc, top-face nodes, E, nu)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_models):
+        etype = int(types[rng.integers(len(types))])
+        ne = float(np.exp(rng.uniform(np.log(min_elems), np.log(max_elems))))
+        E = float(rng.uniform(70000.0, 210000.0))
+        nu = float(rng.uniform(0.25, 0.35))
+        m, spc, top = batch_box(etype, ne, 0.1, seed * 100003 + k, E, nu)
+        out.append((m, spc, top, E, nu))
+    return out

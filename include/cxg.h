@@ -228,6 +228,75 @@ CXG_API int cxg_element_tangent_force_noalloc(int32_t elem_type, int64_t n_elems
 CXG_API int cxg_adjoint_compliance(cxg_plan* plan, const double* u, double* dc_dE, double* dc_dX,
                            void* stream);
 
+/* ---- batches: many independent linear-elastic models in one launch ------------------
+ * No counterpart in the reference, whose drivers assemble one model per call
+ * (assemble_linear_static, src/fem/assembly.cpp:225-257); per model the results are
+ * those of cxg_assemble_linear on that model alone. A batch groups its models by
+ * element type. Each group is one block-diagonal system (the models' meshes and DOF
+ * maps concatenated in input order) that one element pass and one row gather
+ * assemble. All models' outputs share one vals and one rhs buffer at the offsets that
+ * cxg_batch_get_model_info reports, and the load vector is read at 3 * node_offset.
+ * Groups are ordered by element type code. Models whose material has a *PLASTIC table
+ * are rejected with CXG_ERR_UNSUPPORTED. */
+typedef struct cxg_batch cxg_batch;
+
+typedef struct {
+  int32_t elem_type;
+  int32_t group;
+  int64_t n_nodes;
+  int64_t n_elems;
+  int32_t n_free;
+  int64_t nnz;
+  int64_t vals_offset;  /* first K_ff value of the model in the batch's vals */
+  int64_t rhs_offset;   /* first equation of the model in the batch's rhs */
+  int64_t node_offset;  /* first node of the model in the batch's node order */
+} cxg_batch_model_info;
+
+typedef struct {
+  int32_t n_models;
+  int32_t n_groups;
+  int64_t n_nodes;
+  int64_t n_elems;
+  int64_t n_free;
+  int64_t nnz;
+  int64_t device_bytes;
+} cxg_batch_info;
+
+CXG_API int cxg_batch_create(int32_t n_models, const cxg_mesh_desc* meshes, const cxg_dofmap_desc* dofs,
+                             int32_t precision, cxg_batch** out);
+CXG_API int cxg_batch_destroy(cxg_batch* batch);
+CXG_API int cxg_batch_get_info(const cxg_batch* batch, cxg_batch_info* info);
+CXG_API int cxg_batch_get_model_info(const cxg_batch* batch, int32_t model, cxg_batch_model_info* info);
+/* The model's own CSR pattern: row_ptr[n_free + 1] from 0, col_idx[nnz] in the
+ * model's equation numbers. */
+CXG_API int cxg_batch_get_pattern(const cxg_batch* batch, int32_t model, int64_t* row_ptr, int32_t* col_idx);
+CXG_API int cxg_batch_set_precision(cxg_batch* batch, int32_t precision);
+/* Assemble every model on `stream` (vals, rhs, f_ext host or device; f_ext may be
+ * NULL). */
+CXG_API int cxg_batch_assemble(cxg_batch* batch, double* vals, double* rhs, const double* f_ext, void* stream);
+/* The same work as one CUDA graph, the groups as independent branches. The first
+ * call for a set of buffers and a precision captures the graph; later calls replay it.
+ * Device pointers only. */
+CXG_API int cxg_batch_graph_launch(cxg_batch* batch, double* vals, double* rhs, const double* f_ext,
+                                   void* stream);
+/* Synchronise and report the first in-kernel error of any group. */
+CXG_API int cxg_batch_check(cxg_batch* batch);
+/* Autotuner. For every group and the current precision it times each candidate launch
+ * shape on the batch's own data with CUDA events: the element-pass node-pair tile
+ * (2x4, 2x2 and, in mixed precision, 4x4), its persistent grid (blocks per SM) and
+ * the row gather's warps per block. It keeps the fastest of each pass. vals and rhs
+ * (device memory) serve as scratch and hold a complete assembly on return. Results are
+ * looked up in and added to the JSON file cache_path (NULL: no cache), keyed by SM
+ * count, element type, precision and element-count bucket. */
+CXG_API int cxg_batch_tune(cxg_batch* batch, double* vals, double* rhs, const double* f_ext,
+                           const char* cache_path, void* stream);
+/* Read or pin a group's launch shape (tile 0 = 2x4, 1 = 2x2, 2 = 4x4; 0 for a count
+ * means the default). */
+CXG_API int cxg_batch_group_config(const cxg_batch* batch, int32_t group, int32_t* elem_type, int32_t* tile,
+                                   int32_t* p1_blocks_per_sm, int32_t* p2_warps);
+CXG_API int cxg_batch_set_group_config(cxg_batch* batch, int32_t group, int32_t tile, int32_t p1_blocks_per_sm,
+                                       int32_t p2_warps);
+
 #ifdef __cplusplus
 }
 #endif

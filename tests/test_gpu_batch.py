@@ -1,0 +1,116 @@
+"""Batched assembly of many independent models (cxg_batch_*): every model's slice of the
+batch output equals the assembly of that model alone, bit for bit, in FP64 and mixed
+precision, whatever launch shape the groups run with, directly or as a CUDA graph;
+the autotuner's cache round-trips; plastic models are rejected."""
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from calculixpp_b200 import Batch, CxgError, Plan
+from calculixpp_b200 import meshgen as mg
+from calculixpp_b200.assembly import Material, Model
+from tests.helpers import to_np
+
+pytestmark = pytest.mark.gpu
+
+
+def small_models(seed=0):
+    rng = np.random.default_rng(seed)
+    out = []
+    types = [mg.C3D8, mg.C3D20R, mg.C3D6, mg.C3D8R, mg.C3D15, mg.C3D8, mg.C3D20, mg.C3D15, mg.C3D6, mg.C3D20R]
+    for k, t in enumerate(types):
+        ne = int(rng.integers(8, 300))
+        E, nu = float(rng.uniform(7e4, 2.1e5)), float(rng.uniform(0.25, 0.35))
+        m, spc, top = mg.batch_box(t, ne, 0.1, seed * 1000 + k, E, nu)
+        if k % 3 == 0:
+            m.young = m.young * rng.uniform(0.5, 1.5, m.n_elems)
+        loads = (top, np.zeros(top.size, dtype=np.int64), np.full(top.size, 1.0 / top.size))
+        out.append(Model(m, [Material(E, nu)], None, spc, loads))
+    return out
+
+
+@pytest.fixture(scope="module")
+def models():
+    return small_models()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_equals_single_model_plans(cuda, models, precision):
+    b = Batch(models, precision)
+    f = torch.as_tensor(b.load_vector(), device=b.device)
+    vals, rhs = b.assemble(f)
+    assert b.n_groups == len({m.mesh.etype for m in models})
+    for k, model in enumerate(models):
+        plan = Plan(model, precision)
+        v1, r1 = plan.assemble_linear(model.external_load_vector())
+        vk, rk = b.slices(k, vals, rhs)
+        rp, ci = b.pattern(k)
+        rp1, ci1 = (to_np(t) for t in plan.pattern())
+        assert np.array_equal(rp, rp1) and np.array_equal(ci, ci1)
+        assert torch.equal(vk, v1), k
+        assert torch.equal(rk, r1), k
+        plan.close()
+    b.close()
+
+
+def test_graph_launch_and_tile_shapes(cuda, models):
+    b = Batch(models, "mixed")
+    f = torch.as_tensor(b.load_vector(), device=b.device)
+    ref_v, ref_r = b.assemble(f)
+    ref_v, ref_r = ref_v.clone(), ref_r.clone()
+    vals, rhs = b.buffers()
+    for _ in range(3):
+        vals.fill_(np.nan)
+        b.graph_launch(f, vals, rhs, check=True)
+    assert torch.equal(vals, ref_v) and torch.equal(rhs, ref_r)
+    # every tile shape and launch shape gives the same bits (graph re-captured on change)
+    for tile in (1, 2):
+        for g in range(b.n_groups):
+            b.set_group_config(g, tile=tile, p1_blocks_per_sm=1, p2_warps=4)
+        vals.zero_()
+        b.graph_launch(f, vals, rhs, check=True)
+        assert torch.equal(vals, ref_v), tile
+    b.set_precision("fp64")
+    with pytest.raises(CxgError):
+        b.set_group_config(0, tile=2)
+    b.close()
+
+
+def test_tuner_cache_round_trip(cuda, models, tmp_path):
+    b = Batch(models, "mixed")
+    f = torch.as_tensor(b.load_vector(), device=b.device)
+    ref_v, ref_r = (t.clone() for t in b.assemble(f))
+    vals, rhs = b.buffers()
+    cache = tmp_path / "tune.json"
+    cfg = b.tune(f, vals, rhs, cache)
+    assert torch.equal(vals, ref_v) and torch.equal(rhs, ref_r)
+    data = json.loads(cache.read_text())
+    assert len(data) == b.n_groups
+    for key, entry in data.items():
+        assert key.startswith("sm") and "/mixed/" in key
+        assert entry["tile"] in (0, 1, 2) and entry["p2_warps"] in (2, 4, 8, 16) and entry["p1_ms"] > 0
+    # a second batch reads the cache instead of measuring, and picks the same shapes
+    b2 = Batch(models, "mixed")
+    before = cache.read_text()
+    assert b2.tune(f, vals, rhs, cache) == cfg
+    assert cache.read_text() == before
+    b.close()
+    b2.close()
+
+
+def test_host_buffers_and_rejections(cuda, models):
+    b = Batch(models[:3], "fp64")
+    f = b.load_vector()
+    hv = torch.empty(b.nnz, dtype=torch.float64)
+    hr = torch.empty(b.n_free, dtype=torch.float64)
+    b.assemble(torch.as_tensor(f), hv, hr)
+    dv, dr = b.assemble(torch.as_tensor(f, device=b.device))
+    assert torch.equal(hv, dv.cpu()) and torch.equal(hr, dr.cpu())
+    b.close()
+    m = models[0]
+    plastic = Model(m.mesh, [Material(2.1e5, 0.3, (np.array([0.0, 1.0]), np.array([250.0, 1250.0])))], None, m.spc)
+    with pytest.raises(CxgError) as exc:
+        Batch([models[1], plastic])
+    assert exc.value.code == 5
