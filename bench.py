@@ -190,8 +190,10 @@ def j2_newton(args, world, dev, stream):
 
     out = {}
     keep = {}
+    shapes = {}
     for prec in ("fp64", "mixed"):
         plan.set_precision(prec)
+        shapes[prec] = plan.tune(step, tangent=True)
         for _ in range(args.warmup):
             step()
         plan.check()
@@ -200,7 +202,8 @@ def j2_newton(args, world, dev, stream):
         t = max_over_ranks(time_steps(step, args.steps, stream), world)
         plan.check()
         keep[prec] = (vals.clone(), f_int.clone(), plan.state(committed=False).clone())
-        out[prec] = {"value": world * m.n_elems * args.steps / t, "ms_per_step": t / args.steps * 1e3}
+        out[prec] = {"value": world * m.n_elems * args.steps / t, "ms_per_step": t / args.steps * 1e3,
+                     "launch_shape": shapes[prec]}
     (v64, f64, s64), (vm, fm, sm) = keep["fp64"], keep["mixed"]
     yielded = float((s64[:, 6] > 0).double().mean())
     B = j2_algorithmic_bytes(plan, model)

@@ -185,6 +185,39 @@ class Plan:
         bad = C.c_int64()
         _lib.check(self.lib.cxg_plan_check(self.h, C.byref(bad)))
 
+    def set_launch_config(self, tangent=False, tile=0, p1_blocks_per_sm=0, p2_warps=0):
+        """Launch shape of the current precision's linear (or tangent) passes; tile 0 = 2x4,
+        1 = 2x2, 2 = 4x4. Results do not depend on it."""
+        _lib.check(self.lib.cxg_plan_set_launch_config(self.h, int(tangent), tile, p1_blocks_per_sm, p2_warps))
+
+    def tune(self, step, tangent=False, reps=3):
+        """Time `step()` (one assembly through this plan) with CUDA events for every tile
+        and element-pass grid shape of the current precision, keep the fastest and return
+        it with its time in ms."""
+        tiles = (0, 1) if tangent else (0, 1, 2)
+        best = None
+        for tile in tiles:
+            for bps in (0, 1, 2):
+                try:
+                    self.set_launch_config(tangent, tile, bps, 0)
+                except _lib.CxgError:
+                    continue
+                step()
+                torch.cuda.synchronize(self.device)
+                t = []
+                for _ in range(reps):
+                    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    s.record()
+                    step()
+                    e.record()
+                    e.synchronize()
+                    t.append(s.elapsed_time(e))
+                ms = sorted(t)[len(t) // 2]
+                if best is None or ms < best[0]:
+                    best = (ms, tile, bps)
+        self.set_launch_config(tangent, best[1], best[2], 0)
+        return {"tile": {0: "2x4", 1: "2x2", 2: "4x4"}[best[1]], "p1_blocks_per_sm": best[2], "ms": best[0]}
+
     # -- assembly --------------------------------------------------------------------
     def assemble_linear(self, f_ext=None, vals=None, rhs=None, check=True):
         dev = self.device

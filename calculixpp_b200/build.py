@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libcxg.so")
 SOURCES = ["cxg_api.cu", "cxg_kernels.cu", "cxg_pattern.cu", "cxg_v2.cu", "cxg_solve.cu", "cxg_batch.cu"]
-HEADERS = ["cxg_internal.cuh", "cxg_elements.hpp", os.path.join("..", "..", "include", "cxg.h")]
+HEADERS = ["cxg_internal.cuh", "cxg_elements.hpp", "cxg_plan.hpp", os.path.join("..", "..", "include", "cxg.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -44,14 +44,17 @@ def build(verbose: bool = False, force: bool = False) -> str:
     deps = srcs + [os.path.join(CSRC, h) for h in HEADERS]
     if not force and not _stale(LIB, deps):
         return LIB
-    objs = []
-    for src in srcs:
+    objs, procs = [], []
+    for src in srcs:  # the translation units compile in parallel
         obj = os.path.join(OUT_DIR, os.path.basename(src).replace(".cu", ".o"))
         cmd = [_nvcc(), *NVCC_FLAGS, "-dc", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+        procs.append((cmd, subprocess.Popen(cmd)))
         objs.append(obj)
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
            *objs, "-o", LIB]
     subprocess.run(cmd, check=True)

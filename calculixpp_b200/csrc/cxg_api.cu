@@ -224,6 +224,7 @@ ElemArgs base_args(cxg_plan* p) {
   a.node_eq0 = p->pat.node_eq0;
   a.prescribed = p->prescribed;
   a.slot = p->pat.slot;
+  a.conn_mask = p->pat.conn_mask;
   a.n_gauss = p->n_gauss;
   a.status = p->status;
   return a;
@@ -354,7 +355,7 @@ int cxg_plan_destroy(cxg_plan* p) {
   if (p->last_stream) cudaStreamSynchronize(p->last_stream);
   void* bufs[] = {p->coords, p->conn, p->young, p->poisson, p->elem_mat, p->mats, p->dof_eq, p->prescribed,
                   p->pat.row_ptr, p->pat.col_idx, p->pat.node_base, p->pat.node_rowlen, p->pat.node_mask,
-                  p->pat.node_eq0, p->pat.slot, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
+                  p->pat.node_eq0, p->pat.slot, p->pat.conn_mask, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
                   p->status, p->edata, p->fdata};
   for (void* b : bufs) cudaFree(b);
   for (void* b : p->stage) cudaFree(b);
@@ -412,6 +413,18 @@ int cxg_plan_update_young(cxg_plan* p, const double* young) {
   if (!p || !young) return set_err(CXG_ERR_INVALID_ARGUMENT, "null argument");
   CHECK_CUDA(cudaMemcpy(p->young, young, sizeof(double) * static_cast<size_t>(p->n_elems), cudaMemcpyDefault),
              "young update");
+  return CXG_OK;
+}
+
+int cxg_plan_set_launch_config(cxg_plan* p, int32_t mode, int32_t tile, int32_t p1_blocks_per_sm, int32_t p2_warps) {
+  if (!p || (mode != 0 && mode != 1)) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad plan or mode");
+  if (tile < 0 || tile > 2 || (tile == 2 && (mode == 1 || p->precision == CXG_FP64)) || p1_blocks_per_sm < 0 ||
+      p2_warps < 0 || p2_warps > 32)
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "bad launch shape (4x4 tiles: linear pass, mixed precision only)");
+  LaunchCfg& c = mode ? p->tcfg[p->precision] : p->cfg[p->precision];
+  c.tile = tile;
+  c.p1_blocks_per_sm = p1_blocks_per_sm;
+  c.p2_warps = p2_warps;
   return CXG_OK;
 }
 
@@ -476,7 +489,8 @@ int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_i
   a.u = static_cast<const double*>(du);
   a.state_c = p->state[0];
   a.state_t = p->state[1];
-  CHECK_CUDA(launch_v2(p->type, MODE_TANGENT, p->precision, a, v2_args(p, static_cast<const double*>(df), false), s),
+  CHECK_CUDA(launch_v2(p->type, MODE_TANGENT, p->precision, a, v2_args(p, static_cast<const double*>(df), false), s,
+                       p->tcfg[p->precision]),
              "assembly kernels");
   if ((rc = copy_out(vals, dv, vb, s))) return rc;
   if ((rc = copy_out(rhs, dr, rb, s))) return rc;

@@ -64,6 +64,7 @@ struct ElemArgs {
   const int32_t* node_eq0;    // [N] first free equation of the node (or -1)
   const double* prescribed;   // [3N]
   const uint16_t* slot;       // [E*n*n] column offset of node b inside node a's rows
+  const uint8_t* conn_mask;   // [E*n] node_mask of every element node
   // state (tangent mode), SoA [13][G]
   const double* state_c;
   double* state_t;
@@ -91,7 +92,7 @@ struct V2Args {
   int accumulate;           // add into vals / rhs / f_int instead of overwriting
 };
 // Launch shape of the two passes. tile: element-pass node-pair tile (0 = 2x4, 1 = 2x2,
-// 2 = 4x4; 1 and 2 in the linear pass only, 2 with FP32 accumulators only);
+// 2 = 4x4, the last in the linear pass with FP32 accumulators only);
 // *_blocks_per_sm: persistent grid per SM (0 = as many as are resident); p2_warps:
 // warps per row-gather block (0 = up to 8 as shared memory allows); passes: bit 0 the
 // element pass, bit 1 the row gather.
@@ -133,6 +134,7 @@ struct PatternOut {
   uint8_t* node_mask = nullptr;
   int32_t* node_eq0 = nullptr;
   uint16_t* slot = nullptr;     // [E*n*n]
+  uint8_t* conn_mask = nullptr; // [E*n] free-component mask of each element node
   // node -> incident elements, ascending element order: codes e*n + local node index
   int64_t* inc_ptr = nullptr;   // [N+1]
   int32_t* inc_code = nullptr;  // [E*n]

@@ -56,6 +56,14 @@ __global__ void check_numbering_kernel(const int32_t* dof_eq, const int32_t* sca
   }
 }
 
+// Free-component mask of every element node, so the row gather needs no connectivity
+// lookup before it knows which columns of a block exist.
+__global__ void conn_mask_kernel(const int32_t* conn, int64_t count, const uint8_t* node_mask, uint8_t* out) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = node_mask[conn[i]];
+}
+
 __global__ void node_info_kernel(const int32_t* dof_eq, int64_t n_nodes, uint8_t* mask,
                                  int32_t* eq0) {
   for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a < n_nodes;
@@ -357,6 +365,10 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
   CXG_TRY(dalloc(&out->row_ptr, static_cast<size_t>(n_free) + 1, &out->device_bytes));
   CXG_TRY(dalloc(&out->col_idx, static_cast<size_t>(out->nnz), &out->device_bytes));
   CXG_TRY(dalloc(&out->slot, static_cast<size_t>(P), &out->device_bytes));
+  CXG_TRY(dalloc(&out->conn_mask, static_cast<size_t>(n_elems) * npe, &out->device_bytes));
+  if (n_elems > 0)
+    conn_mask_kernel<<<grid_for(n_elems * npe), 256, 0, s>>>(d_conn, n_elems * npe, out->node_mask, out->conn_mask);
+  CXG_TRY(cudaGetLastError());
   row_ptr_kernel<<<grid_for(n_nodes), 256, 0, s>>>(n_nodes, out->node_mask, out->node_eq0, out->node_base,
                                                    out->node_rowlen, out->row_ptr);
   CXG_TRY(cudaGetLastError());

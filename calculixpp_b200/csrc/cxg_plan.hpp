@@ -34,7 +34,8 @@ struct cxg_plan {
   // staging buffers for host pointers, grown on demand and reused
   void* stage[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   size_t stage_bytes[6] = {0, 0, 0, 0, 0, 0};
-  cxg::LaunchCfg cfg[2];  // launch shape of the linear passes per precision (FP64, mixed)
+  cxg::LaunchCfg cfg[2];   // launch shape of the linear passes per precision (FP64, mixed)
+  cxg::LaunchCfg tcfg[2];  // launch shape of the material-point (tangent) passes
 };
 
 

@@ -534,37 +534,42 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
 }
 
 // ---- P2: row gather ------------------------------------------------------------------
-// Lanes map to (incident element in flight, column node lb of that element); EG
-// elements are in flight per pass (EG = 1 for 15/20-node families, 32/n otherwise).
-// Every lane issues its loads (connectivity, node mask, slot, the 9 block values)
-// independently, so a pass costs one round of memory latency, not a chain per column.
+// One warp per node a. Lanes form EG groups of GS lanes (GS = n rounded up to a power of
+// two); lane lb of group s handles column node lb of incident element k + s, so EG
+// elements are applied per pass. The node's incident-element codes come in with one
+// coalesced load per 32 elements and are handed out by shuffles; the free-component
+// mask of each column node comes from the per-element-node mask array, so one pass
+// waits for a single round of independent loads (slot, mask, the 9 block values); the
+// connectivity is read only for constrained columns. In mixed precision the diagonal
+// block of each element row is minus the FP64 sum of the row's off-diagonal FP32 blocks,
+// formed by a butterfly over the group's lanes.
 template <int ET>
 struct P2Geo {
   static constexpr int n = nodes_of(ET);
-  static constexpr int EG = n >= 16 ? 1 : 32 / n;
+  static constexpr int GS = n <= 8 ? 8 : (n <= 16 ? 16 : 32);
+  static constexpr int EG = 32 / GS;
 };
 
 template <int ET, bool TAN, typename R, bool DIAGFIX>
 __global__ void p2_kernel(ElemArgs A, V2Args V) {
   using G = Geo<ET>;
   constexpr int n = G::n, NB = G::NB;
-  constexpr int EG = P2Geo<ET>::EG;
+  constexpr int GS = P2Geo<ET>::GS, EG = P2Geo<ET>::EG;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t wstride = V.row_stride + (DIAGFIX ? 32 * 9 : 0);
-  double* buf = reinterpret_cast<double*>(smem) + static_cast<int64_t>(warp) * wstride;
-  double* part = buf + V.row_stride;  // [32][9] diagonal partials (mixed precision)
+  double* buf = reinterpret_cast<double*>(smem) + static_cast<int64_t>(warp) * V.row_stride;
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   const R* ed = reinterpret_cast<const R*>(V.edata);
-  const int sub = lane / n, lb = lane % n;
-  const bool lane_ok = sub < EG;
+  const int sub = lane / GS, lb = lane % GS;
+  const bool lane_ok = lb < n;
   for (int64_t a = gwarp; a < A.n_nodes; a += nwarps) {
     const int ma = A.node_mask[a];
     const int nf = __popc(ma);
     const int64_t L = A.node_rowlen[a];
     const int64_t total = nf * L;
     const int64_t base = A.node_base[a];
+    const int64_t i0 = V.inc_ptr[a], i1 = V.inc_ptr[a + 1];
     if (V.accumulate) {
       for (int64_t t = lane; t < total; t += 32) buf[t] = A.vals[base + t];
     } else {
@@ -573,27 +578,29 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
     __syncwarp();
     double rr[3] = {0.0, 0.0, 0.0};
     double fs[3] = {0.0, 0.0, 0.0};
-    const int64_t i0 = V.inc_ptr[a], i1 = V.inc_ptr[a + 1];
-    for (int64_t inc0 = i0; inc0 < i1; inc0 += EG) {
-      const int64_t inc = inc0 + sub;
-      const bool active = lane_ok && inc < i1;
-      if (active) {
-        const int code = V.inc_code[inc];
+    for (int64_t c0 = i0; c0 < i1; c0 += 32) {
+      const int cnt = static_cast<int>(i1 - c0 < 32 ? i1 - c0 : 32);
+      const int code_l = lane < cnt ? V.inc_code[c0 + lane] : 0;
+      for (int k = 0; k < cnt; k += EG) {
+        const int code = __shfl_sync(0xffffffffu, code_l, (k + sub) & 31);
+        const bool active = lane_ok && k + sub < cnt;
         const int64_t e = code / n;
         const int la = code % n;
-        const int64_t nb = A.conn[e * n + lb];
-        const int mb = A.node_mask[nb];
-        const int slotv = A.slot[(e * n + la) * n + lb];
-        const bool tr = lb < la;
-        const R* blk = ed + e * (NB * 9) + (tr ? blk_index(n, lb, la) : blk_index(n, la, lb)) * 9;
         double v[9];
+        int mb = 0, slotv = 0;
+        if (active) {
+          mb = A.conn_mask[e * n + lb];
+          slotv = A.slot[(e * n + la) * n + lb];
+          const bool tr = lb < la;
+          const R* blk = ed + e * (NB * 9) + (tr ? blk_index(n, lb, la) : blk_index(n, la, lb)) * 9;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = static_cast<double>(blk[tr ? 3 * (k % 3) + k / 3 : k]);
-        if (DIAGFIX) {
+          for (int q = 0; q < 9; ++q) v[q] = static_cast<double>(blk[tr ? 3 * (q % 3) + q / 3 : q]);
+        } else {
 #pragma unroll
-          for (int k = 0; k < 9; ++k) part[lane * 9 + k] = lb == la ? 0.0 : v[k];
+          for (int q = 0; q < 9; ++q) v[q] = 0.0;
         }
-        if (!DIAGFIX || lb != la) {
+        if (active && (!DIAGFIX || lb != la)) {
+          int64_t nb = -1;
 #pragma unroll
           for (int i = 0; i < 3; ++i) {
             if (!((ma >> i) & 1)) continue;
@@ -607,43 +614,50 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
                 else
                   *t += v[3 * i + j];
               } else {
+                if (nb < 0) nb = A.conn[e * n + lb];
                 const double pv = A.prescribed[3 * nb + j];
                 if (pv != 0.0) rr[i] -= v[3 * i + j] * pv;
               }
             }
           }
         }
-        if (TAN && lb == la) {
+        if (TAN && active && lb == la) {
 #pragma unroll
           for (int d = 0; d < 3; ++d) fs[d] += V.fdata[e * (3 * n) + 3 * la + d];
         }
-      }
-      if (DIAGFIX) {
-        __syncwarp();
-        for (int t = lane; t < EG * 9; t += 32) {
-          const int s = t / 9, ij = t % 9, i = ij / 3, j = ij % 3;
-          const int64_t incs = inc0 + s;
-          if (incs >= i1 || !((ma >> i) & 1)) continue;
-          double sum = 0.0;
-          for (int k = 0; k < n; ++k) sum += part[(s * n + k) * 9 + ij];
-          const int code = V.inc_code[incs];
-          const int64_t e = code / n;
-          const int la = code % n;
-          const double diag = -sum;
-          if ((ma >> j) & 1) {
-            double* tp = buf + __popc(ma & ((1 << i) - 1)) * L + A.slot[(e * n + la) * n + la] +
-                         __popc(ma & ((1 << j) - 1));
-            if (EG > 1)
-              atomicAdd(tp, diag);
-            else
-              *tp += diag;
-          } else {
-            const double pv = A.prescribed[3 * a + j];
-            if (pv != 0.0) rr[i] -= diag * pv;
+        if (DIAGFIX) {
+          // minus the sum of the element row's off-diagonal blocks, over the group's lanes
+          double d9[9];
+#pragma unroll
+          for (int q = 0; q < 9; ++q) {
+            double x = lb == la ? 0.0 : v[q];
+#pragma unroll
+            for (int off = GS / 2; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+            d9[q] = -x;
+          }
+          if (active && lb == la) {  // this lane's slot is slot(la, la)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+              if (!((ma >> i) & 1)) continue;
+              const int64_t row = __popc(ma & ((1 << i) - 1)) * L + slotv;
+#pragma unroll
+              for (int j = 0; j < 3; ++j) {
+                if ((ma >> j) & 1) {
+                  double* t = buf + row + __popc(ma & ((1 << j) - 1));
+                  if (EG > 1)
+                    atomicAdd(t, d9[3 * i + j]);
+                  else
+                    *t += d9[3 * i + j];
+                } else {
+                  const double pv = A.prescribed[3 * a + j];
+                  if (pv != 0.0) rr[i] -= d9[3 * i + j] * pv;
+                }
+              }
+            }
           }
         }
+        __syncwarp();
       }
-      __syncwarp();
     }
     if (A.rhs) {
 #pragma unroll
@@ -705,15 +719,13 @@ cudaError_t launch_p1_tile(const ElemArgs& a, const V2Args& v, const LaunchCfg& 
   return cudaGetLastError();
 }
 
-// Tile shapes instantiated: 2x4 everywhere; 2x2 and (FP32 accumulators only) 4x4 in
-// the linear pass, where the batched autotuner chooses among them.
+// Tile shapes instantiated: 2x4 and 2x2 everywhere, 4x4 in the linear pass with FP32
+// accumulators.
 template <int ET, int MODE, typename R>
 cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg, cudaStream_t s) {
-  if constexpr (MODE == MODE_LINEAR) {
-    if (cfg.tile == 1) return launch_p1_tile<ET, MODE, R, 1>(a, v, cfg, s);
-    if constexpr (sizeof(R) == 4) {
-      if (cfg.tile == 2) return launch_p1_tile<ET, MODE, R, 2>(a, v, cfg, s);
-    }
+  if (cfg.tile == 1) return launch_p1_tile<ET, MODE, R, 1>(a, v, cfg, s);
+  if constexpr (MODE == MODE_LINEAR && sizeof(R) == 4) {
+    if (cfg.tile == 2) return launch_p1_tile<ET, MODE, R, 2>(a, v, cfg, s);
   }
   if (cfg.tile != 0) return cudaErrorInvalidValue;
   return launch_p1_tile<ET, MODE, R, 0>(a, v, cfg, s);
@@ -725,7 +737,7 @@ cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaS
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
   // configured count when it fits)
   const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
-  const int64_t wbytes = (stride + (DF ? 32 * 9 : 0)) * 8;
+  const int64_t wbytes = stride * 8;
   int warps = cfg.p2_warps > 0 ? std::min(cfg.p2_warps, 32) : 8;
   while (warps > 1 && warps * wbytes > 160 * 1024) warps /= 2;
   const size_t smem = static_cast<size_t>(warps) * wbytes;

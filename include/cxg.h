@@ -140,6 +140,14 @@ CXG_API int cxg_plan_pattern_device(const cxg_plan* plan, const int64_t** row_pt
 CXG_API int cxg_plan_update_coords(cxg_plan* plan, const double* coords);
 /* Replace per-element Young's moduli [n_elems]. */
 CXG_API int cxg_plan_update_young(cxg_plan* plan, const double* young);
+/* Launch shape of the plan's two passes for the current precision; mode 0 = linear
+ * assembly, 1 = material-point (tangent) assembly. tile: node-pair tile of the element
+ * pass, 0 = 2x4 (default), 1 = 2x2, 2 = 4x4 (linear, mixed precision only);
+ * p1_blocks_per_sm: persistent grid of the element pass (0 = all resident);
+ * p2_warps: warps per row-gather block (0 = up to 8 as shared memory allows). Results
+ * do not depend on the shape. */
+CXG_API int cxg_plan_set_launch_config(cxg_plan* plan, int32_t mode, int32_t tile, int32_t p1_blocks_per_sm,
+                                       int32_t p2_warps);
 /* Synchronise the stream of the last launch and report the first in-kernel error
  * (CXG_ERR_NEGATIVE_JACOBIAN, CXG_ERR_UNKNOWN_NODE) with the offending element. */
 CXG_API int cxg_plan_check(cxg_plan* plan, int64_t* bad_element);

@@ -98,3 +98,27 @@ def test_state_roundtrip(cuda):
     s = np.random.default_rng(1).standard_normal((plan.n_gauss, 13))
     plan.set_state(s, committed=True)
     assert np.array_equal(to_np(plan.state(committed=True)), s)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("etype", ALL_TYPES)
+def test_launch_shapes_give_identical_bits(cuda, etype, precision):
+    """Every node-pair tile and grid shape of the element pass, and every row-gather
+    block size, produce the same bits in the tangent and in the linear assembly."""
+    quad = etype in (mg.C3D20, mg.C3D20R, mg.C3D15)
+    model = box_model(etype, *((2, 2, 2) if quad else (4, 3, 2)), jitter=0.08, seed=etype, materials=[J2_STEEL],
+                      load=False)
+    plan = Plan(model, precision)
+    u = displacement_field(model, 0.0012)
+    ref_t = [t.clone() for t in plan.assemble_tangent(u)]
+    ref_l = [t.clone() for t in plan.assemble_linear()]
+    tiles = (0, 1, 2) if precision == "mixed" else (0, 1)
+    for tile in tiles:
+        for bps, warps in ((0, 0), (1, 2), (2, 16)):
+            plan.set_launch_config(tangent=False, tile=tile, p1_blocks_per_sm=bps, p2_warps=warps)
+            assert all(bool((a == b).all()) for a, b in zip(plan.assemble_linear(), ref_l)), (tile, bps, warps)
+            if tile < 2:
+                plan.set_launch_config(tangent=True, tile=tile, p1_blocks_per_sm=bps, p2_warps=warps)
+                assert all(bool((a == b).all()) for a, b in zip(plan.assemble_tangent(u), ref_t)), (tile, bps, warps)
+    with pytest.raises(Exception):
+        plan.set_launch_config(tangent=True, tile=2)
