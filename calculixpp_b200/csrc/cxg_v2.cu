@@ -78,6 +78,41 @@ struct Geo {
 
 __host__ __device__ constexpr int blk_index(int n, int a, int b) { return a * n - a * (a - 1) / 2 + (b - a); }
 
+// Stored 3x3 blocks are padded to 16 bytes (10 doubles, 12 floats) so that they move
+// with 128-bit accesses.
+template <typename R>
+__host__ __device__ constexpr int blk_stride() { return sizeof(R) == 8 ? 10 : 12; }
+
+template <typename R>
+__device__ __forceinline__ void store_block(R* dst, const R (&v)[9]) {
+  if constexpr (sizeof(R) == 8) {
+    double2* d = reinterpret_cast<double2*>(dst);
+    d[0] = make_double2(v[0], v[1]);
+    d[1] = make_double2(v[2], v[3]);
+    d[2] = make_double2(v[4], v[5]);
+    d[3] = make_double2(v[6], v[7]);
+    d[4] = make_double2(v[8], 0.0);
+  } else {
+    float4* d = reinterpret_cast<float4*>(dst);
+    d[0] = make_float4(v[0], v[1], v[2], v[3]);
+    d[1] = make_float4(v[4], v[5], v[6], v[7]);
+    d[2] = make_float4(v[8], 0.f, 0.f, 0.f);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void load_block(const R* src, double (&v)[9]) {
+  if constexpr (sizeof(R) == 8) {
+    const double2* d = reinterpret_cast<const double2*>(src);
+    const double2 a = __ldg(d), b = __ldg(d + 1), c = __ldg(d + 2), e = __ldg(d + 3), f = __ldg(d + 4);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = e.x; v[7] = e.y; v[8] = f.x;
+  } else {
+    const float4* d = reinterpret_cast<const float4*>(src);
+    const float4 a = __ldg(d), b = __ldg(d + 1), c = __ldg(d + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w; v[8] = c.x;
+  }
+}
+
 __device__ __forceinline__ void hardening2(const J2Mat& M, double ep, double& sy, double& h) {
   const int n = M.n;
   if (n == 1 || ep <= M.ep[0]) {
@@ -481,7 +516,7 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
             }
           }
         }
-        R* out = reinterpret_cast<R*>(V.edata) + e * (NB * 9);
+        R* out = reinterpret_cast<R*>(V.edata) + e * (NB * blk_stride<R>());
 #pragma unroll
         for (int i = 0; i < TR; ++i)
 #pragma unroll
@@ -494,9 +529,10 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
                 for (int al = 0; al < 4; ++al) hd += W.gam[ei][al * 8 + a] * W.gam[ei][al * 8 + b];
                 h = static_cast<R>(hd * W.kappa[ei]);
               }
-              R* blk = out + blk_index(n, a, b) * 9;
+              R bv[9];
 #pragma unroll
-              for (int k = 0; k < 9; ++k) blk[k] = acc[i][j][k] + ((k % 4 == 0) ? h : R(0));
+              for (int k = 0; k < 9; ++k) bv[k] = acc[i][j][k] + ((k % 4 == 0) ? h : R(0));
+              store_block<R>(out + blk_index(n, a, b) * blk_stride<R>(), bv);
             }
           }
       }
@@ -536,13 +572,15 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
 // ---- P2: row gather ------------------------------------------------------------------
 // One warp per node a. Lanes form EG groups of GS lanes (GS = n rounded up to a power of
 // two); lane lb of group s handles column node lb of incident element k + s, so EG
-// elements are applied per pass. The node's incident-element codes come in with one
-// coalesced load per 32 elements and are handed out by shuffles; the free-component
-// mask of each column node comes from the per-element-node mask array, so one pass
-// waits for a single round of independent loads (slot, mask, the 9 block values); the
-// connectivity is read only for constrained columns. In mixed precision the diagonal
-// block of each element row is minus the FP64 sum of the row's off-diagonal FP32 blocks,
-// formed by a butterfly over the group's lanes.
+// elements are applied per pass. Each group adds into its own copy of the node's rows
+// in shared memory (within one element every target is distinct, so plain adds, no
+// atomics); the copies are summed in a fixed order when the rows are stored. The
+// node's incident-element codes come in with one coalesced load per 32 elements and
+// are handed out by shuffles; the free-component mask of each column node comes from
+// the per-element-node mask array; the next pass's loads are issued before the current
+// pass is applied. The connectivity is read only for constrained columns. In mixed
+// precision the diagonal block of each element row is minus the FP64 sum of the row's
+// off-diagonal FP32 blocks, formed by a butterfly over the group's lanes.
 template <int ET>
 struct P2Geo {
   static constexpr int n = nodes_of(ET);
@@ -550,19 +588,53 @@ struct P2Geo {
   static constexpr int EG = 32 / GS;
 };
 
+
+template <typename R>
+struct P2Pass {
+  double v[9];
+  int64_t e;
+  int la, mb, slotv;
+  bool active;
+};
+
+template <int ET, typename R>
+__device__ __forceinline__ void p2_fetch(const ElemArgs& A, const R* ed, int code, bool active, int lb, P2Pass<R>& p) {
+  constexpr int n = nodes_of(ET), NB = n * (n + 1) / 2;
+  p.active = active;
+  p.e = code / n;
+  p.la = code % n;
+  if (active) {
+    p.mb = __ldg(A.conn_mask + p.e * n + lb);
+    p.slotv = __ldg(A.slot + (p.e * n + p.la) * n + lb);
+    const bool tr = lb < p.la;
+    double raw[9];
+    load_block<R>(ed + p.e * (NB * blk_stride<R>()) +
+                      (tr ? blk_index(n, lb, p.la) : blk_index(n, p.la, lb)) * blk_stride<R>(),
+                  raw);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p.v[q] = tr ? raw[3 * (q % 3) + q / 3] : raw[q];
+  } else {
+    p.mb = 0;
+    p.slotv = 0;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p.v[q] = 0.0;
+  }
+}
+
 template <int ET, bool TAN, typename R, bool DIAGFIX>
 __global__ void p2_kernel(ElemArgs A, V2Args V) {
-  using G = Geo<ET>;
-  constexpr int n = G::n, NB = G::NB;
+  constexpr int n = nodes_of(ET);
   constexpr int GS = P2Geo<ET>::GS, EG = P2Geo<ET>::EG;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* buf = reinterpret_cast<double*>(smem) + static_cast<int64_t>(warp) * V.row_stride;
+  const int64_t stride = V.row_stride;
+  double* buf = reinterpret_cast<double*>(smem) + static_cast<int64_t>(warp) * (EG * stride);
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   const R* ed = reinterpret_cast<const R*>(V.edata);
   const int sub = lane / GS, lb = lane % GS;
   const bool lane_ok = lb < n;
+  double* mine = buf + sub * stride;
   for (int64_t a = gwarp; a < A.n_nodes; a += nwarps) {
     const int ma = A.node_mask[a];
     const int nf = __popc(ma);
@@ -570,84 +642,64 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
     const int64_t total = nf * L;
     const int64_t base = A.node_base[a];
     const int64_t i0 = V.inc_ptr[a], i1 = V.inc_ptr[a + 1];
-    if (V.accumulate) {
-      for (int64_t t = lane; t < total; t += 32) buf[t] = A.vals[base + t];
-    } else {
-      for (int64_t t = lane; t < total; t += 32) buf[t] = 0.0;
-    }
+    for (int g = 0; g < EG; ++g)
+      for (int64_t t = lane; t < total; t += 32)
+        buf[g * stride + t] = (g == 0 && V.accumulate) ? A.vals[base + t] : 0.0;
     __syncwarp();
     double rr[3] = {0.0, 0.0, 0.0};
     double fs[3] = {0.0, 0.0, 0.0};
     for (int64_t c0 = i0; c0 < i1; c0 += 32) {
       const int cnt = static_cast<int>(i1 - c0 < 32 ? i1 - c0 : 32);
-      const int code_l = lane < cnt ? V.inc_code[c0 + lane] : 0;
+      const int code_l = lane < cnt ? __ldg(V.inc_code + c0 + lane) : 0;
+      P2Pass<R> cur;
+      p2_fetch<ET, R>(A, ed, __shfl_sync(0xffffffffu, code_l, sub & 31), lane_ok && sub < cnt, lb, cur);
       for (int k = 0; k < cnt; k += EG) {
-        const int code = __shfl_sync(0xffffffffu, code_l, (k + sub) & 31);
-        const bool active = lane_ok && k + sub < cnt;
-        const int64_t e = code / n;
-        const int la = code % n;
-        double v[9];
-        int mb = 0, slotv = 0;
-        if (active) {
-          mb = A.conn_mask[e * n + lb];
-          slotv = A.slot[(e * n + la) * n + lb];
-          const bool tr = lb < la;
-          const R* blk = ed + e * (NB * 9) + (tr ? blk_index(n, lb, la) : blk_index(n, la, lb)) * 9;
-#pragma unroll
-          for (int q = 0; q < 9; ++q) v[q] = static_cast<double>(blk[tr ? 3 * (q % 3) + q / 3 : q]);
-        } else {
-#pragma unroll
-          for (int q = 0; q < 9; ++q) v[q] = 0.0;
-        }
-        if (active && (!DIAGFIX || lb != la)) {
+        // issue the next pass's loads first
+        const int kn = k + EG;
+        const int code_n = __shfl_sync(0xffffffffu, code_l, (kn + sub) & 31);
+        P2Pass<R> nxt;
+        p2_fetch<ET, R>(A, ed, code_n, lane_ok && kn + sub < cnt, lb, nxt);
+        if (cur.active && (!DIAGFIX || lb != cur.la)) {
           int64_t nb = -1;
 #pragma unroll
           for (int i = 0; i < 3; ++i) {
             if (!((ma >> i) & 1)) continue;
-            const int64_t row = __popc(ma & ((1 << i) - 1)) * L + slotv;
+            const int64_t row = __popc(ma & ((1 << i) - 1)) * L + cur.slotv;
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-              if ((mb >> j) & 1) {
-                double* t = buf + row + __popc(mb & ((1 << j) - 1));
-                if (EG > 1)
-                  atomicAdd(t, v[3 * i + j]);
-                else
-                  *t += v[3 * i + j];
+              if ((cur.mb >> j) & 1) {
+                mine[row + __popc(cur.mb & ((1 << j) - 1))] += cur.v[3 * i + j];
               } else {
-                if (nb < 0) nb = A.conn[e * n + lb];
+                if (nb < 0) nb = A.conn[cur.e * n + lb];
                 const double pv = A.prescribed[3 * nb + j];
-                if (pv != 0.0) rr[i] -= v[3 * i + j] * pv;
+                if (pv != 0.0) rr[i] -= cur.v[3 * i + j] * pv;
               }
             }
           }
         }
-        if (TAN && active && lb == la) {
+        if (TAN && cur.active && lb == cur.la) {
 #pragma unroll
-          for (int d = 0; d < 3; ++d) fs[d] += V.fdata[e * (3 * n) + 3 * la + d];
+          for (int d = 0; d < 3; ++d) fs[d] += __ldg(V.fdata + cur.e * (3 * n) + 3 * cur.la + d);
         }
         if (DIAGFIX) {
-          // minus the sum of the element row's off-diagonal blocks, over the group's lanes
+          // minus the sum of the element row's off-diagonal blocks, butterfly over the group
           double d9[9];
 #pragma unroll
           for (int q = 0; q < 9; ++q) {
-            double x = lb == la ? 0.0 : v[q];
+            double x = lb == cur.la ? 0.0 : cur.v[q];
 #pragma unroll
             for (int off = GS / 2; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
             d9[q] = -x;
           }
-          if (active && lb == la) {  // this lane's slot is slot(la, la)
+          if (cur.active && lb == cur.la) {  // this lane's slot is slot(la, la)
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
               if (!((ma >> i) & 1)) continue;
-              const int64_t row = __popc(ma & ((1 << i) - 1)) * L + slotv;
+              const int64_t row = __popc(ma & ((1 << i) - 1)) * L + cur.slotv;
 #pragma unroll
               for (int j = 0; j < 3; ++j) {
                 if ((ma >> j) & 1) {
-                  double* t = buf + row + __popc(ma & ((1 << j) - 1));
-                  if (EG > 1)
-                    atomicAdd(t, d9[3 * i + j]);
-                  else
-                    *t += d9[3 * i + j];
+                  mine[row + __popc(ma & ((1 << j) - 1))] += d9[3 * i + j];
                 } else {
                   const double pv = A.prescribed[3 * a + j];
                   if (pv != 0.0) rr[i] -= d9[3 * i + j] * pv;
@@ -657,6 +709,7 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
           }
         }
         __syncwarp();
+        cur = nxt;
       }
     }
     if (A.rhs) {
@@ -679,7 +732,12 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
         if (lane == 0) A.f_int[3 * a + d] = (V.accumulate ? A.f_int[3 * a + d] : 0.0) + v;
       }
     }
-    for (int64_t t = lane; t < total; t += 32) A.vals[base + t] = buf[t];
+    for (int64_t t = lane; t < total; t += 32) {
+      double v = buf[t];
+#pragma unroll
+      for (int g = 1; g < EG; ++g) v += buf[g * stride + t];
+      A.vals[base + t] = v;
+    }
     __syncwarp();
   }
 }
@@ -737,7 +795,7 @@ cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaS
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
   // configured count when it fits)
   const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
-  const int64_t wbytes = stride * 8;
+  const int64_t wbytes = P2Geo<ET>::EG * stride * 8;
   int warps = cfg.p2_warps > 0 ? std::min(cfg.p2_warps, 32) : 8;
   while (warps > 1 && warps * wbytes > 160 * 1024) warps /= 2;
   const size_t smem = static_cast<size_t>(warps) * wbytes;
@@ -774,7 +832,8 @@ cudaError_t launch_v2_type(int mode, int precision, const ElemArgs& a, const V2A
 
 size_t v2_edata_bytes(int t, int64_t n_elems, int precision) {
   const int n = nodes_of(t);
-  return static_cast<size_t>(n_elems) * (n * (n + 1) / 2) * 9 * (precision ? 4 : 8);
+  return static_cast<size_t>(n_elems) * (n * (n + 1) / 2) *
+         (precision ? blk_stride<float>() * sizeof(float) : blk_stride<double>() * sizeof(double));
 }
 
 cudaError_t launch_v2(int t, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s,
