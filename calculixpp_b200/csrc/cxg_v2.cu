@@ -275,7 +275,26 @@ struct P1Smem {
 };
 
 template <int ET, int MODE, typename R, int TILE>
-__global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
+constexpr size_t p1_smem_bytes() {
+  using WS = P1Smem<ET, MODE, R, TILE>;
+  constexpr int n = nodes_of(ET), nq = gauss_of(ET);
+  return (sizeof(double) * (n * 3 * nq + nq) + 15) / 16 * 16 + kW1 * ((sizeof(WS) + 15) / 16 * 16);
+}
+
+// Resident blocks per SM the element pass asks the register allocator for: as many as
+// its shared memory allows, at most 3 (<= 170 registers per thread) for the tiles whose
+// accumulators fit that budget without spilling (2x2, and 2x4 in FP32), else 2 (no
+// limit below the 255-register ceiling).
+template <int ET, int MODE, typename R, int TILE>
+constexpr int p1_min_blocks() {
+  constexpr size_t per_sm = 227 * 1024;
+  constexpr int by_smem = static_cast<int>(per_sm / (p1_smem_bytes<ET, MODE, R, TILE>() + 1024));
+  constexpr int cap = (TILE == 1 || (TILE == 0 && sizeof(R) == 4)) ? 3 : 2;
+  return by_smem < 1 ? 1 : (by_smem > cap ? cap : by_smem);
+}
+
+template <int ET, int MODE, typename R, int TILE>
+__global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_kernel(ElemArgs A, V2Args V) {
   using G = Geo<ET, TILE>;
   constexpr int n = G::n, nq = G::nq, npad = G::npad, EPW = G::EPW, NT = G::NT, NB = G::NB;
   constexpr int TR = G::TR, TC = G::TC;
@@ -577,8 +596,8 @@ __global__ void __launch_bounds__(kT1) p1_kernel(ElemArgs A, V2Args V) {
 // atomics); the copies are summed in a fixed order when the rows are stored. The
 // node's incident-element codes come in with one coalesced load per 32 elements and
 // are handed out by shuffles; the free-component mask of each column node comes from
-// the per-element-node mask array; the next pass's loads are issued before the current
-// pass is applied. The connectivity is read only for constrained columns. In mixed
+// the per-element-node mask array, so a pass waits for one round of independent loads.
+// The connectivity is read only for constrained columns. In mixed
 // precision the diagonal block of each element row is minus the FP64 sum of the row's
 // off-diagonal FP32 blocks, formed by a butterfly over the group's lanes.
 template <int ET>
@@ -651,14 +670,9 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
     for (int64_t c0 = i0; c0 < i1; c0 += 32) {
       const int cnt = static_cast<int>(i1 - c0 < 32 ? i1 - c0 : 32);
       const int code_l = lane < cnt ? __ldg(V.inc_code + c0 + lane) : 0;
-      P2Pass<R> cur;
-      p2_fetch<ET, R>(A, ed, __shfl_sync(0xffffffffu, code_l, sub & 31), lane_ok && sub < cnt, lb, cur);
       for (int k = 0; k < cnt; k += EG) {
-        // issue the next pass's loads first
-        const int kn = k + EG;
-        const int code_n = __shfl_sync(0xffffffffu, code_l, (kn + sub) & 31);
-        P2Pass<R> nxt;
-        p2_fetch<ET, R>(A, ed, code_n, lane_ok && kn + sub < cnt, lb, nxt);
+        P2Pass<R> cur;
+        p2_fetch<ET, R>(A, ed, __shfl_sync(0xffffffffu, code_l, (k + sub) & 31), lane_ok && k + sub < cnt, lb, cur);
         if (cur.active && (!DIAGFIX || lb != cur.la)) {
           int64_t nb = -1;
 #pragma unroll
@@ -709,7 +723,6 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
           }
         }
         __syncwarp();
-        cur = nxt;
       }
     }
     if (A.rhs) {
@@ -758,10 +771,7 @@ int64_t persistent_grid(int64_t need, int resident, int blocks_per_sm) {
 
 template <int ET, int MODE, typename R, int TILE>
 cudaError_t launch_p1_tile(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg, cudaStream_t s) {
-  using WS = P1Smem<ET, MODE, R, TILE>;
-  constexpr int n = nodes_of(ET), nq = gauss_of(ET);
-  constexpr size_t cta_bytes = (sizeof(double) * (n * 3 * nq + nq) + 15) / 16 * 16;
-  constexpr size_t smem = cta_bytes + kW1 * ((sizeof(WS) + 15) / 16 * 16);
+  constexpr size_t smem = p1_smem_bytes<ET, MODE, R, TILE>();
   static_assert(smem <= 227 * 1024, "element pass shared memory");
   auto kern = p1_kernel<ET, MODE, R, TILE>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
