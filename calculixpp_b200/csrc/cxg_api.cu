@@ -419,7 +419,7 @@ int cxg_plan_update_young(cxg_plan* p, const double* young) {
 int cxg_plan_set_launch_config(cxg_plan* p, int32_t mode, int32_t tile, int32_t p1_blocks_per_sm, int32_t p2_warps) {
   if (!p || (mode != 0 && mode != 1)) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad plan or mode");
   if (tile < 0 || tile > 2 || (tile == 2 && (mode == 1 || p->precision == CXG_FP64)) || p1_blocks_per_sm < 0 ||
-      p2_warps < 0 || p2_warps > 32)
+      p2_warps < 0 || p2_warps > 8)
     return set_err(CXG_ERR_INVALID_ARGUMENT, "bad launch shape (4x4 tiles: linear pass, mixed precision only)");
   LaunchCfg& c = mode ? p->tcfg[p->precision] : p->cfg[p->precision];
   c.tile = tile;

@@ -579,7 +579,7 @@ int cxg_batch_tune(cxg_batch* b, double* vals, double* rhs, const double* f_ext,
         }
       }
     best.p2_ms = 1e30;
-    for (int warps : {2, 4, 8, 16}) {
+    for (int warps : {2, 4, 8}) {
       LaunchCfg c;
       c.p2_warps = warps;
       c.passes = 2;
@@ -625,7 +625,7 @@ int cxg_batch_group_config(const cxg_batch* b, int32_t gi, int32_t* type, int32_
 
 int cxg_batch_set_group_config(cxg_batch* b, int32_t gi, int32_t tile, int32_t p1, int32_t warps) {
   if (!b || gi < 0 || gi >= static_cast<int32_t>(b->groups.size())) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad group");
-  if (tile < 0 || tile > 2 || (tile == 2 && b->precision == CXG_FP64) || p1 < 0 || warps < 0 || warps > 32)
+  if (tile < 0 || tile > 2 || (tile == 2 && b->precision == CXG_FP64) || p1 < 0 || warps < 0 || warps > 8)
     return set_err(CXG_ERR_INVALID_ARGUMENT, "bad launch shape (4x4 tiles need mixed precision)");
   LaunchCfg& c = b->groups[static_cast<size_t>(gi)].plan->cfg[b->precision];
   c.tile = tile;

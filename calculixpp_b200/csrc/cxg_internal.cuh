@@ -94,7 +94,7 @@ struct V2Args {
 // Launch shape of the two passes. tile: element-pass node-pair tile (0 = 2x4, 1 = 2x2,
 // 2 = 4x4, the last in the linear pass with FP32 accumulators only);
 // *_blocks_per_sm: persistent grid per SM (0 = as many as are resident); p2_warps:
-// warps per row-gather block (0 = up to 8 as shared memory allows); passes: bit 0 the
+// warps per row-gather block, at most 8 (0 = up to 8 as shared memory allows); passes: bit 0 the
 // element pass, bit 1 the row gather.
 struct LaunchCfg {
   int tile = 0;

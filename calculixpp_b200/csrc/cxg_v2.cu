@@ -597,9 +597,11 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 // node's incident-element codes come in with one coalesced load per 32 elements and
 // are handed out by shuffles; the free-component mask of each column node comes from
 // the per-element-node mask array, so a pass waits for one round of independent loads.
-// The connectivity is read only for constrained columns. In mixed
-// precision the diagonal block of each element row is minus the FP64 sum of the row's
-// off-diagonal FP32 blocks, formed by a butterfly over the group's lanes.
+// The connectivity is read only for constrained columns. In mixed precision the
+// diagonal 3x3 block of node a is minus the FP64 sum of all off-diagonal FP32 blocks of
+// its element rows: every lane keeps a running sum of the blocks it adds, and one
+// butterfly over the warp per node forms the block, so rigid translations stay in the
+// null space of the assembled rows to FP64 accuracy.
 template <int ET>
 struct P2Geo {
   static constexpr int n = nodes_of(ET);
@@ -641,7 +643,7 @@ __device__ __forceinline__ void p2_fetch(const ElemArgs& A, const R* ed, int cod
 }
 
 template <int ET, bool TAN, typename R, bool DIAGFIX>
-__global__ void p2_kernel(ElemArgs A, V2Args V) {
+__device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   constexpr int n = nodes_of(ET);
   constexpr int GS = P2Geo<ET>::GS, EG = P2Geo<ET>::EG;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -667,6 +669,10 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
     __syncwarp();
     double rr[3] = {0.0, 0.0, 0.0};
     double fs[3] = {0.0, 0.0, 0.0};
+    double dsum[9];  // this lane's FP64 sum of the off-diagonal blocks it added (DIAGFIX)
+#pragma unroll
+    for (int q = 0; q < 9; ++q) dsum[q] = 0.0;
+    int slot_aa = 0;  // column offset of node a in its own rows
     for (int64_t c0 = i0; c0 < i1; c0 += 32) {
       const int cnt = static_cast<int>(i1 - c0 < 32 ? i1 - c0 : 32);
       const int code_l = lane < cnt ? __ldg(V.inc_code + c0 + lane) : 0;
@@ -695,35 +701,45 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
 #pragma unroll
           for (int d = 0; d < 3; ++d) fs[d] += __ldg(V.fdata + cur.e * (3 * n) + 3 * cur.la + d);
         }
-        if (DIAGFIX) {
-          // minus the sum of the element row's off-diagonal blocks, butterfly over the group
-          double d9[9];
+        if (DIAGFIX && cur.active) {
+          if (lb != cur.la) {
 #pragma unroll
-          for (int q = 0; q < 9; ++q) {
-            double x = lb == cur.la ? 0.0 : cur.v[q];
-#pragma unroll
-            for (int off = GS / 2; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
-            d9[q] = -x;
-          }
-          if (cur.active && lb == cur.la) {  // this lane's slot is slot(la, la)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              if (!((ma >> i) & 1)) continue;
-              const int64_t row = __popc(ma & ((1 << i) - 1)) * L + cur.slotv;
-#pragma unroll
-              for (int j = 0; j < 3; ++j) {
-                if ((ma >> j) & 1) {
-                  mine[row + __popc(ma & ((1 << j) - 1))] += d9[3 * i + j];
-                } else {
-                  const double pv = A.prescribed[3 * a + j];
-                  if (pv != 0.0) rr[i] -= d9[3 * i + j] * pv;
-                }
-              }
-            }
+            for (int q = 0; q < 9; ++q) dsum[q] += cur.v[q];
+          } else {
+            slot_aa = cur.slotv;  // slot(la, la)
           }
         }
         __syncwarp();
       }
+    }
+    if (DIAGFIX) {
+      // diagonal block of node a: minus the FP64 sum of every off-diagonal FP32 block
+      // added to its rows, reduced over the warp in a fixed order
+      double d9[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        double x = dsum[q];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+        d9[q] = -x;
+      }
+      slot_aa = static_cast<int>(__reduce_max_sync(0xffffffffu, static_cast<unsigned>(slot_aa)));
+      if (lane < 9 && i1 > i0) {
+        const int i = lane / 3, j = lane % 3;
+        double d = d9[0];
+#pragma unroll
+        for (int q = 1; q < 9; ++q)
+          if (q == lane) d = d9[q];
+        if ((ma >> i) & 1) {
+          if ((ma >> j) & 1) {
+            buf[__popc(ma & ((1 << i) - 1)) * L + slot_aa + __popc(ma & ((1 << j) - 1))] += d;
+          } else {
+            const double pv = A.prescribed[3 * a + j];
+            if (pv != 0.0) rr[i] -= d * pv;
+          }
+        }
+      }
+      __syncwarp();
     }
     if (A.rhs) {
 #pragma unroll
@@ -753,6 +769,19 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
     }
     __syncwarp();
   }
+}
+
+// Blocks of at most 8 warps. The mixed-precision gather of the <= 8-node families is
+// compiled for 3 resident blocks per SM (<= 85 registers), which its short rows leave
+// room for in shared memory; the other gathers are compiled without a register budget.
+template <int ET, bool TAN, typename R, bool DIAGFIX>
+__global__ void p2_kernel(ElemArgs A, V2Args V) {
+  p2_body<ET, TAN, R, DIAGFIX>(A, V);
+}
+
+template <int ET, bool TAN, typename R, bool DIAGFIX>
+__global__ void __launch_bounds__(256, 3) p2_kernel_short(ElemArgs A, V2Args V) {
+  p2_body<ET, TAN, R, DIAGFIX>(A, V);
 }
 
 int sm_count() {
@@ -801,12 +830,12 @@ cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg
 
 template <int ET, bool TAN, typename R, bool DF>
 cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaStream_t s) {
-  auto kern = p2_kernel<ET, TAN, R, DF>;
+  auto kern = (DF && nodes_of(ET) <= 8) ? p2_kernel_short<ET, TAN, R, DF> : p2_kernel<ET, TAN, R, DF>;
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
   // configured count when it fits)
   const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
   const int64_t wbytes = P2Geo<ET>::EG * stride * 8;
-  int warps = cfg.p2_warps > 0 ? std::min(cfg.p2_warps, 32) : 8;
+  int warps = cfg.p2_warps > 0 ? std::min(cfg.p2_warps, 8) : 8;
   while (warps > 1 && warps * wbytes > 160 * 1024) warps /= 2;
   const size_t smem = static_cast<size_t>(warps) * wbytes;
   if (smem > 220 * 1024) return cudaErrorInvalidConfiguration;

@@ -144,7 +144,7 @@ CXG_API int cxg_plan_update_young(cxg_plan* plan, const double* young);
  * assembly, 1 = material-point (tangent) assembly. tile: node-pair tile of the element
  * pass, 0 = 2x4 (default), 1 = 2x2, 2 = 4x4 (linear, mixed precision only);
  * p1_blocks_per_sm: persistent grid of the element pass (0 = all resident);
- * p2_warps: warps per row-gather block (0 = up to 8 as shared memory allows). Results
+ * p2_warps: warps per row-gather block, 1 to 8 (0 = up to 8 as shared memory allows). Results
  * do not depend on the shape. */
 CXG_API int cxg_plan_set_launch_config(cxg_plan* plan, int32_t mode, int32_t tile, int32_t p1_blocks_per_sm,
                                        int32_t p2_warps);
