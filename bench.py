@@ -207,6 +207,7 @@ def j2_newton(args, world, dev, stream):
     (v64, f64, s64), (vm, fm, sm) = keep["fp64"], keep["mixed"]
     yielded = float((s64[:, 6] > 0).double().mean())
     B = j2_algorithmic_bytes(plan, model)
+    traffic = json.load(open(TRAFFIC_FILE)) if os.path.exists(TRAFFIC_FILE) else {}
     peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
     ach = B / (out["fp64"]["ms_per_step"] * 1e-3) / 1e9
@@ -221,6 +222,8 @@ def j2_newton(args, world, dev, stream):
                         "f_int_rel_l2": float(torch.linalg.norm(fm - f64) / torch.linalg.norm(f64)),
                         "state_max_abs": float((sm - s64).abs().max())},
         "roofline_fp64": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                          "traffic": traffic.get(f"c3d8_j2_{args.j2_n}_fp64_tangent"),
+                          "kernel": "p1_kernel + p2_kernel (element pass with J2 return + row gather), C3D8 tangent, FP64",
                           "algorithmic_bytes": B, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "gpu_launches_per_step": 2,
     }
