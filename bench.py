@@ -1,19 +1,24 @@
 """Benchmark: element-integrations/s of the element-integration + CSR assembly path.
 
-Workload (default): the C3D20 full-integration (27-point) linear-elastic block, 64^3
-quadratic hexes of a unit cube (262,144 elements, 1,085,825 nodes, 3,257,475 DOF,
-557,286,921 CSR non-zeros), node jitter uniform +-0.05 h, per-element E lognormal
-(median 200000, sigma 0.3), nu 0.3, z=0 face clamped. Synthetic and seeded.
+Headline workload (`value`): the C3D20 full-integration (27-point) linear-elastic block,
+64^3 quadratic hexes of a unit cube (262,144 elements, 1,085,825 nodes, 3,219,840 free
+DOF, 550,501,596 CSR values), node jitter uniform +-0.05 h, per-element E lognormal
+(median 200000, sigma 0.3), nu 0.3, z=0 face clamped. Synthetic and seeded. One step =
+one assembly of K_ff and the rhs (every element integrated, every CSR value written
+once). `value` = mixed precision (FP32 blocks, FP64 Jacobians and accumulation),
+inputs resident in HBM; the FP64 path is timed in the same run ("fp64"). e2e = the same
+through the C ABI with host buffers (load vector in, K_ff + rhs out every step).
 
-One step = one assembly of K_ff and the rhs (vals zeroed, rhs from the load vector,
-every element integrated and scattered). `value` = mixed precision (FP32 integration,
-FP64 Jacobians and accumulation) element-integrations/s with all inputs resident in
-HBM; the FP64 path is measured in the same run ("fp64"). e2e = the same through the
-C ABI with host buffers: the load vector copied in and K_ff + rhs copied out each step.
+Further sections of the same JSON line:
+  j2_newton  C3D8 128^3 J2 block, residual + consistent tangent of the last increment of a
+             graded uniaxial ramp (~40 % of Gauss points yielding), FP64 and mixed;
+  batched    256 independent models of five element types in one CUDA graph, autotuned;
+  adjoint    C3D8 96x96x48 cantilever: device CG solve, then dc/dE and dc/dX per step;
+  cpu_baseline  the reference's own element routine on the host cores (oracle/_ref).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--n 64]
-Multi-GPU (torchrun): every rank assembles its own block (weak scaling, no collective
-on the data path); timing is max over ranks.
+Multi-GPU (torchrun): every rank assembles its own workloads (weak scaling, no
+collective on the data path); timing is max over ranks.
 """
 from __future__ import annotations
 
@@ -47,6 +52,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--j2-n", type=int, default=128, help="cells per axis of the C3D8 J2 block (0: skip)")
     ap.add_argument("--batch-models", type=int, default=256, help="models of the batched workload (0: skip)")
+    ap.add_argument("--adj-n", type=int, default=96, help="cells along x and y of the adjoint cantilever (0: skip)")
     return ap.parse_args()
 
 
@@ -312,6 +318,65 @@ def batched(args, world, rank, dev, stream):
     return res
 
 
+def adjoint_section(args, world, dev, stream):
+    """Compliance sensitivities of the C3D8 cantilever: assembly + device CG solve once,
+    then the adjoint kernel (dc/dE per element, dc/dX per node) timed per step. Checks at
+    full size: sum_e E_e dc/dE_e = -c, sum_nodes dc/dX = 0, sum X.dc/dX = -c."""
+    import ctypes as C
+
+    import torch
+
+    from calculixpp_b200 import Plan, _lib
+    from calculixpp_b200 import meshgen as mg
+    from calculixpp_b200.assembly import Material, Model
+    nx = args.adj_n
+    cfg = mg.adjoint_cantilever(nx, nx, nx // 2)
+    m = cfg["mesh"]
+    model = Model(m, [Material(210000.0, 0.3)], None, cfg["spc"], cfg["cloads"])
+    plan = Plan(model, "fp64")
+    f = torch.as_tensor(model.external_load_vector(), device=dev)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    vals, rhs = plan.assemble_linear(f)
+    s0.record(stream)
+    x, iters, rel = plan.solve_cg(vals, rhs, rtol=1e-10, max_iter=100000)
+    s1.record(stream)
+    s1.synchronize()
+    t_solve = s0.elapsed_time(s1) * 1e-3
+    c = float(torch.dot(rhs, x))
+    u = plan.expand(x)
+    dE = torch.empty(m.n_elems, dtype=torch.float64, device=dev)
+    dX = torch.empty(3 * m.n_nodes, dtype=torch.float64, device=dev)
+    lib = _lib.load()
+    vp = C.c_void_p
+
+    def step():
+        _lib.check(lib.cxg_adjoint_compliance(plan.h, vp(u.data_ptr()), vp(dE.data_ptr()), vp(dX.data_ptr()),
+                                              vp(stream.cuda_stream)))
+
+    for _ in range(args.warmup):
+        step()
+    plan.check()
+    torch.cuda.synchronize()
+    barrier(world)
+    t = max_over_ranks(time_steps(step, args.steps, stream), world)
+    plan.check()
+    E = torch.as_tensor(m.young, device=dev)
+    X = torch.as_tensor(m.coords, device=dev).reshape(-1)
+    res = {"workload": f"C3D8 cantilever {nx}x{nx}x{nx // 2}, E = 2.1e5 rho^3, rho ~ U[0.1, 1], x=0 clamped, tip load",
+           "elements": m.n_elems, "n_free": plan.n_free,
+           "solve": {"kind": "Jacobi-PCG on the device", "rtol": 1e-10, "iterations": iters, "rel_residual": rel,
+                     "seconds": t_solve},
+           "adjoint": {"value": world * m.n_elems * args.steps / t, "unit": "element-integrations/s",
+                       "ms_per_step": t / args.steps * 1e3},
+           "identities": {"sum_E_dcdE_plus_c_rel": abs(float(E @ dE) + c) / abs(c),
+                          "sum_dcdX_rel": float(dX.view(-1, 3).sum(0).abs().max() / dX.abs().sum()),
+                          "sum_X_dcdX_plus_c_rel": abs(float(X @ dX) + c) / abs(c)}}
+    del vals, rhs, x, u, dE, dX
+    plan.close()
+    torch.cuda.empty_cache()
+    return res
+
+
 def algorithmic_bytes(plan, model):
     """Compulsory bytes of one linear assembly launch: connectivity, node coordinates,
     per-element E and nu read once, every K_ff value written once."""
@@ -504,6 +569,7 @@ def main():
     torch.cuda.empty_cache()
     j2 = j2_newton(args, world, dev, stream) if args.j2_n > 0 else None
     batch = batched(args, world, rank, dev, stream) if args.batch_models > 0 else None
+    adj = adjoint_section(args, world, dev, stream) if args.adj_n > 0 else None
 
     # accuracy of the mixed path against FP64 on a reduced block (host sparse solve)
     acc = None
@@ -558,6 +624,7 @@ def main():
                      "algorithmic_bytes": B, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "j2_newton": j2,
         "batched": batch,
+        "adjoint": adj,
         "cpu_baseline": cpu,
         "e2e": {"value": world * E * e2e_steps / t_e2e, "unit": "element-integrations/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -294,3 +294,17 @@ def batched_workload(n_models=256, min_elems=1000, max_elems=200000, seed=0, typ
         m, spc, top = batch_box(etype, ne, 0.1, seed * 100003 + k, E, nu)
         out.append((m, spc, top, E, nu))
     return out
+
+
+def adjoint_cantilever(nx=96, ny=96, nz=48, seed=0, E0=210000.0, nu=0.3, load=-1000.0):
+    """Adjoint-sensitivity workload: nx*ny*nz C3D8 cantilever of unit cells, per-element
+    E = E0 * rho^3 with rho ~ U[0.1, 1] (seeded), x=0 face clamped, total load `load` in
+    z spread evenly over the nodes of the x = nx face."""
+    m = box_mesh(C3D8, nx, ny, nz, float(nx), float(ny), float(nz), jitter=0.0, seed=seed)
+    rho = np.random.default_rng(seed).uniform(0.1, 1.0, m.n_elems)
+    m.young = E0 * rho ** 3
+    m.poisson = np.full(m.n_elems, nu)
+    spc = clamp_face_spc(m, 0, 0.0)
+    tip = face_nodes(m, 0, float(nx))
+    return {"mesh": m, "spc": spc, "cloads": (tip, np.full(tip.size, 2), np.full(tip.size, load / tip.size)),
+            "rho": rho}

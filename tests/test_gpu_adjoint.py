@@ -134,3 +134,21 @@ def test_adjoint_rejects_reduced_hex(cuda):
     with pytest.raises(CxgError) as exc:
         plan.adjoint_compliance(np.zeros(3 * plan.model.mesh.n_nodes))
     assert exc.value.code == 5
+
+
+def test_adjoint_identities(cuda):
+    """Size-independent checks of the adjoint, used at full size by the bench:
+    K is linear in E, so sum_e E_e dc/dE_e = -c; a rigid translation of every node leaves
+    c unchanged, so sum_nodes dc/dX = 0; K scales like the length in 3-D elasticity, so
+    sum X . dc/dX = -c."""
+    model = cantilever_rho(8, 4, 3, seed=3)
+    plan = Plan(model)
+    f = model.external_load_vector()
+    x, rhs = host_solution(plan, f)
+    c = float(x @ rhs)
+    u = to_np(plan.expand(torch.as_tensor(x, device=plan.device)))
+    dE, dX = (to_np(t) for t in plan.adjoint_compliance(u))
+    X = model.mesh.coords
+    assert abs(float(model.mesh.young @ dE) + c) <= 1e-10 * abs(c)
+    assert np.abs(dX.reshape(-1, 3).sum(0)).max() <= 1e-9 * np.abs(dX).sum()
+    assert abs(float((X.reshape(-1) * dX.reshape(-1)).sum()) + c) <= 1e-9 * abs(c)
