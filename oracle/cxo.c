@@ -889,6 +889,142 @@ cxo_system* cxo_assemble_tangent(int64_t n_nodes, const double* coords, int64_t 
                   prescribed, n_free, f_ext, u, sc, st, f_int);
 }
 
+/* ---- mass and geometric (initial-stress) stiffness ------------------------------ */
+/* element_mass, src/fem/element.cpp:786-812: M[3a+d][3b+d] += (rho detJ w) N_a N_b. */
+int cxo_element_mass(int type, const double* x, double rho, double* Me) {
+  const int n = cxo_nodes_per_element(type);
+  if (n == 0) return fail("unsupported element type");
+  const int ndof = 3 * n;
+  memset(Me, 0, sizeof(double) * (size_t)ndof * (size_t)ndof);
+  if (rho == 0.0) return 0;
+  double gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det;
+  const int ng = cxo_gauss_rule(type, gp);
+  for (int q = 0; q < ng; ++q) {
+    cxo_shape(type, gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
+    if (gradients_from_shape(n, dN, x, g, &det)) return -1;
+    const double scale = rho * det * gp[4 * q + 3];
+    for (int a = 0; a < n; ++a)
+      for (int b = 0; b < n; ++b) {
+        const double m = scale * N[a] * N[b];
+        for (int d = 0; d < 3; ++d) Me[(3 * a + d) * ndof + 3 * b + d] += m;
+      }
+  }
+  return 0;
+}
+
+/* element_mass_lumped, element.cpp:814-831: the diagonal takes the row sum of the
+ * consistent mass. */
+int cxo_element_mass_lumped(int type, const double* x, double rho, double* Ml) {
+  const int n = cxo_nodes_per_element(type);
+  if (n == 0) return fail("unsupported element type");
+  const int ndof = 3 * n;
+  double Mc[60 * 60];
+  if (cxo_element_mass(type, x, rho, Mc)) return -1;
+  memset(Ml, 0, sizeof(double) * (size_t)ndof * (size_t)ndof);
+  for (int i = 0; i < ndof; ++i) {
+    double row = 0.0;
+    for (int j = 0; j < ndof; ++j) row += Mc[i * ndof + j];
+    Ml[i * ndof + i] = row;
+  }
+  return 0;
+}
+
+/* element_geometric_stiffness + accumulate_kgeo, element.cpp:482-508, 833-854:
+ * K[3a+d][3b+d] += (detJ w) (g_a . sigma . g_b) on the upper triangle, then mirrored.
+ * gp_stress holds one Voigt6 per Gauss point (may be NULL: zero field). */
+int cxo_element_geometric_stiffness(int type, const double* x, const double* gp_stress, double* Ke) {
+  const int n = cxo_nodes_per_element(type);
+  if (n == 0) return fail("unsupported element type");
+  const int ndof = 3 * n;
+  memset(Ke, 0, sizeof(double) * (size_t)ndof * (size_t)ndof);
+  double gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det;
+  const int ng = cxo_gauss_rule(type, gp);
+  for (int q = 0; q < ng; ++q) {
+    cxo_shape(type, gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
+    if (gradients_from_shape(n, dN, x, g, &det)) return -1;
+    static const double zero6[6] = {0, 0, 0, 0, 0, 0};
+    const double* sg = gp_stress ? gp_stress + 6 * q : zero6;
+    const double scale = det * gp[4 * q + 3];
+    for (int a = 0; a < n; ++a) {
+      const double* ga = g + 3 * a;
+      for (int b = a; b < n; ++b) {
+        const double* gb = g + 3 * b;
+        const double senergy = sg[0] * ga[0] * gb[0] + sg[1] * ga[1] * gb[1] + sg[2] * ga[2] * gb[2] +
+                               sg[3] * (ga[0] * gb[1] + ga[1] * gb[0]) +
+                               sg[4] * (ga[0] * gb[2] + ga[2] * gb[0]) +
+                               sg[5] * (ga[1] * gb[2] + ga[2] * gb[1]);
+        const double v = scale * senergy;
+        for (int d = 0; d < 3; ++d) {
+          const int ia = 3 * a + d, ib = 3 * b + d;
+          if (ib >= ia) Ke[ia * ndof + ib] += v;
+        }
+      }
+    }
+  }
+  mirror_upper(ndof, Ke);
+  return 0;
+}
+
+/* assemble_mass / assemble_geometric_stiffness, src/fem/assembly.cpp:259-331: the same
+ * SPC-only scatter as the stiffness with the rhs side effect discarded (the returned
+ * rhs is zero). kind 1: consistent mass, 2: lumped mass, 3: geometric stiffness.
+ * density[E] per element (kinds 1, 2); gp_stress[6 * G] (kind 3, element order). */
+cxo_system* cxo_assemble_scalar(int kind, int64_t n_nodes, const double* coords, int64_t n_elems,
+                                const int32_t* types, const int64_t* conn_ptr, const int32_t* conn,
+                                const double* density, const double* gp_stress, const int32_t* dof_eq,
+                                const double* prescribed, int32_t n_free) {
+  triplets_t t = {0};
+  double* rhs = calloc((size_t)n_free + 1, sizeof(double));
+  double* dummy = calloc((size_t)n_free + 1, sizeof(double));
+  double x[3 * MAXN], Ke[60 * 60];
+  int64_t gd[60];
+  int64_t gp_off = 0;
+  for (int64_t e = 0; e < n_elems; ++e) {
+    const int type = types[e];
+    const int n = cxo_nodes_per_element(type);
+    if (n == 0 || conn_ptr[e + 1] - conn_ptr[e] != n) {
+      fail("unsupported element type or bad connectivity length");
+      goto error;
+    }
+    const int32_t* c = conn + conn_ptr[e];
+    for (int k = 0; k < n; ++k) {
+      if (c[k] < 0 || c[k] >= n_nodes) {
+        fail("element references unknown node");
+        goto error;
+      }
+      for (int d = 0; d < 3; ++d) {
+        x[3 * k + d] = coords[3 * (int64_t)c[k] + d];
+        gd[3 * k + d] = 3 * (int64_t)c[k] + d;
+      }
+    }
+    double gpb[4 * 27];
+    const int ng = cxo_gauss_rule(type, gpb);
+    int rc;
+    if (kind == 1)
+      rc = cxo_element_mass(type, x, density[e], Ke);
+    else if (kind == 2)
+      rc = cxo_element_mass_lumped(type, x, density[e], Ke);
+    else
+      rc = cxo_element_geometric_stiffness(type, x, gp_stress ? gp_stress + 6 * gp_off : NULL, Ke);
+    if (rc) goto error;
+    gp_off += ng;
+    if (scatter(Ke, 3 * n, gd, dof_eq, prescribed, n_free, &t, dummy)) goto error;
+  }
+  free(dummy);
+  {
+    cxo_system* s = finish(&t, n_free, rhs);
+    if (!s) goto error2;
+    return s;
+  }
+error:
+  free(dummy);
+error2:
+  free(t.key);
+  free(t.val);
+  free(rhs);
+  return NULL;
+}
+
 int cxo_system_info(const cxo_system* s, int32_t* n_free, int64_t* nnz) {
   *n_free = s->n_free;
   *nnz = s->nnz;

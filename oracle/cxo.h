@@ -82,6 +82,19 @@ cxo_system* cxo_assemble_tangent(int64_t n_nodes, const double* coords, int64_t 
                                  const double* state_committed, double* state_trial,
                                  double* f_int);
 
+/* element_mass / element_mass_lumped / element_geometric_stiffness
+ * (include/calculixpp/fem/element.hpp:93-118): dense 3n x 3n. gp_stress[6 * points]. */
+int cxo_element_mass(int type, const double* coords, double rho, double* Me);
+int cxo_element_mass_lumped(int type, const double* coords, double rho, double* Ml);
+int cxo_element_geometric_stiffness(int type, const double* coords, const double* gp_stress, double* Ke);
+
+/* assemble_mass (kind 1 consistent, 2 lumped) and assemble_geometric_stiffness (kind 3),
+ * src/fem/assembly.cpp:259-331; the rhs of the returned system is zero. */
+cxo_system* cxo_assemble_scalar(int kind, int64_t n_nodes, const double* coords, int64_t n_elems,
+                                const int32_t* types, const int64_t* conn_ptr, const int32_t* conn,
+                                const double* density, const double* gp_stress, const int32_t* dof_eq,
+                                const double* prescribed, int32_t n_free);
+
 int cxo_system_info(const cxo_system* s, int32_t* n_free, int64_t* nnz);
 int cxo_system_copy(const cxo_system* s, int64_t* row_ptr, int32_t* col_idx,
                     double* vals, double* rhs);

@@ -123,6 +123,29 @@ class _Base:
         self._check(f(int(etype), _p(_f64(coords)), float(E), float(nu), _p(Ke)))
         return Ke.reshape(3 * n, 3 * n)
 
+    def element_mass(self, etype, coords, rho, lumped=False):
+        """element_mass / element_mass_lumped (element.hpp:93-102)."""
+        n = NODES[etype]
+        M = np.zeros((3 * n) ** 2)
+        if self.prefix == "ref":
+            f = self._fn("element_mass")
+            f.argtypes = [C.c_int, _vp, C.c_double, C.c_int, _vp]
+            self._check(f(int(etype), _p(_f64(coords)), float(rho), int(lumped), _p(M)))
+        else:
+            f = self._fn("element_mass_lumped" if lumped else "element_mass")
+            f.argtypes = [C.c_int, _vp, C.c_double, _vp]
+            self._check(f(int(etype), _p(_f64(coords)), float(rho), _p(M)))
+        return M.reshape(3 * n, 3 * n)
+
+    def element_geometric_stiffness(self, etype, coords, gp_stress):
+        """element_geometric_stiffness (element.hpp:117-119); gp_stress (points, 6)."""
+        n = NODES[etype]
+        K = np.zeros((3 * n) ** 2)
+        f = self._fn("element_geometric_stiffness")
+        f.argtypes = [C.c_int, _vp, _vp, _vp]
+        self._check(f(int(etype), _p(_f64(coords)), _p(_f64(gp_stress)), _p(K)))
+        return K.reshape(3 * n, 3 * n)
+
     def material_evaluate(self, mat, strain, committed=None):
         committed = np.zeros(13) if committed is None else _f64(committed)
         trial = np.zeros(13)
@@ -205,6 +228,24 @@ class Port(_Base):
               _p(trial), _p(f_int))
         rp, ci, v, rhs = self._system(s)
         return rp, ci, v, rhs, f_int, trial
+
+    def assemble_scalar(self, kind, mesh, dof_eq, prescribed, n_free, density=None, gp_stress=None):
+        """assemble_mass (kind "mass" / "lumped") or assemble_geometric_stiffness
+        (kind "geometric") as canonical CSR (rp, ci, vals); density per element,
+        gp_stress (G, 6) in element order."""
+        E = mesh.n_elems
+        n = mesh.conn.shape[1]
+        types = np.full(E, mesh.etype, dtype=np.int32)
+        conn_ptr = np.arange(E + 1, dtype=np.int64) * n
+        f = self._fn("assemble_scalar")
+        f.restype = _vp
+        f.argtypes = [C.c_int, C.c_int64, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32]
+        code = {"mass": 1, "lumped": 2, "geometric": 3}[kind]
+        s = f(code, mesh.n_nodes, _p(_f64(mesh.coords)), E, _p(types), _p(conn_ptr), _p(_i32(mesh.conn.ravel())),
+              _p(None if density is None else _f64(density)), _p(None if gp_stress is None else _f64(gp_stress)),
+              _p(_i32(dof_eq)), _p(_f64(prescribed)), int(n_free))
+        rp, ci, v, _ = self._system(s)
+        return rp, ci, v
 
     def element_compliance_grad_fd(self, etype, coords, ue, E, nu, h):
         n = NODES[etype]
@@ -319,6 +360,22 @@ class RefModel:
     def assemble_linear_static(self):
         """Returns the reference LinearSystem (COO in hash-map order) as a dict."""
         return self._take(self.ref._fn("assemble_linear_static")(_vp(self.h)))
+
+    def set_density(self, rho_per_material):
+        rho = _f64(rho_per_material)
+        self.ref._check(self.ref.lib.ref_model_set_density(_vp(self.h), C.c_int32(rho.size), _p(rho)))
+
+    def assemble_mass(self, lumped=False):
+        f = self.ref._fn("assemble_mass")
+        f.restype = _vp
+        f.argtypes = [_vp, C.c_int]
+        return self._take(f(_vp(self.h), int(lumped)))
+
+    def assemble_geometric(self, gp_stress):
+        f = self.ref._fn("assemble_geometric")
+        f.restype = _vp
+        f.argtypes = [_vp, _vp]
+        return self._take(f(_vp(self.h), _p(_f64(gp_stress))))
 
     def material_points(self):
         lib = self.ref.lib

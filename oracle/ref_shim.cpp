@@ -307,6 +307,83 @@ void* ref_model_create(int64_t n_nodes, const double* coords, int64_t n_elems,
 
 void ref_model_free(void* model) { delete static_cast<RefModel*>(model); }
 
+// element_mass (lumped = 0) / element_mass_lumped (lumped = 1), element.hpp:93-102.
+int ref_element_mass(int type, const double* coords, double rho, int lumped, double* Me) {
+  try {
+    const ElementType t = static_cast<ElementType>(type);
+    const int n = nodes_per_element(t);
+    std::vector<Vec3> x(static_cast<std::size_t>(n));
+    for (int k = 0; k < n; ++k) x[static_cast<std::size_t>(k)] = {coords[3 * k], coords[3 * k + 1], coords[3 * k + 2]};
+    const std::vector<Real> M = lumped ? element_mass_lumped(t, x, rho) : element_mass(t, x, rho);
+    std::memcpy(Me, M.data(), M.size() * sizeof(double));
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// element_geometric_stiffness, element.hpp:117-119; gp_stress[6 * points] (Voigt6).
+int ref_element_geometric_stiffness(int type, const double* coords, const double* gp_stress, double* Ke) {
+  try {
+    const ElementType t = static_cast<ElementType>(type);
+    const int n = nodes_per_element(t);
+    std::vector<Vec3> x(static_cast<std::size_t>(n));
+    for (int k = 0; k < n; ++k) x[static_cast<std::size_t>(k)] = {coords[3 * k], coords[3 * k + 1], coords[3 * k + 2]};
+    const std::size_t ng = gauss_rule(t).size();
+    std::vector<Voigt6> sg(ng);
+    for (std::size_t q = 0; q < ng; ++q)
+      for (int c = 0; c < 6; ++c) sg[q][static_cast<std::size_t>(c)] = gp_stress[6 * q + c];
+    const std::vector<Real> K = element_geometric_stiffness(t, x, sg);
+    std::memcpy(Ke, K.data(), K.size() * sizeof(double));
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// Per-material density (Material::density) of a model built by ref_model_create.
+int ref_model_set_density(void* model, int32_t n_mats, const double* rho) {
+  try {
+    Model& m = static_cast<RefModel*>(model)->model;
+    for (int32_t k = 0; k < n_mats; ++k) {
+      auto it = m.materials.find("M" + std::to_string(k));
+      if (it != m.materials.end()) it->second.density = rho[k];
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// assemble_mass (assembly.cpp:259-298).
+void* ref_assemble_mass(void* model, int lumped) {
+  try {
+    return new LinearSystem(assemble_mass(static_cast<RefModel*>(model)->model, lumped != 0));
+  } catch (const std::exception& e) {
+    fail(e);
+    return nullptr;
+  }
+}
+
+// assemble_geometric_stiffness (assembly.cpp:300-331); gp_stress[6 * G], element order.
+void* ref_assemble_geometric(void* model, const double* gp_stress) {
+  try {
+    const Model& m = static_cast<RefModel*>(model)->model;
+    std::vector<std::vector<Voigt6>> sg(m.mesh.num_elements());
+    std::size_t off = 0;
+    for (std::size_t e = 0; e < m.mesh.num_elements(); ++e) {
+      const std::size_t ng = gauss_rule(m.mesh.elements()[e].type).size();
+      sg[e].resize(ng);
+      for (std::size_t q = 0; q < ng; ++q, ++off)
+        for (int c = 0; c < 6; ++c) sg[e][q][static_cast<std::size_t>(c)] = gp_stress[6 * off + c];
+    }
+    return new LinearSystem(assemble_geometric_stiffness(m, sg));
+  } catch (const std::exception& e) {
+    fail(e);
+    return nullptr;
+  }
+}
+
 void* ref_assemble_linear_static(void* model) {
   try {
     auto* sys = new LinearSystem(assemble_linear_static(static_cast<RefModel*>(model)->model));

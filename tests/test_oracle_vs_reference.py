@@ -134,3 +134,39 @@ def test_assemble_material_tangent_identical(port, ref, etype):
         rm.commit()
         committed = st2
     assert np.any(committed.reshape(-1, 13)[:, 6] > 0)
+
+
+@pytest.mark.parametrize("etype", ALL_TYPES)
+def test_element_mass_and_geometric_identical(port, ref, etype):
+    rng = np.random.default_rng(300 + etype)
+    for x in distorted_elements(etype, 4, seed=etype + 40, amp=0.1):
+        for lumped in (False, True):
+            assert np.array_equal(port.element_mass(etype, x, 7.85e-9, lumped),
+                                  ref.element_mass(etype, x, 7.85e-9, lumped))
+        s = rng.normal(0.0, 100.0, (mg.NGP[etype], 6))
+        assert np.array_equal(port.element_geometric_stiffness(etype, x, s),
+                              ref.element_geometric_stiffness(etype, x, s))
+
+
+@pytest.mark.parametrize("etype", ALL_TYPES)
+def test_assemble_mass_and_geometric_identical(port, ref, etype):
+    """assemble_mass (consistent and lumped) and assemble_geometric_stiffness
+    (src/fem/assembly.cpp:259-331) against the reference's own drivers."""
+    quad = etype in (mg.C3D20, mg.C3D20R, mg.C3D15)
+    dims = (2, 2, 1) if quad else (3, 2, 2)
+    n_el = mg.box_mesh(etype, *dims).n_elems
+    E = np.random.default_rng(etype).uniform(70e3, 210e3, n_el)
+    model = box_model(etype, *dims, jitter=0.1, seed=etype, young=E, prescribe=0.01)
+    mats, em = per_element_materials(model)
+    rho_mat = 7.85e-9 * (1.0 + 0.1 * np.arange(len(mats)))
+    rm = ref.model(model.mesh, mats, em, model.spc, model.cloads)
+    rm.set_density(rho_mat)
+    dof_eq, pre, nf = model.dof_map()
+    gs = np.random.default_rng(etype + 1).normal(0.0, 50.0, (n_el * mg.NGP[etype], 6))
+    for kind in ("mass", "lumped", "geometric"):
+        s = rm.assemble_geometric(gs) if kind == "geometric" else rm.assemble_mass(kind == "lumped")
+        rp, ci, v = coo_to_csr(s["n_free"], s["rows"], s["cols"], s["vals"])
+        rp2, ci2, v2 = port.assemble_scalar(kind, model.mesh, dof_eq, pre, nf, density=rho_mat[em], gp_stress=gs)
+        assert np.array_equal(rp, rp2) and np.array_equal(ci, ci2), kind
+        assert np.array_equal(v, v2), kind
+        assert not np.any(s["rhs"]), kind
