@@ -87,6 +87,8 @@ SIGNATURES = {
     "cxg_assemble_linear": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "cxg_assemble_linear_ex": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int32, _vp]),
     "cxg_assemble_tangent": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "cxg_assemble_mass": (C.c_int, [_vp, _vp, C.c_int32, _vp, _vp]),
+    "cxg_assemble_geometric": (C.c_int, [_vp, _vp, _vp, _vp]),
     "cxg_state_get": (C.c_int, [_vp, C.c_int32, _vp]),
     "cxg_state_set": (C.c_int, [_vp, C.c_int32, _vp]),
     "cxg_state_commit": (C.c_int, [_vp, _vp]),

@@ -251,6 +251,28 @@ class Plan:
                 self.check()
         return vals, f_int, rhs
 
+    def assemble_mass(self, density, lumped=False, vals=None, check=True):
+        """Mass matrix M_ff on the plan's pattern (assemble_mass, src/fem/assembly.cpp:259-298);
+        density per element."""
+        vals = torch.empty(self.nnz, dtype=torch.float64, device=self.device) if vals is None else vals
+        d = _dev(density, torch.float64, self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_assemble_mass(self.h, _ptr(d), int(bool(lumped)), _ptr(vals), _stream()))
+            if check:
+                self.check()
+        return vals
+
+    def assemble_geometric_stiffness(self, gp_stress, vals=None, check=True):
+        """Initial-stress stiffness K_geo on the plan's pattern (assemble_geometric_stiffness,
+        src/fem/assembly.cpp:300-331); gp_stress (n_gauss, 6) Voigt per Gauss point."""
+        vals = torch.empty(self.nnz, dtype=torch.float64, device=self.device) if vals is None else vals
+        sg = None if gp_stress is None else _dev(gp_stress, torch.float64, self.device).reshape(-1)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_assemble_geometric(self.h, _ptr(sg), _ptr(vals), _stream()))
+            if check:
+                self.check()
+        return vals
+
     # -- material state -------------------------------------------------------------
     def state(self, committed=True):
         out = torch.empty(self.n_gauss * 13, dtype=torch.float64, device=self.device)

@@ -499,6 +499,56 @@ int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_i
   return CXG_OK;
 }
 
+namespace {
+
+// The scalar-block operators (mass, geometric stiffness) on the FP64 element buffer
+// and the FP64 row gather; the rhs side effect of prescribed columns is discarded, as
+// in the reference (src/fem/assembly.cpp:286-288, 320-322).
+int assemble_scalar(cxg_plan* p, int kind, const double* input, size_t input_bytes, double* vals, void* stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
+  void *dv, *din = nullptr;
+  int rc = staged(p, 0, vals, vb, false, s, &dv);
+  if (!rc && input) rc = staged(p, 5, input, input_bytes, true, s, &din);
+  if (rc) return rc;
+  const size_t need = v2_edata_bytes(p->type, p->n_elems, CXG_FP64);
+  if (p->edata_bytes < need) {
+    cudaFree(p->edata);
+    p->edata = nullptr;
+    p->device_bytes -= static_cast<int64_t>(p->edata_bytes);
+    p->edata_bytes = 0;
+    CHECK_CUDA(cudaMalloc(&p->edata, std::max<size_t>(need, 16)), "element buffer");
+    p->edata_bytes = need;
+    p->device_bytes += static_cast<int64_t>(need);
+  }
+  ElemArgs a = base_args(p);
+  a.vals = static_cast<double*>(dv);
+  a.rhs = nullptr;
+  const V2Args v = v2_args(p, nullptr, false);
+  const double* d = static_cast<const double*>(din);
+  CHECK_CUDA(launch_scalar_pass(p->type, kind, a, v, kind == 3 ? nullptr : d, kind == 3 ? d : nullptr, s),
+             "element pass");
+  LaunchCfg gather_only;
+  gather_only.passes = 2;
+  CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, CXG_FP64, a, v, s, gather_only), "row gather");
+  if ((rc = copy_out(vals, dv, vb, s))) return rc;
+  if (dv != vals) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
+  return CXG_OK;
+}
+
+}  // namespace
+
+int cxg_assemble_mass(cxg_plan* p, const double* density, int32_t lumped, double* vals, void* stream) {
+  if (!p || !density || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, density and vals are required");
+  return assemble_scalar(p, lumped ? 2 : 1, density, sizeof(double) * static_cast<size_t>(p->n_elems), vals, stream);
+}
+
+int cxg_assemble_geometric(cxg_plan* p, const double* gp_stress, double* vals, void* stream) {
+  if (!p || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan and vals are required");
+  return assemble_scalar(p, 3, gp_stress, sizeof(double) * 6 * static_cast<size_t>(p->n_gauss), vals, stream);
+}
+
 int cxg_state_get(const cxg_plan* cp, int32_t slot, double* out) {
   auto* p = const_cast<cxg_plan*>(cp);
   if (!p || !out || (slot != 0 && slot != 1)) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");

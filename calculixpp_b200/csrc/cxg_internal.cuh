@@ -42,6 +42,15 @@ constexpr int dn_offset(int t) {
 }
 constexpr int kDnTotal = dn_offset(C3D15) + dn_size(C3D15);
 extern __constant__ double c_dN[kDnTotal];
+// Shape-function values N[k][q] (Gauss point fastest) of every family.
+constexpr int nn_size(int t) { return nodes_of(t) * gauss_of(t); }
+constexpr int nn_offset(int t) {
+  int off = 0;
+  for (int u = C3D8; u < t; ++u) off += nn_size(u);
+  return off;
+}
+constexpr int kNTotal = nn_offset(C3D15) + nn_size(C3D15);
+extern __constant__ double c_N[kNTotal];
 extern __constant__ double c_w[8][kMaxGauss];
 
 // Everything an element-integration launch reads or writes. Pointers are device
@@ -104,6 +113,12 @@ struct LaunchCfg {
   int passes = 3;
 };
 size_t v2_edata_bytes(int elem_type, int64_t n_elems, int precision);
+// Element pass of the scalar-block operators (every 3x3 block is a scalar times I):
+// kind 1 consistent mass rho N_a N_b, 2 lumped mass (row sums on the diagonal), 3
+// geometric stiffness g_a . sigma . g_b. Writes FP64 blocks for the FP64 row gather.
+// density[E] (kinds 1, 2), gp_stress[6 G] (kind 3).
+cudaError_t launch_scalar_pass(int elem_type, int kind, const ElemArgs& a, const V2Args& v, const double* density,
+                               const double* gp_stress, cudaStream_t s);
 cudaError_t launch_v2(int elem_type, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s,
                       const LaunchCfg& cfg = LaunchCfg{});
 

@@ -32,6 +32,7 @@ namespace cxg {
 
 __constant__ double c_dN[kDnTotal];
 __constant__ double c_w[8][kMaxGauss];
+__constant__ double c_N[kNTotal];
 
 namespace {
 
@@ -659,7 +660,7 @@ cudaError_t ensure_tables() {
   if (err != cudaSuccess) return err;
   std::lock_guard<std::mutex> lock(g_tables_mu);
   if (static_cast<int>(g_tables_ready.size()) > dev && g_tables_ready[dev]) return cudaSuccess;
-  std::vector<double> dn(kDnTotal, 0.0);
+  std::vector<double> dn(kDnTotal, 0.0), nv(kNTotal, 0.0);
   double w[8][kMaxGauss] = {};
   for (int t = C3D8; t <= C3D15; ++t) {
     GaussPt pts[kMaxGauss];
@@ -668,14 +669,18 @@ cudaError_t ensure_tables() {
     for (int q = 0; q < nq; ++q) {
       double N[kMaxNodes], d[kMaxNodes][3];
       shape_derivatives(t, pts[q].xi, pts[q].et, pts[q].ze, N, d);
-      for (int k = 0; k < n; ++k)
+      for (int k = 0; k < n; ++k) {
         for (int j = 0; j < 3; ++j) dn[dn_offset(t) + (3 * k + j) * nq + q] = d[k][j];
+        nv[nn_offset(t) + k * nq + q] = N[k];
+      }
       w[t][q] = pts[q].w;
     }
   }
   err = cudaMemcpyToSymbol(c_dN, dn.data(), sizeof(double) * kDnTotal);
   if (err != cudaSuccess) return err;
   err = cudaMemcpyToSymbol(c_w, w, sizeof(w));
+  if (err != cudaSuccess) return err;
+  err = cudaMemcpyToSymbol(c_N, nv.data(), sizeof(double) * kNTotal);
   if (err != cudaSuccess) return err;
   if (static_cast<int>(g_tables_ready.size()) <= dev) g_tables_ready.resize(dev + 1, 0);
   g_tables_ready[dev] = 1;

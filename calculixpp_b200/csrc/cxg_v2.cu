@@ -867,6 +867,141 @@ cudaError_t launch_v2_type(int mode, int precision, const ElemArgs& a, const V2A
   return precision ? launch_p2_t<ET, true, float, true>(a, v, c, s) : launch_p2_t<ET, true, double, false>(a, v, c, s);
 }
 
+// ---- scalar-block element pass (mass, geometric stiffness) ---------------------------
+// Every 3x3 block of these operators is a scalar times I: m_ab = sum_q rho detJ w N_a N_b
+// (element_mass, src/fem/element.cpp:786-812), its row sums on the diagonal for the
+// lumped mass (element.cpp:814-831), k_ab = sum_q detJ w g_a . sigma_q . g_b
+// (element_geometric_stiffness + accumulate_kgeo, element.cpp:482-508, 833-854). One
+// warp per element: lanes take Gauss points for detJ (and the gradients), then node
+// pairs (a <= b) for the scalar sums; the blocks go to the FP64 element buffer the row
+// gather reads.
+constexpr int kScalarWarps = 4;
+
+template <int ET, int KIND>
+constexpr int scalar_warp_doubles() {
+  constexpr int n = nodes_of(ET), nq = gauss_of(ET);
+  return 3 * n + nq + (KIND == 3 ? nq * n * 3 + nq * 6 : 0);
+}
+
+template <int ET, int KIND>
+__global__ void __launch_bounds__(kScalarWarps * 32) scalar_kernel(ElemArgs A, V2Args V, const double* density,
+                                                                   const double* gp_stress) {
+  constexpr int n = nodes_of(ET), nq = gauss_of(ET), NB = n * (n + 1) / 2;
+  constexpr bool GEO = KIND == 3;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ unsigned char s_pa[NB], s_pb[NB];
+  for (int p = threadIdx.x; p < NB; p += blockDim.x) {
+    int a = 0, r = p;
+    while (r >= n - a) {
+      r -= n - a;
+      ++a;
+    }
+    s_pa[p] = static_cast<unsigned char>(a);
+    s_pb[p] = static_cast<unsigned char>(a + r);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* x = reinterpret_cast<double*>(smem) + warp * scalar_warp_doubles<ET, KIND>();
+  double* sq = x + 3 * n;   // [nq] rho detJ w (mass) or detJ w (geometric)
+  double* g = sq + nq;      // [nq][n][3] physical gradients (geometric)
+  double* sig = g + nq * n * 3;  // [nq][6] stress (geometric)
+  const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * kScalarWarps + warp;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kScalarWarps;
+  for (int64_t e = gwarp; e < A.n_elems; e += nwarps) {
+    for (int t = lane; t < 3 * n; t += 32) x[t] = A.coords[3 * static_cast<int64_t>(A.conn[e * n + t / 3]) + t % 3];
+    __syncwarp();
+    for (int q = lane; q < nq; q += 32) {
+      double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int k = 0; k < n; ++k)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) J[i][j] += x[3 * k + i] * c_dN[dn_offset(ET) + (3 * k + j) * nq + q];
+      const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+      const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+      const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+      const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+      if (!(det > 0.0)) {
+        atomicCAS(&A.status->code, 0, 4);
+        atomicMin(&A.status->bad_elem, static_cast<unsigned long long>(e));
+      }
+      if (!GEO) {
+        sq[q] = density[e] * det * c_w[ET][q];
+      } else {
+        sq[q] = det * c_w[ET][q];
+        const double inv = 1.0 / det;
+        const double it[3][3] = {
+            {c00 * inv, c01 * inv, c02 * inv},
+            {(J[0][2] * J[2][1] - J[0][1] * J[2][2]) * inv, (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * inv,
+             (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * inv},
+            {(J[0][1] * J[1][2] - J[0][2] * J[1][1]) * inv, (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * inv,
+             (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * inv}};
+        for (int k = 0; k < n; ++k) {
+          const double d0 = c_dN[dn_offset(ET) + (3 * k) * nq + q], d1 = c_dN[dn_offset(ET) + (3 * k + 1) * nq + q],
+                       d2 = c_dN[dn_offset(ET) + (3 * k + 2) * nq + q];
+          for (int i = 0; i < 3; ++i) g[(q * n + k) * 3 + i] = it[i][0] * d0 + it[i][1] * d1 + it[i][2] * d2;
+        }
+        for (int c = 0; c < 6; ++c) sig[q * 6 + c] = gp_stress ? gp_stress[(e * nq + q) * 6 + c] : 0.0;
+      }
+    }
+    __syncwarp();
+    double* out = reinterpret_cast<double*>(V.edata) + e * (NB * blk_stride<double>());
+    for (int p = lane; p < NB; p += 32) {
+      const int a = s_pa[p], b = s_pb[p];
+      double val = 0.0;
+      if (KIND == 1) {
+        for (int q = 0; q < nq; ++q) val += sq[q] * c_N[nn_offset(ET) + a * nq + q] * c_N[nn_offset(ET) + b * nq + q];
+      } else if (KIND == 2) {
+        if (a == b)
+          for (int bb = 0; bb < n; ++bb) {
+            double m = 0.0;
+            for (int q = 0; q < nq; ++q)
+              m += sq[q] * c_N[nn_offset(ET) + a * nq + q] * c_N[nn_offset(ET) + bb * nq + q];
+            val += m;
+          }
+      } else {
+        for (int q = 0; q < nq; ++q) {
+          const double* ga = g + (q * n + a) * 3;
+          const double* gb = g + (q * n + b) * 3;
+          const double* sg = sig + q * 6;
+          const double se = sg[0] * ga[0] * gb[0] + sg[1] * ga[1] * gb[1] + sg[2] * ga[2] * gb[2] +
+                            sg[3] * (ga[0] * gb[1] + ga[1] * gb[0]) + sg[4] * (ga[0] * gb[2] + ga[2] * gb[0]) +
+                            sg[5] * (ga[1] * gb[2] + ga[2] * gb[1]);
+          val += sq[q] * se;
+        }
+      }
+      const double bv[9] = {val, 0.0, 0.0, 0.0, val, 0.0, 0.0, 0.0, val};
+      store_block<double>(out + p * blk_stride<double>(), bv);
+    }
+    __syncwarp();
+  }
+}
+
+template <int ET, int KIND>
+cudaError_t launch_scalar_t(const ElemArgs& a, const V2Args& v, const double* density, const double* gp_stress,
+                            cudaStream_t s) {
+  if (a.n_elems == 0) return cudaSuccess;
+  auto kern = scalar_kernel<ET, KIND>;
+  const size_t smem = sizeof(double) * kScalarWarps * scalar_warp_doubles<ET, KIND>();
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  int per_sm = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kScalarWarps * 32, smem);
+  if (err != cudaSuccess) return err;
+  const int64_t grid = persistent_grid((a.n_elems + kScalarWarps - 1) / kScalarWarps, per_sm, 0);
+  kern<<<static_cast<unsigned>(grid), kScalarWarps * 32, smem, s>>>(a, v, density, gp_stress);
+  return cudaGetLastError();
+}
+
+template <int ET>
+cudaError_t launch_scalar_type(int kind, const ElemArgs& a, const V2Args& v, const double* density,
+                               const double* gp_stress, cudaStream_t s) {
+  switch (kind) {
+    case 1: return launch_scalar_t<ET, 1>(a, v, density, gp_stress, s);
+    case 2: return launch_scalar_t<ET, 2>(a, v, density, gp_stress, s);
+    case 3: return launch_scalar_t<ET, 3>(a, v, density, gp_stress, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 }  // namespace
 
 size_t v2_edata_bytes(int t, int64_t n_elems, int precision) {
@@ -884,6 +1019,19 @@ cudaError_t launch_v2(int t, int mode, int precision, const ElemArgs& a, const V
     case C3D20R: return launch_v2_type<C3D20R>(mode, precision, a, v, c, s);
     case C3D6: return launch_v2_type<C3D6>(mode, precision, a, v, c, s);
     case C3D15: return launch_v2_type<C3D15>(mode, precision, a, v, c, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_scalar_pass(int t, int kind, const ElemArgs& a, const V2Args& v, const double* density,
+                               const double* gp_stress, cudaStream_t s) {
+  switch (t) {
+    case C3D8: return launch_scalar_type<C3D8>(kind, a, v, density, gp_stress, s);
+    case C3D8R: return launch_scalar_type<C3D8R>(kind, a, v, density, gp_stress, s);
+    case C3D20: return launch_scalar_type<C3D20>(kind, a, v, density, gp_stress, s);
+    case C3D20R: return launch_scalar_type<C3D20R>(kind, a, v, density, gp_stress, s);
+    case C3D6: return launch_scalar_type<C3D6>(kind, a, v, density, gp_stress, s);
+    case C3D15: return launch_scalar_type<C3D15>(kind, a, v, density, gp_stress, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -174,6 +174,21 @@ CXG_API int cxg_assemble_linear_ex(cxg_plan* plan, double* vals, double* rhs, co
 CXG_API int cxg_assemble_tangent(cxg_plan* plan, const double* u, double* vals, double* f_int,
                          double* rhs, const double* f_ext, void* stream);
 
+/* Consistent (lumped = 0) or lumped (row-sum) mass matrix M_ff on the plan's pattern
+ * (assemble_mass, src/fem/assembly.cpp:259-298; element_mass / element_mass_lumped,
+ * include/calculixpp/fem/element.hpp:93-102): M_e[3a+i][3b+j] = delta_ij sum_q rho_e
+ * detJ w N_a N_b. density[n_elems] per element (Model::element_density). Entries the
+ * reference omits as exact zeros (all off-diagonal entries when lumped) are present
+ * here as 0.0. *MASS point masses are not part of this entry point. */
+CXG_API int cxg_assemble_mass(cxg_plan* plan, const double* density, int32_t lumped, double* vals,
+                              void* stream);
+/* Geometric (initial-stress) stiffness K_geo on the plan's pattern
+ * (assemble_geometric_stiffness, src/fem/assembly.cpp:300-331; element_geometric_stiffness,
+ * element.hpp:104-119): K_e[3a+i][3b+j] = delta_ij sum_q detJ w g_a . sigma_q . g_b.
+ * gp_stress[6 * n_gauss_points] Voigt {xx,yy,zz,xy,xz,yz} per Gauss point, element
+ * order then the Gauss rule's order; NULL means a zero field. */
+CXG_API int cxg_assemble_geometric(cxg_plan* plan, const double* gp_stress, double* vals, void* stream);
+
 /* ---- per-Gauss-point history (MaterialPoints, include/calculixpp/fem/assembly.hpp:76-88)
  * committed/trial buffers, 13 doubles per Gauss point. */
 CXG_API int cxg_state_get(const cxg_plan* plan, int32_t slot, double* out);
