@@ -1025,6 +1025,141 @@ error2:
   return NULL;
 }
 
+/* ---- field recovery: src/fem/stress.cpp (elastic, no thermal strain) ------------- */
+/* strain_stress_at, stress.cpp:19-42 (eps_th = 0): du[i][j] = sum_k g_k[j] u_k[i],
+ * engineering strain, sigma = D eps. */
+static void strain_stress_at(const double* g, int n, const double* ue, const double* D, double* strain,
+                             double* stress) {
+  double du[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < n; ++k) v += g[3 * k + j] * ue[3 * k + i];
+      du[i][j] = v;
+    }
+  strain[0] = du[0][0];
+  strain[1] = du[1][1];
+  strain[2] = du[2][2];
+  strain[3] = du[0][1] + du[1][0];
+  strain[4] = du[0][2] + du[2][0];
+  strain[5] = du[1][2] + du[2][1];
+  for (int i = 0; i < 6; ++i) {
+    double v = 0.0;
+    for (int j = 0; j < 6; ++j) v += D[6 * i + j] * (strain[j] - 0.0);
+    stress[i] = v;
+  }
+}
+
+static int gather_element(int64_t n_nodes, const double* coords, const int32_t* c, int n, const double* u,
+                          double* x, double* ue) {
+  for (int k = 0; k < n; ++k) {
+    if (c[k] < 0 || c[k] >= n_nodes) return fail("element references unknown node");
+    for (int d = 0; d < 3; ++d) {
+      x[3 * k + d] = coords[3 * (int64_t)c[k] + d];
+      ue[3 * k + d] = u[3 * (int64_t)c[k] + d];
+    }
+  }
+  return 0;
+}
+
+/* recover_gauss_stress, stress.cpp:147-187: out[6 * G] (element order, Gauss-rule order);
+ * young/poisson per element. */
+int cxo_recover_gauss_stress(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                             const int64_t* conn_ptr, const int32_t* conn, const double* young,
+                             const double* poisson, const double* u, double* out) {
+  double x[3 * MAXN], ue[3 * MAXN], D[36], gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det, strain[6];
+  int64_t off = 0;
+  for (int64_t e = 0; e < n_elems; ++e) {
+    const int n = cxo_nodes_per_element(types[e]);
+    if (n == 0 || conn_ptr[e + 1] - conn_ptr[e] != n) return fail("unsupported element type or bad connectivity");
+    if (gather_element(n_nodes, coords, conn + conn_ptr[e], n, u, x, ue)) return -1;
+    elastic_D(young[e], poisson[e], D);
+    const int ng = cxo_gauss_rule(types[e], gp);
+    for (int q = 0; q < ng; ++q, ++off) {
+      cxo_shape(types[e], gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
+      if (gradients_from_shape(n, dN, x, g, &det)) return -1;
+      strain_stress_at(g, n, ue, D, strain, out + 6 * off);
+    }
+  }
+  return 0;
+}
+
+/* recover_fields, stress.cpp:189-271 (elastic, no thermal strain; the families here
+ * extrapolate by the Gauss-point mean, extrapolation.hpp:34-41): nodal strain/stress
+ * averaged over the incident elements, reaction = f_int - f_ext with
+ * f_int = sum_e K_e u_e (accumulate_internal_force, stress.cpp:56-75). */
+int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                       const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
+                       const double* u, const double* f_ext, double* strain_out, double* stress_out,
+                       double* reaction) {
+  double x[3 * MAXN], ue[3 * MAXN], D[36], gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det;
+  double Ke[60 * 60], gs[27][6], ge[27][6];
+  int* count = calloc((size_t)n_nodes, sizeof(int));
+  double* f_int = calloc((size_t)(3 * n_nodes), sizeof(double));
+  if (!count || !f_int) {
+    free(count);
+    free(f_int);
+    return fail("out of memory");
+  }
+  memset(strain_out, 0, sizeof(double) * 6 * (size_t)n_nodes);
+  memset(stress_out, 0, sizeof(double) * 6 * (size_t)n_nodes);
+  int rc = 0;
+  for (int64_t e = 0; e < n_elems && !rc; ++e) {
+    const int n = cxo_nodes_per_element(types[e]);
+    const int32_t* c = conn + conn_ptr[e];
+    if (n == 0 || conn_ptr[e + 1] - conn_ptr[e] != n) {
+      rc = fail("unsupported element type or bad connectivity");
+      break;
+    }
+    if ((rc = gather_element(n_nodes, coords, c, n, u, x, ue))) break;
+    elastic_D(young[e], poisson[e], D);
+    if ((rc = cxo_element_stiffness(types[e], x, young[e], poisson[e], Ke))) break;
+    const int ndof = 3 * n;
+    for (int a = 0; a < ndof; ++a) {
+      double v = 0.0;
+      for (int b = 0; b < ndof; ++b) v += Ke[a * ndof + b] * ue[b];
+      f_int[3 * (int64_t)c[a / 3] + a % 3] += v;
+    }
+    const int ng = cxo_gauss_rule(types[e], gp);
+    for (int q = 0; q < ng; ++q) {
+      cxo_shape(types[e], gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
+      if ((rc = gradients_from_shape(n, dN, x, g, &det))) break;
+      strain_stress_at(g, n, ue, D, ge[q], gs[q]);
+    }
+    if (rc) break;
+    double ms[6] = {0}, me[6] = {0};
+    for (int q = 0; q < ng; ++q)
+      for (int k = 0; k < 6; ++k) {
+        me[k] += ge[q][k];
+        ms[k] += gs[q][k];
+      }
+    const double inv = ng ? 1.0 / (double)ng : 0.0;
+    for (int k = 0; k < 6; ++k) {
+      me[k] *= inv;
+      ms[k] *= inv;
+    }
+    for (int i = 0; i < n; ++i) {
+      for (int k = 0; k < 6; ++k) {
+        strain_out[6 * (int64_t)c[i] + k] += me[k];
+        stress_out[6 * (int64_t)c[i] + k] += ms[k];
+      }
+      ++count[c[i]];
+    }
+  }
+  if (!rc) {
+    for (int64_t i = 0; i < n_nodes; ++i)
+      if (count[i] > 0)
+        for (int k = 0; k < 6; ++k) {
+          strain_out[6 * i + k] /= count[i];
+          stress_out[6 * i + k] /= count[i];
+        }
+    for (int64_t i = 0; i < 3 * n_nodes; ++i) reaction[i] = f_int[i] - (f_ext ? f_ext[i] : 0.0);
+  }
+  free(count);
+  free(f_int);
+  return rc;
+}
+
 int cxo_system_info(const cxo_system* s, int32_t* n_free, int64_t* nnz) {
   *n_free = s->n_free;
   *nnz = s->nnz;

@@ -95,6 +95,16 @@ cxo_system* cxo_assemble_scalar(int kind, int64_t n_nodes, const double* coords,
                                 const double* density, const double* gp_stress, const int32_t* dof_eq,
                                 const double* prescribed, int32_t n_free);
 
+/* recover_gauss_stress / recover_fields (src/fem/stress.cpp:147-271), elastic without
+ * thermal strain: gp_stress[6 G]; nodal strain/stress [6N] averaged over incident
+ * elements; reaction[3N] = f_int - f_ext (f_ext may be NULL). */
+int cxo_recover_gauss_stress(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                             const int64_t* conn_ptr, const int32_t* conn, const double* young,
+                             const double* poisson, const double* u, double* gp_stress);
+int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                       const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
+                       const double* u, const double* f_ext, double* strain, double* stress, double* reaction);
+
 int cxo_system_info(const cxo_system* s, int32_t* n_free, int64_t* nnz);
 int cxo_system_copy(const cxo_system* s, int64_t* row_ptr, int32_t* col_idx,
                     double* vals, double* rhs);

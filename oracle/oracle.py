@@ -247,6 +247,31 @@ class Port(_Base):
         rp, ci, v, _ = self._system(s)
         return rp, ci, v
 
+    def _recover_args(self, mesh, young, poisson):
+        E = mesh.n_elems
+        n = mesh.conn.shape[1]
+        return (mesh.n_nodes, _p(_f64(mesh.coords)), E, _p(np.full(E, mesh.etype, dtype=np.int32)),
+                _p(np.arange(E + 1, dtype=np.int64) * n), _p(_i32(mesh.conn.ravel())), _p(_f64(young)),
+                _p(_f64(poisson)))
+
+    def recover_gauss_stress(self, mesh, young, poisson, u):
+        """recover_gauss_stress (src/fem/stress.cpp:147-187): (G, 6)."""
+        out = np.zeros(6 * mesh.n_elems * NGP[mesh.etype])
+        f = self._fn("recover_gauss_stress")
+        f.argtypes = [C.c_int64, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+        self._check(f(*self._recover_args(mesh, young, poisson), _p(_f64(u)), _p(out)))
+        return out.reshape(-1, 6)
+
+    def recover_fields(self, mesh, young, poisson, u, f_ext=None):
+        """recover_fields (stress.cpp:189-271): nodal strain (N,6), stress (N,6), reaction (N,3)."""
+        N = mesh.n_nodes
+        st, ss, rf = np.zeros(6 * N), np.zeros(6 * N), np.zeros(3 * N)
+        f = self._fn("recover_fields")
+        f.argtypes = [C.c_int64, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+        self._check(f(*self._recover_args(mesh, young, poisson), _p(_f64(u)),
+                      _p(None if f_ext is None else _f64(f_ext)), _p(st), _p(ss), _p(rf)))
+        return st.reshape(N, 6), ss.reshape(N, 6), rf.reshape(N, 3)
+
     def element_compliance_grad_fd(self, etype, coords, ue, E, nu, h):
         n = NODES[etype]
         out = np.zeros(3 * n)
@@ -360,6 +385,17 @@ class RefModel:
     def assemble_linear_static(self):
         """Returns the reference LinearSystem (COO in hash-map order) as a dict."""
         return self._take(self.ref._fn("assemble_linear_static")(_vp(self.h)))
+
+    def recover_gauss_stress(self, u):
+        out = np.zeros(6 * self.mesh.n_elems * NGP[self.mesh.etype])
+        self.ref._check(self.ref.lib.ref_recover_gauss_stress(_vp(self.h), _p(_f64(u)), _p(out)))
+        return out.reshape(-1, 6)
+
+    def recover_fields(self, u):
+        N = self.mesh.n_nodes
+        st, ss, rf = np.zeros(6 * N), np.zeros(6 * N), np.zeros(3 * N)
+        self.ref._check(self.ref.lib.ref_recover_fields(_vp(self.h), _p(_f64(u)), _p(st), _p(ss), _p(rf)))
+        return st.reshape(N, 6), ss.reshape(N, 6), rf.reshape(N, 3)
 
     def set_density(self, rho_per_material):
         rho = _f64(rho_per_material)

@@ -30,6 +30,7 @@
 
 #include "calculixpp/core/model.hpp"
 #include "calculixpp/fem/assembly.hpp"
+#include "calculixpp/fem/stress.hpp"
 #include "calculixpp/fem/element.hpp"
 #include "calculixpp/fem/material_model.hpp"
 #include "calculixpp/numerics/sensitivity.hpp"
@@ -381,6 +382,46 @@ void* ref_assemble_geometric(void* model, const double* gp_stress) {
   } catch (const std::exception& e) {
     fail(e);
     return nullptr;
+  }
+}
+
+// recover_gauss_stress (stress.cpp:147-187): out[6 G] in element order.
+int ref_recover_gauss_stress(void* model, const double* u, double* out) {
+  try {
+    const Model& m = static_cast<RefModel*>(model)->model;
+    std::vector<Vec3> uu(m.mesh.num_nodes());
+    for (std::size_t i = 0; i < uu.size(); ++i) uu[i] = {u[3 * i], u[3 * i + 1], u[3 * i + 2]};
+    const auto sg = recover_gauss_stress(m, uu);
+    std::size_t off = 0;
+    for (const auto& e : sg)
+      for (const auto& v : e) {
+        for (int c = 0; c < 6; ++c) out[6 * off + c] = v[static_cast<std::size_t>(c)];
+        ++off;
+      }
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// recover_fields (stress.cpp:189-271): nodal strain/stress [6N], reaction [3N].
+int ref_recover_fields(void* model, const double* u, double* strain, double* stress, double* reaction) {
+  try {
+    const Model& m = static_cast<RefModel*>(model)->model;
+    StaticFields f;
+    f.displacement.resize(m.mesh.num_nodes());
+    for (std::size_t i = 0; i < f.displacement.size(); ++i) f.displacement[i] = {u[3 * i], u[3 * i + 1], u[3 * i + 2]};
+    recover_fields(m, f);
+    for (std::size_t i = 0; i < f.displacement.size(); ++i) {
+      for (int c = 0; c < 6; ++c) {
+        strain[6 * i + c] = f.strain[i][static_cast<std::size_t>(c)];
+        stress[6 * i + c] = f.stress[i][static_cast<std::size_t>(c)];
+      }
+      for (int c = 0; c < 3; ++c) reaction[3 * i + c] = f.reaction[i][static_cast<std::size_t>(c)];
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
   }
 }
 

@@ -170,3 +170,23 @@ def test_assemble_mass_and_geometric_identical(port, ref, etype):
         assert np.array_equal(rp, rp2) and np.array_equal(ci, ci2), kind
         assert np.array_equal(v, v2), kind
         assert not np.any(s["rhs"]), kind
+
+
+@pytest.mark.parametrize("etype", ALL_TYPES)
+def test_recover_stress_and_fields_identical(port, ref, etype):
+    """recover_gauss_stress and recover_fields (src/fem/stress.cpp:147-271) of the
+    restatement against the reference, for a displacement field with a load."""
+    quad = etype in (mg.C3D20, mg.C3D20R, mg.C3D15)
+    dims = (2, 2, 1) if quad else (3, 2, 2)
+    n_el = mg.box_mesh(etype, *dims).n_elems
+    E = np.random.default_rng(etype).uniform(70e3, 210e3, n_el)
+    model = box_model(etype, *dims, jitter=0.1, seed=etype, young=E)
+    m = model.mesh
+    mats, em = per_element_materials(model)
+    rm = ref.model(m, mats, em, model.spc, model.cloads)
+    u = np.random.default_rng(etype + 7).uniform(-1e-3, 1e-3, 3 * m.n_nodes)
+    assert np.array_equal(port.recover_gauss_stress(m, m.young, m.poisson, u), rm.recover_gauss_stress(u))
+    a = port.recover_fields(m, m.young, m.poisson, u, model.external_load_vector())
+    b = rm.recover_fields(u)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
