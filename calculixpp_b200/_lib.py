@@ -89,6 +89,8 @@ SIGNATURES = {
     "cxg_assemble_tangent": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cxg_assemble_mass": (C.c_int, [_vp, _vp, C.c_int32, _vp, _vp]),
     "cxg_assemble_geometric": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "cxg_recover_gauss_stress": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "cxg_recover_fields": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cxg_state_get": (C.c_int, [_vp, C.c_int32, _vp]),
     "cxg_state_set": (C.c_int, [_vp, C.c_int32, _vp]),
     "cxg_state_commit": (C.c_int, [_vp, _vp]),

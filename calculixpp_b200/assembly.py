@@ -273,6 +273,30 @@ class Plan:
                 self.check()
         return vals
 
+    def recover_gauss_stress(self, u):
+        """Gauss-point stress (n_gauss, 6) for the full displacement u (recover_gauss_stress,
+        src/fem/stress.cpp:147-187)."""
+        out = torch.empty(self.n_gauss * 6, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_recover_gauss_stress(self.h, _ptr(_dev(u, torch.float64, self.device)), _ptr(out),
+                                                         _stream()))
+            self.check()
+        return out.view(-1, 6)
+
+    def recover_fields(self, u, f_ext=None):
+        """(nodal strain (N,6), nodal stress (N,6), reaction (N,3)) for the full
+        displacement u (recover_fields, src/fem/stress.cpp:189-271)."""
+        N = self.model.mesh.n_nodes
+        st = torch.empty(6 * N, dtype=torch.float64, device=self.device)
+        ss = torch.empty(6 * N, dtype=torch.float64, device=self.device)
+        rf = torch.empty(3 * N, dtype=torch.float64, device=self.device)
+        fe = None if f_ext is None else _dev(f_ext, torch.float64, self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_recover_fields(self.h, _ptr(_dev(u, torch.float64, self.device)), _ptr(fe),
+                                                   _ptr(st), _ptr(ss), _ptr(rf), _stream()))
+            self.check()
+        return st.view(N, 6), ss.view(N, 6), rf.view(N, 3)
+
     # -- material state -------------------------------------------------------------
     def state(self, committed=True):
         out = torch.empty(self.n_gauss * 13, dtype=torch.float64, device=self.device)

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libcxg.so")
-SOURCES = ["cxg_api.cu", "cxg_kernels.cu", "cxg_pattern.cu", "cxg_v2.cu", "cxg_solve.cu", "cxg_batch.cu"]
+SOURCES = ["cxg_api.cu", "cxg_kernels.cu", "cxg_pattern.cu", "cxg_v2.cu", "cxg_solve.cu", "cxg_batch.cu", "cxg_recover.cu"]
 HEADERS = ["cxg_internal.cuh", "cxg_elements.hpp", "cxg_plan.hpp", os.path.join("..", "..", "include", "cxg.h")]
 
 NVCC_FLAGS = [

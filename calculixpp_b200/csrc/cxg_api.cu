@@ -549,6 +549,64 @@ int cxg_assemble_geometric(cxg_plan* p, const double* gp_stress, double* vals, v
   return assemble_scalar(p, 3, gp_stress, sizeof(double) * 6 * static_cast<size_t>(p->n_gauss), vals, stream);
 }
 
+int cxg_recover_gauss_stress(cxg_plan* p, const double* u, double* gp_stress, void* stream) {
+  if (!p || !u || !gp_stress) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, u and gp_stress are required");
+  if (p->has_plastic) return set_err(CXG_ERR_UNSUPPORTED, "Gauss-point stress recovery is for linear elasticity");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  const size_t ub = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
+  const size_t gb = sizeof(double) * 6 * static_cast<size_t>(p->n_gauss);
+  void *du, *dg;
+  int rc = staged(p, 3, u, ub, true, s, &du);
+  if (!rc) rc = staged(p, 0, gp_stress, gb, false, s, &dg);
+  if (rc) return rc;
+  ElemArgs a = base_args(p);
+  a.u = static_cast<const double*>(du);
+  CHECK_CUDA(launch_recover(p->type, a, nullptr, nullptr, static_cast<double*>(dg), nullptr, nullptr, nullptr, nullptr,
+                            nullptr, nullptr, s),
+             "recovery kernel");
+  if ((rc = copy_out(gp_stress, dg, gb, s))) return rc;
+  if (dg != gp_stress) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
+  return CXG_OK;
+}
+
+int cxg_recover_fields(cxg_plan* p, const double* u, const double* f_ext, double* strain, double* stress,
+                       double* reaction, void* stream) {
+  if (!p || !u) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan and u are required");
+  if (p->has_plastic) return set_err(CXG_ERR_UNSUPPORTED, "field recovery here is for linear elasticity");
+  if (p->type == C3D8R)
+    return set_err(CXG_ERR_UNSUPPORTED, "field recovery of the hourglass-stabilised C3D8R is not provided");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  const size_t ub = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
+  const size_t sb = 2 * ub;
+  void *du, *df = nullptr, *dst = nullptr, *dss = nullptr, *drf = nullptr;
+  int rc = staged(p, 3, u, ub, true, s, &du);
+  if (!rc) rc = staged(p, 2, f_ext, ub, true, s, &df);
+  if (!rc) rc = staged(p, 1, strain, sb, false, s, &dst);
+  if (!rc) rc = staged(p, 4, stress, sb, false, s, &dss);
+  if (!rc) rc = staged(p, 5, reaction, ub, false, s, &drf);
+  if (rc) return rc;
+  const int n = nodes_of(p->type);
+  double* scratch = nullptr;
+  const size_t scratch_doubles = static_cast<size_t>(p->n_elems) * (12 + 3 * n);
+  CHECK_CUDA(cudaMallocAsync(&scratch, sizeof(double) * std::max<size_t>(scratch_doubles, 1), s), "recovery scratch");
+  ElemArgs a = base_args(p);
+  a.u = static_cast<const double*>(du);
+  const cudaError_t err = launch_recover(p->type, a, p->pat.inc_ptr, p->pat.inc_code, nullptr, scratch,
+                                         scratch + 12 * static_cast<size_t>(p->n_elems),
+                                         static_cast<const double*>(df), static_cast<double*>(dst),
+                                         static_cast<double*>(dss), static_cast<double*>(drf), s);
+  cudaFreeAsync(scratch, s);
+  CHECK_CUDA(err, "recovery kernels");
+  if ((rc = copy_out(strain, dst, sb, s))) return rc;
+  if ((rc = copy_out(stress, dss, sb, s))) return rc;
+  if ((rc = copy_out(reaction, drf, ub, s))) return rc;
+  if ((strain && dst != strain) || (stress && dss != stress) || (reaction && drf != reaction))
+    CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
+  return CXG_OK;
+}
+
 int cxg_state_get(const cxg_plan* cp, int32_t slot, double* out) {
   auto* p = const_cast<cxg_plan*>(cp);
   if (!p || !out || (slot != 0 && slot != 1)) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");

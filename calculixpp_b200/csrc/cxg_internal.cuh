@@ -129,6 +129,12 @@ cudaError_t launch_rhs_init(const int32_t* dof_eq, const double* f_ext, int64_t 
                             double* rhs, cudaStream_t s);
 cudaError_t launch_state_transpose(const double* src, double* dst, int64_t G, bool to_soa,
                                    cudaStream_t s);
+// Field recovery (cxg_recover.cu): a.u is the full displacement. gp_stress[6G] may be
+// null; emean[12E] and felem[3nE] are scratch for the node pass (both null: Gauss-point
+// stress only); strain/stress[6N], reaction[3N] outputs.
+cudaError_t launch_recover(int elem_type, const ElemArgs& a, const int64_t* inc_ptr, const int32_t* inc_code,
+                           double* gp_stress, double* emean, double* felem, const double* f_ext, double* strain,
+                           double* stress, double* reaction, cudaStream_t s);
 cudaError_t launch_adjoint(int elem_type, const ElemArgs& a, double* dc_dE, double* dc_dX,
                            cudaStream_t s);
 cudaError_t launch_spmv(int32_t nrows, const int64_t* rp, const int32_t* ci, const double* v, const double* x,

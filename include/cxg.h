@@ -189,6 +189,18 @@ CXG_API int cxg_assemble_mass(cxg_plan* plan, const double* density, int32_t lum
  * order then the Gauss rule's order; NULL means a zero field. */
 CXG_API int cxg_assemble_geometric(cxg_plan* plan, const double* gp_stress, double* vals, void* stream);
 
+/* ---- field recovery from a displacement field u[3*n_nodes] (linear elasticity) -------
+ * recover_gauss_stress (src/fem/stress.cpp:147-187): gp_stress[6 * n_gauss_points],
+ * sigma = D B u_e per Gauss point (Voigt, engineering shear), element order. */
+CXG_API int cxg_recover_gauss_stress(cxg_plan* plan, const double* u, double* gp_stress, void* stream);
+/* recover_fields (stress.cpp:189-271) without thermal strain: nodal strain and stress
+ * [6 * n_nodes], the Gauss-point means of the incident elements (the extrapolation of
+ * these families, include/calculixpp/fem/extrapolation.hpp:34-41) averaged over the
+ * elements; reaction[3 * n_nodes] = f_int - f_ext with f_int = sum_e K_e u_e. Any output
+ * and f_ext may be NULL. C3D8R (hourglass forces) is rejected with CXG_ERR_UNSUPPORTED. */
+CXG_API int cxg_recover_fields(cxg_plan* plan, const double* u, const double* f_ext, double* strain,
+                               double* stress, double* reaction, void* stream);
+
 /* ---- per-Gauss-point history (MaterialPoints, include/calculixpp/fem/assembly.hpp:76-88)
  * committed/trial buffers, 13 doubles per Gauss point. */
 CXG_API int cxg_state_get(const cxg_plan* plan, int32_t slot, double* out);
