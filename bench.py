@@ -537,8 +537,10 @@ def main():
 
     results = {}
     clocks = None
+    shapes = {}
     for prec in ("fp64", "mixed"):
         plan.set_precision(prec)
+        shapes[prec] = plan.tune(step)
         for _ in range(args.warmup):
             step()
         plan.check()
@@ -557,7 +559,7 @@ def main():
         tk = time_steps(kernel_only, args.steps, stream)
         tk = max_over_ranks(tk, world)
         plan.check()
-        results[prec] = {"t": t, "t_kernel": tk}
+        results[prec] = {"t": t, "t_kernel": tk, "launch_shape": shapes[prec]}
 
     # e2e through the C ABI with host buffers (pinned): load vector in, K_ff + rhs out.
     h_f = torch.as_tensor(f_ext).pin_memory()
@@ -632,7 +634,9 @@ def main():
                    "precision": "mixed: FP32 gradients/Gram blocks, FP64 Jacobians, diagonal blocks and accumulation",
                    "l2": "outputs (8*nnz bytes) far larger than L2; no flush needed",
                    "parallelism": f"independent block per GPU x{world}"},
+        "launch_shape": mix["launch_shape"],
         "fp64": {"value": world * E * args.steps / f64["t"], "ms_per_step": f64["t"] / args.steps * 1e3,
+                 "launch_shape": f64["launch_shape"],
                  "kernel_ms": f64["t_kernel"] / args.steps * 1e3,
                  "fp64_pipe": {"achieved_tflops": FLOPS_PER_ELEM_C3D20 * E / (f64["t_kernel"] / args.steps) / 1e12,
                                "peak_tflops": pipe.get("fp64_tflops"),
