@@ -589,12 +589,13 @@ int cxg_recover_fields(cxg_plan* p, const double* u, const double* f_ext, double
   if (rc) return rc;
   const int n = nodes_of(p->type);
   double* scratch = nullptr;
-  const size_t scratch_doubles = static_cast<size_t>(p->n_elems) * (12 + 3 * n);
+  const int sets = p->type == C3D10 ? n : 1;  // value sets per element, see cxg_recover.cu
+  const size_t scratch_doubles = static_cast<size_t>(p->n_elems) * (12 * sets + 3 * n);
   CHECK_CUDA(cudaMallocAsync(&scratch, sizeof(double) * std::max<size_t>(scratch_doubles, 1), s), "recovery scratch");
   ElemArgs a = base_args(p);
   a.u = static_cast<const double*>(du);
   const cudaError_t err = launch_recover(p->type, a, p->pat.inc_ptr, p->pat.inc_code, nullptr, scratch,
-                                         scratch + 12 * static_cast<size_t>(p->n_elems),
+                                         scratch + 12 * static_cast<size_t>(sets) * static_cast<size_t>(p->n_elems),
                                          static_cast<const double*>(df), static_cast<double*>(dst),
                                          static_cast<double*>(dss), static_cast<double*>(drf), s);
   cudaFreeAsync(scratch, s);

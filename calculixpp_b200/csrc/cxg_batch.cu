@@ -131,6 +131,8 @@ int prepare(cxg_batch* b) {
 
 const char* type_name(int t) {
   switch (t) {
+    case C3D4: return "C3D4";
+    case C3D10: return "C3D10";
     case C3D8: return "C3D8";
     case C3D8R: return "C3D8R";
     case C3D20: return "C3D20";
@@ -247,7 +249,7 @@ int cxg_batch_create(int32_t n_models, const cxg_mesh_desc* meshes, const cxg_do
   cudaGetDevice(&b->device);
   b->precision = precision;
   b->models.resize(static_cast<size_t>(n_models));
-  for (int t = C3D8; t <= C3D15; ++t) {
+  for (int t = kFirstType; t <= kLastType; ++t) {
     Group g;
     g.type = t;
     for (int32_t k = 0; k < n_models; ++k)

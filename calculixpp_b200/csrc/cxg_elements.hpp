@@ -10,7 +10,8 @@
 // ordered xi fastest, then eta, then zeta. The shape functions are the standard
 // isoparametric ones of CalculiX's shape8h/shape20h/shape6w/shape15w
 // (element.cpp:160-330), written here from node natural coordinates: trilinear and
-// serendipity hexahedra, linear and quadratic wedges over area coordinates.
+// serendipity hexahedra, linear and quadratic wedges over area coordinates, linear and
+// quadratic tetrahedra over volume coordinates (shape4tet / shape10tet, element.cpp:130-158).
 #pragma once
 
 #include <cmath>
@@ -18,16 +19,19 @@
 
 namespace cxg {
 
-enum ElemType : int32_t { C3D8 = 2, C3D8R = 3, C3D20 = 4, C3D20R = 5, C3D6 = 6, C3D15 = 7 };
+enum ElemType : int32_t { C3D4 = 0, C3D10 = 1, C3D8 = 2, C3D8R = 3, C3D20 = 4, C3D20R = 5, C3D6 = 6, C3D15 = 7 };
+constexpr int kFirstType = C3D4, kLastType = C3D15;
 
 constexpr int kMaxNodes = 20;
 constexpr int kMaxGauss = 27;
 
 constexpr int nodes_of(int t) {
-  return (t == C3D8 || t == C3D8R) ? 8 : (t == C3D20 || t == C3D20R) ? 20 : t == C3D6 ? 6 : t == C3D15 ? 15 : 0;
+  return (t == C3D8 || t == C3D8R) ? 8 : (t == C3D20 || t == C3D20R) ? 20 : t == C3D6 ? 6 : t == C3D15 ? 15
+         : t == C3D4 ? 4 : t == C3D10 ? 10 : 0;
 }
 constexpr int gauss_of(int t) {
-  return t == C3D8 ? 8 : t == C3D8R ? 1 : t == C3D20 ? 27 : t == C3D20R ? 8 : t == C3D6 ? 2 : t == C3D15 ? 6 : 0;
+  return t == C3D8 ? 8 : t == C3D8R ? 1 : t == C3D20 ? 27 : t == C3D20R ? 8 : t == C3D6 ? 2 : t == C3D15 ? 6
+         : t == C3D4 ? 1 : t == C3D10 ? 4 : 0;
 }
 constexpr bool supported(int t) { return nodes_of(t) != 0; }
 
@@ -55,6 +59,16 @@ inline int gauss_rule(int t, GaussPt* pts) {
   } else if (t == C3D6) {
     pts[n++] = {1.0 / 3.0, 1.0 / 3.0, -g2, 0.5};
     pts[n++] = {1.0 / 3.0, 1.0 / 3.0, g2, 0.5};
+  } else if (t == C3D4) {
+    pts[n++] = {0.25, 0.25, 0.25, 1.0 / 6.0};
+  } else if (t == C3D10) {
+    // 4-point tetrahedral rule: abscissae a = (5 - sqrt 5)/20 and b = 1 - 3a, the
+    // decimal values of src/fem/element.cpp:10-20.
+    const double a = 0.138196601125010515, b = 0.585410196624968454;
+    pts[n++] = {a, a, a, 1.0 / 24.0};
+    pts[n++] = {b, a, a, 1.0 / 24.0};
+    pts[n++] = {a, b, a, 1.0 / 24.0};
+    pts[n++] = {a, a, b, 1.0 / 24.0};
   } else if (t == C3D15) {
     const double tri[3][2] = {{1.0 / 6.0, 1.0 / 6.0}, {2.0 / 3.0, 1.0 / 6.0}, {1.0 / 6.0, 2.0 / 3.0}};
     for (int c = 0; c < 2; ++c)
@@ -119,6 +133,30 @@ inline int shape_derivatives(int t, double xi, double et, double ze, double* N, 
       }
     }
     return n;
+  }
+  // Tetrahedra: volume coordinates L = (1 - xi - et - ze, xi, et, ze).
+  if (t == C3D4 || t == C3D10) {
+    const double L[4] = {1.0 - xi - et - ze, xi, et, ze};
+    const double dL[4][3] = {{-1.0, -1.0, -1.0}, {1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+    if (t == C3D4) {
+      for (int k = 0; k < 4; ++k) {
+        N[k] = L[k];
+        for (int d = 0; d < 3; ++d) dN[k][d] = dL[k][d];
+      }
+      return 4;
+    }
+    // corners L_i (2 L_i - 1); midsides 4 L_i L_j on edges (0,1) (1,2) (2,0) (0,3) (1,3) (2,3)
+    for (int k = 0; k < 4; ++k) {
+      N[k] = L[k] * (2.0 * L[k] - 1.0);
+      for (int d = 0; d < 3; ++d) dN[k][d] = (4.0 * L[k] - 1.0) * dL[k][d];
+    }
+    static const int edge[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+    for (int m = 0; m < 6; ++m) {
+      const int i = edge[m][0], j = edge[m][1];
+      N[4 + m] = 4.0 * L[i] * L[j];
+      for (int d = 0; d < 3; ++d) dN[4 + m][d] = 4.0 * (dL[i][d] * L[j] + L[i] * dL[j][d]);
+    }
+    return 10;
   }
   // Wedges: area coordinates L = (1 - xi - et, xi, et), dL/dxi = (-1,1,0), dL/det = (-1,0,1).
   const double L[3] = {1.0 - xi - et, xi, et};

@@ -37,7 +37,7 @@ enum KernelMode : int { MODE_LINEAR = 0, MODE_TANGENT = 1 };
 constexpr int dn_size(int t) { return nodes_of(t) * 3 * gauss_of(t); }
 constexpr int dn_offset(int t) {
   int off = 0;
-  for (int u = C3D8; u < t; ++u) off += dn_size(u);
+  for (int u = kFirstType; u < t; ++u) off += dn_size(u);
   return off;
 }
 constexpr int kDnTotal = dn_offset(C3D15) + dn_size(C3D15);
@@ -46,7 +46,7 @@ extern __constant__ double c_dN[kDnTotal];
 constexpr int nn_size(int t) { return nodes_of(t) * gauss_of(t); }
 constexpr int nn_offset(int t) {
   int off = 0;
-  for (int u = C3D8; u < t; ++u) off += nn_size(u);
+  for (int u = kFirstType; u < t; ++u) off += nn_size(u);
   return off;
 }
 constexpr int kNTotal = nn_offset(C3D15) + nn_size(C3D15);

@@ -662,7 +662,7 @@ cudaError_t ensure_tables() {
   if (static_cast<int>(g_tables_ready.size()) > dev && g_tables_ready[dev]) return cudaSuccess;
   std::vector<double> dn(kDnTotal, 0.0), nv(kNTotal, 0.0);
   double w[8][kMaxGauss] = {};
-  for (int t = C3D8; t <= C3D15; ++t) {
+  for (int t = kFirstType; t <= kLastType; ++t) {
     GaussPt pts[kMaxGauss];
     const int nq = gauss_rule(t, pts);
     const int n = nodes_of(t);
@@ -690,6 +690,8 @@ cudaError_t ensure_tables() {
 cudaError_t launch_element_kernel(int t, int mode, bool dense, int precision, const ElemArgs& a,
                                   cudaStream_t s) {
   switch (t) {
+    case C3D4: return launch_type<C3D4>(mode, dense, precision, a, s);
+    case C3D10: return launch_type<C3D10>(mode, dense, precision, a, s);
     case C3D8: return launch_type<C3D8>(mode, dense, precision, a, s);
     case C3D8R: return launch_type<C3D8R>(mode, dense, precision, a, s);
     case C3D20: return launch_type<C3D20>(mode, dense, precision, a, s);

@@ -3,8 +3,9 @@
 //
 // Element pass: one warp per element. Lanes take Gauss points: physical gradients,
 // displacement gradient, engineering strain and sigma = D eps (written out per point
-// when asked); then lanes take (component) means over the Gauss points, which the
-// families here extrapolate to every element node (extrapolation.hpp:34-41), and
+// when asked); then lanes take (component) means over the Gauss points, which the hex
+// and wedge families give every element node (extrapolation.hpp:34-41; C3D10 nodes get
+// the corner extrapolation and midside averages of extrapolation.hpp:43-54), and
 // (node, direction) internal forces f_a = sum_q detJ w sigma_q g_a (= K_e u_e).
 // Node pass: one thread per node sums its incident elements' means and forces in
 // element order (the order of the reference's element loop), divides the means by the
@@ -20,6 +21,13 @@ namespace cxg {
 namespace {
 
 constexpr int kRecWarps = 4;
+
+// Value sets of 12 (strain, stress) per element that the node pass reads: one per node
+// for C3D10 (its corner extrapolation differs per node), one (the mean) otherwise.
+template <int ET>
+constexpr int rec_sets() {
+  return ET == C3D10 ? nodes_of(ET) : 1;
+}
 
 template <int ET>
 constexpr int rec_warp_doubles() {
@@ -101,12 +109,29 @@ __global__ void __launch_bounds__(kRecWarps * 32) rec_elem_kernel(ElemArgs A, do
         for (int c = 0; c < 6; ++c) gp_stress[(e * nq + q) * 6 + c] = st[6 + c];
     }
     __syncwarp();
-    if (emean)
-      for (int c = lane; c < 12; c += 32) {
-        double m = 0.0;
-        for (int q = 0; q < nq; ++q) m += es[12 * q + c];
-        emean[e * 12 + c] = m * (1.0 / nq);
+    if (emean) {
+      if constexpr (ET == C3D10) {
+        // corners: the a4 extrapolation matrix of CalculiX extrapolate.f; midsides: the
+        // mean of their edge's corners (extrapolation.hpp:18-55)
+        constexpr double kA4diag = 1.927050983124842, kA4off = -0.309016994374947;
+        constexpr int kMid[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+        for (int t = lane; t < n * 12; t += 32) {
+          const int i = t / 12, c = t % 12;
+          auto corner = [&](int cn) {
+            double v = 0.0;
+            for (int l = 0; l < 4; ++l) v += (cn == l ? kA4diag : kA4off) * es[12 * l + c];
+            return v;
+          };
+          emean[(e * n + i) * 12 + c] = i < 4 ? corner(i) : 0.5 * (corner(kMid[i - 4][0]) + corner(kMid[i - 4][1]));
+        }
+      } else {
+        for (int c = lane; c < 12; c += 32) {
+          double m = 0.0;
+          for (int q = 0; q < nq; ++q) m += es[12 * q + c];
+          emean[e * 12 + c] = m * (1.0 / nq);
+        }
       }
+    }
     if (felem)
       for (int t = lane; t < 3 * n; t += 32) {
         const int a = t / 3, d = t % 3;
@@ -141,7 +166,8 @@ __global__ void rec_node_kernel(ElemArgs A, const int64_t* inc_ptr, const int32_
       const int code = inc_code[i];
       const int64_t e = code / n;
       const int la = code % n;
-      for (int c = 0; c < 12; ++c) m[c] += emean[e * 12 + c];
+      const int64_t set = rec_sets<ET>() == 1 ? e : e * n + la;
+      for (int c = 0; c < 12; ++c) m[c] += emean[set * 12 + c];
       for (int d = 0; d < 3; ++d) f[d] += felem[e * (3 * n) + 3 * la + d];
     }
     const int64_t cnt = i1 - i0;
@@ -188,6 +214,8 @@ cudaError_t launch_recover(int t, const ElemArgs& a, const int64_t* inc_ptr, con
   switch (t) {
 #define CXG_REC(T) \
   case T: return launch_recover_t<T>(a, inc_ptr, inc_code, gp_stress, emean, felem, f_ext, strain, stress, reaction, s);
+    CXG_REC(C3D4)
+    CXG_REC(C3D10)
     CXG_REC(C3D8)
     CXG_REC(C3D8R)
     CXG_REC(C3D20)

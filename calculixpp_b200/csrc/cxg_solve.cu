@@ -208,6 +208,8 @@ unsigned g1(int64_t n) { return static_cast<unsigned>(std::max<int64_t>(1, std::
 cudaError_t launch_adjoint(int t, const ElemArgs& a, double* dc_dE, double* dc_dX, cudaStream_t s) {
   const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((a.n_elems + 3) / 4, 148 * 16)));
   switch (t) {
+    case C3D4: adjoint_kernel<C3D4><<<grid, 128, 0, s>>>(a, dc_dE, dc_dX); break;
+    case C3D10: adjoint_kernel<C3D10><<<grid, 128, 0, s>>>(a, dc_dE, dc_dX); break;
     case C3D8: adjoint_kernel<C3D8><<<grid, 128, 0, s>>>(a, dc_dE, dc_dX); break;
     case C3D20: adjoint_kernel<C3D20><<<grid, 128, 0, s>>>(a, dc_dE, dc_dX); break;
     case C3D20R: adjoint_kernel<C3D20R><<<grid, 128, 0, s>>>(a, dc_dE, dc_dX); break;

@@ -1013,6 +1013,8 @@ size_t v2_edata_bytes(int t, int64_t n_elems, int precision) {
 cudaError_t launch_v2(int t, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s,
                       const LaunchCfg& c) {
   switch (t) {
+    case C3D4: return launch_v2_type<C3D4>(mode, precision, a, v, c, s);
+    case C3D10: return launch_v2_type<C3D10>(mode, precision, a, v, c, s);
     case C3D8: return launch_v2_type<C3D8>(mode, precision, a, v, c, s);
     case C3D8R: return launch_v2_type<C3D8R>(mode, precision, a, v, c, s);
     case C3D20: return launch_v2_type<C3D20>(mode, precision, a, v, c, s);
@@ -1026,6 +1028,8 @@ cudaError_t launch_v2(int t, int mode, int precision, const ElemArgs& a, const V
 cudaError_t launch_scalar_pass(int t, int kind, const ElemArgs& a, const V2Args& v, const double* density,
                                const double* gp_stress, cudaStream_t s) {
   switch (t) {
+    case C3D4: return launch_scalar_type<C3D4>(kind, a, v, density, gp_stress, s);
+    case C3D10: return launch_scalar_type<C3D10>(kind, a, v, density, gp_stress, s);
     case C3D8: return launch_scalar_type<C3D8>(kind, a, v, density, gp_stress, s);
     case C3D8R: return launch_scalar_type<C3D8R>(kind, a, v, density, gp_stress, s);
     case C3D20: return launch_scalar_type<C3D20>(kind, a, v, density, gp_stress, s);

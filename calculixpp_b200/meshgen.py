@@ -19,10 +19,10 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-C3D8, C3D8R, C3D20, C3D20R, C3D6, C3D15 = 2, 3, 4, 5, 6, 7
-NODES = {C3D8: 8, C3D8R: 8, C3D20: 20, C3D20R: 20, C3D6: 6, C3D15: 15}
-NGP = {C3D8: 8, C3D8R: 1, C3D20: 27, C3D20R: 8, C3D6: 2, C3D15: 6}
-TYPE_NAMES = {C3D8: "C3D8", C3D8R: "C3D8R", C3D20: "C3D20", C3D20R: "C3D20R", C3D6: "C3D6", C3D15: "C3D15"}
+C3D4, C3D10, C3D8, C3D8R, C3D20, C3D20R, C3D6, C3D15 = 0, 1, 2, 3, 4, 5, 6, 7
+NODES = {C3D4: 4, C3D10: 10, C3D8: 8, C3D8R: 8, C3D20: 20, C3D20R: 20, C3D6: 6, C3D15: 15}
+NGP = {C3D4: 1, C3D10: 4, C3D8: 8, C3D8R: 1, C3D20: 27, C3D20R: 8, C3D6: 2, C3D15: 6}
+TYPE_NAMES = {C3D4: "C3D4", C3D10: "C3D10", C3D8: "C3D8", C3D8R: "C3D8R", C3D20: "C3D20", C3D20R: "C3D20R", C3D6: "C3D6", C3D15: "C3D15"}
 NAMES = {C3D8: "C3D8", C3D8R: "C3D8R", C3D20: "C3D20", C3D20R: "C3D20R",
          C3D6: "C3D6", C3D15: "C3D15"}
 BY_NAME = {v: k for k, v in NAMES.items()}
@@ -37,6 +37,12 @@ _HEX_EDGES = np.array([[0, 1], [1, 2], [2, 3], [3, 0], [4, 5], [5, 6],
 _WEDGES = np.array([[0, 1, 3, 4, 5, 7], [1, 2, 3, 5, 6, 7]])
 _W15_EDGES = np.array([[0, 1], [1, 2], [2, 0], [3, 4], [4, 5], [5, 3],
                        [0, 3], [1, 4], [2, 5]])
+# Kuhn split of a hex cell into 6 tetrahedra along the main diagonal (corner 0 to
+# corner 6 of _HEX): one per axis permutation, corners ordered for a positive Jacobian.
+# Conforming across cells (every face is cut along the diagonal through its lowest
+# corner).
+_TETS = np.array([[0, 1, 2, 6], [0, 2, 3, 6], [0, 3, 7, 6], [0, 7, 4, 6], [0, 4, 5, 6], [0, 5, 1, 6]])
+_T10_EDGES = np.array([[0, 1], [1, 2], [2, 0], [0, 3], [1, 3], [2, 3]])
 
 
 @dataclass
@@ -84,13 +90,16 @@ def box_mesh(etype: int, nx: int, ny: int, nz: int, lx=1.0, ly=1.0, lz=1.0,
     """
     if etype not in NODES:
         raise ValueError(f"unsupported element type {etype}")
-    quadratic = etype in (C3D20, C3D20R, C3D15)
+    quadratic = etype in (C3D20, C3D20R, C3D15, C3D10)
     nc = np.array([nx, ny, nz], dtype=np.int64)
     if quadratic:
         n2 = 2 * nc + 1
         if etype == C3D15:
             def mask(x, y, z):
                 return (z % 2 == 0) | ((x % 2 == 0) & (y % 2 == 0))
+        elif etype == C3D10:
+            def mask(x, y, z):
+                return np.ones_like(x, dtype=bool)
         else:
             def mask(x, y, z):
                 return ((x % 2) + (y % 2) + (z % 2)) <= 1
@@ -116,6 +125,13 @@ def box_mesh(etype: int, nx: int, ny: int, nz: int, lx=1.0, ly=1.0, lz=1.0,
     elif etype in (C3D20, C3D20R):
         mids = (corner_lat[:, _HEX_EDGES[:, 0]] + corner_lat[:, _HEX_EDGES[:, 1]]) // 2
         conn = np.concatenate([lat_index(corner_lat), lat_index(mids)], axis=1)
+    elif etype in (C3D4, C3D10):
+        tet = corner_lat[:, _TETS].reshape(-1, 4, 3)
+        if etype == C3D4:
+            conn = lat_index(tet)
+        else:
+            mids = (tet[:, _T10_EDGES[:, 0]] + tet[:, _T10_EDGES[:, 1]]) // 2
+            conn = np.concatenate([lat_index(tet), lat_index(mids)], axis=1)
     else:
         w = corner_lat[:, _WEDGES]  # (C,2,6,3)
         w = w.reshape(-1, 6, 3)
@@ -140,6 +156,8 @@ def box_mesh(etype: int, nx: int, ny: int, nz: int, lx=1.0, ly=1.0, lz=1.0,
         if straight_edges and quadratic:
             if etype == C3D15:
                 nc_, edges = 6, _W15_EDGES
+            elif etype == C3D10:
+                nc_, edges = 4, _T10_EDGES
             else:
                 nc_, edges = 8, _HEX_EDGES
             for i, (a, b) in enumerate(edges):

@@ -10,7 +10,7 @@
  * include/calculixpp/fem/element.hpp:12-61):
  *   - element type codes are the ordinals of cxpp::ElementType
  *     (include/calculixpp/core/element.hpp:13-22): C3D8=2, C3D8R=3, C3D20=4,
- *     C3D20R=5, C3D6=6, C3D15=7 (C3D4/C3D10 are not handled here);
+ *     C3D20R=5, C3D6=6, C3D15=7, and the tetrahedra C3D4=0, C3D10=1;
  *   - node indices are 0-based int32; DOF g = 3*node + component;
  *   - element DOF order node-major [u1,v1,w1,u2,...]; Voigt xx,yy,zz,xy,xz,yz with
  *     engineering shear;
@@ -194,9 +194,9 @@ CXG_API int cxg_assemble_geometric(cxg_plan* plan, const double* gp_stress, doub
  * sigma = D B u_e per Gauss point (Voigt, engineering shear), element order. */
 CXG_API int cxg_recover_gauss_stress(cxg_plan* plan, const double* u, double* gp_stress, void* stream);
 /* recover_fields (stress.cpp:189-271) without thermal strain: nodal strain and stress
- * [6 * n_nodes], the Gauss-point means of the incident elements (the extrapolation of
- * these families, include/calculixpp/fem/extrapolation.hpp:34-41) averaged over the
- * elements; reaction[3 * n_nodes] = f_int - f_ext with f_int = sum_e K_e u_e. Any output
+ * [6 * n_nodes]: each incident element's Gauss-point values extrapolated to the node
+ * (the mean for hexahedra, wedges and C3D4; the corner matrix and midside averages for
+ * C3D10, include/calculixpp/fem/extrapolation.hpp:26-55), averaged over the elements; reaction[3 * n_nodes] = f_int - f_ext with f_int = sum_e K_e u_e. Any output
  * and f_ext may be NULL. C3D8R (hourglass forces) is rejected with CXG_ERR_UNSUPPORTED. */
 CXG_API int cxg_recover_fields(cxg_plan* plan, const double* u, const double* f_ext, double* strain,
                                double* stress, double* reaction, void* stream);

@@ -18,7 +18,7 @@ static int fail(const char* msg) {
 
 const char* cxo_last_error(void) { return g_err; }
 
-enum { T_C3D8 = 2, T_C3D8R = 3, T_C3D20 = 4, T_C3D20R = 5, T_C3D6 = 6, T_C3D15 = 7 };
+enum { T_C3D4 = 0, T_C3D10 = 1, T_C3D8 = 2, T_C3D8R = 3, T_C3D20 = 4, T_C3D20R = 5, T_C3D6 = 6, T_C3D15 = 7 };
 #define MAXN 20
 
 /* include/calculixpp/core/element.hpp:24-44 */
@@ -28,6 +28,8 @@ int cxo_nodes_per_element(int type) {
     case T_C3D20: case T_C3D20R: return 20;
     case T_C3D6: return 6;
     case T_C3D15: return 15;
+    case T_C3D4: return 4;
+    case T_C3D10: return 10;
     default: return 0;
   }
 }
@@ -68,6 +70,15 @@ int cxo_gauss_rule(int type, double* out) {
       const double kT = 1.0 / 6.0, kU = 2.0 / 3.0; /* element.cpp:72-77 */
       GP(kT, kT, -kG2, kT); GP(kU, kT, -kG2, kT); GP(kT, kU, -kG2, kT);
       GP(kT, kT, kG2, kT); GP(kU, kT, kG2, kT); GP(kT, kU, kG2, kT);
+      break;
+    }
+    case T_C3D4:
+      GP(0.25, 0.25, 0.25, 1.0 / 6.0); /* element.cpp:14 */
+      break;
+    case T_C3D10: {
+      const double kA = 0.138196601125010515, kB = 0.585410196624968454; /* element.cpp:10-20 */
+      GP(kA, kA, kA, 1.0 / 24.0); GP(kB, kA, kA, 1.0 / 24.0);
+      GP(kA, kB, kA, 1.0 / 24.0); GP(kA, kA, kB, 1.0 / 24.0);
       break;
     }
     default:
@@ -216,12 +227,35 @@ static void shape_c3d15(double xi, double et, double ze, double* N, double* dN) 
   }
 }
 
+/* shape_c3d4 / shape_c3d10, element.cpp:130-158: volume coordinates, a = 1-xi-et-ze. */
+static void shape_c3d4(double xi, double et, double ze, double* N, double* dN) {
+  N[0] = 1.0 - xi - et - ze; N[1] = xi; N[2] = et; N[3] = ze;
+  const double d[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int k = 0; k < 4; ++k)
+    for (int j = 0; j < 3; ++j) dN[3 * k + j] = d[k][j];
+}
+
+static void shape_c3d10(double xi, double et, double ze, double* N, double* dN) {
+  const double a = 1.0 - xi - et - ze;
+  N[0] = (2 * a - 1) * a;  N[1] = xi * (2 * xi - 1); N[2] = et * (2 * et - 1); N[3] = ze * (2 * ze - 1);
+  N[4] = 4 * xi * a;       N[5] = 4 * xi * et;       N[6] = 4 * et * a;        N[7] = 4 * ze * a;
+  N[8] = 4 * xi * ze;      N[9] = 4 * et * ze;
+  const double d[10][3] = {{1 - 4 * a, 1 - 4 * a, 1 - 4 * a}, {4 * xi - 1, 0, 0}, {0, 4 * et - 1, 0},
+                           {0, 0, 4 * ze - 1}, {4 * (a - xi), -4 * xi, -4 * xi}, {4 * et, 4 * xi, 0},
+                           {-4 * et, 4 * (a - et), -4 * et}, {-4 * ze, -4 * ze, 4 * (a - ze)},
+                           {4 * ze, 0, 4 * xi}, {0, 4 * ze, 4 * et}};
+  for (int k = 0; k < 10; ++k)
+    for (int j = 0; j < 3; ++j) dN[3 * k + j] = d[k][j];
+}
+
 int cxo_shape(int type, double xi, double et, double ze, double* N, double* dN) {
   switch (type) {
     case T_C3D8: case T_C3D8R: shape_c3d8(xi, et, ze, N, dN); return 8;
     case T_C3D20: case T_C3D20R: shape_c3d20(xi, et, ze, N, dN); return 20;
     case T_C3D6: shape_c3d6(xi, et, ze, N, dN); return 6;
     case T_C3D15: shape_c3d15(xi, et, ze, N, dN); return 15;
+    case T_C3D4: shape_c3d4(xi, et, ze, N, dN); return 4;
+    case T_C3D10: shape_c3d10(xi, et, ze, N, dN); return 10;
     default: return 0;
   }
 }
@@ -1084,8 +1118,7 @@ int cxo_recover_gauss_stress(int64_t n_nodes, const double* coords, int64_t n_el
   return 0;
 }
 
-/* recover_fields, stress.cpp:189-271 (elastic, no thermal strain; the families here
- * extrapolate by the Gauss-point mean, extrapolation.hpp:34-41): nodal strain/stress
+/* recover_fields, stress.cpp:189-271 (elastic, no thermal strain): nodal strain/stress
  * averaged over the incident elements, reaction = f_int - f_ext with
  * f_int = sum_e K_e u_e (accumulate_internal_force, stress.cpp:56-75). */
 int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
@@ -1127,21 +1160,50 @@ int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, c
       strain_stress_at(g, n, ue, D, ge[q], gs[q]);
     }
     if (rc) break;
-    double ms[6] = {0}, me[6] = {0};
-    for (int q = 0; q < ng; ++q)
+    /* extrapolate_gp_to_nodes (extrapolation.hpp:26-55): C3D10 corners by the a4 matrix
+     * of CalculiX extrapolate.f, midsides the mean of their edge's corners; the other
+     * families the Gauss-point mean at every node (a single point for C3D4). */
+    double ne[MAXN][6], ns[MAXN][6];
+    if (types[e] == T_C3D10) {
+      static const double kA4diag = 1.927050983124842, kA4off = -0.309016994374947;
+      static const int kMid[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+      for (int cn = 0; cn < 4; ++cn)
+        for (int k = 0; k < 6; ++k) {
+          double ve = 0.0, vs = 0.0;
+          for (int l = 0; l < 4; ++l) {
+            ve += (cn == l ? kA4diag : kA4off) * ge[l][k];
+            vs += (cn == l ? kA4diag : kA4off) * gs[l][k];
+          }
+          ne[cn][k] = ve;
+          ns[cn][k] = vs;
+        }
+      for (int m = 0; m < 6; ++m)
+        for (int k = 0; k < 6; ++k) {
+          ne[4 + m][k] = 0.5 * (ne[kMid[m][0]][k] + ne[kMid[m][1]][k]);
+          ns[4 + m][k] = 0.5 * (ns[kMid[m][0]][k] + ns[kMid[m][1]][k]);
+        }
+    } else {
+      double ms[6] = {0}, me[6] = {0};
+      for (int q = 0; q < ng; ++q)
+        for (int k = 0; k < 6; ++k) {
+          me[k] += ge[q][k];
+          ms[k] += gs[q][k];
+        }
+      const double inv = ng ? 1.0 / (double)ng : 0.0;
       for (int k = 0; k < 6; ++k) {
-        me[k] += ge[q][k];
-        ms[k] += gs[q][k];
+        me[k] *= inv;
+        ms[k] *= inv;
       }
-    const double inv = ng ? 1.0 / (double)ng : 0.0;
-    for (int k = 0; k < 6; ++k) {
-      me[k] *= inv;
-      ms[k] *= inv;
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 6; ++k) {
+          ne[i][k] = me[k];
+          ns[i][k] = ms[k];
+        }
     }
     for (int i = 0; i < n; ++i) {
       for (int k = 0; k < 6; ++k) {
-        strain_out[6 * (int64_t)c[i] + k] += me[k];
-        stress_out[6 * (int64_t)c[i] + k] += ms[k];
+        strain_out[6 * (int64_t)c[i] + k] += ne[i][k];
+        stress_out[6 * (int64_t)c[i] + k] += ns[i][k];
       }
       ++count[c[i]];
     }

@@ -20,8 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_lib", "libcxo.so")
 REF_SO = os.path.join(HERE, "_ref", "libcxpp_ref.so")
 
-NODES = {2: 8, 3: 8, 4: 20, 5: 20, 6: 6, 7: 15}
-NGP = {2: 8, 3: 1, 4: 27, 5: 8, 6: 2, 7: 6}
+NODES = {0: 4, 1: 10, 2: 8, 3: 8, 4: 20, 5: 20, 6: 6, 7: 15}
+NGP = {0: 1, 1: 4, 2: 8, 3: 1, 4: 27, 5: 8, 6: 2, 7: 6}
 
 _vp = C.c_void_p
 

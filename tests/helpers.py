@@ -6,7 +6,7 @@ import numpy as np
 from calculixpp_b200 import meshgen as mg
 from calculixpp_b200.assembly import Material, Model
 
-ALL_TYPES = (mg.C3D8, mg.C3D8R, mg.C3D20, mg.C3D20R, mg.C3D6, mg.C3D15)
+ALL_TYPES = (mg.C3D8, mg.C3D8R, mg.C3D20, mg.C3D20R, mg.C3D6, mg.C3D15, mg.C3D4, mg.C3D10)
 
 # Isotropic hardening table used by the reference's own plasticity tests
 # (tests/test_plasticity.cpp:27-33): sy0 = 800 at ep = 0, sy = 960 at ep = 0.02.

@@ -37,7 +37,7 @@ def test_version_and_tables():
     for t in mg.NODES:
         assert lib.cxg_nodes_per_element(t) == mg.NODES[t]
         assert lib.cxg_gauss_points_per_element(t) == mg.NGP[t]
-    assert lib.cxg_nodes_per_element(0) == 0  # C3D4 is not on this path
+    assert lib.cxg_nodes_per_element(8) == 0  # not an element type code
 
 
 def test_plan_create_without_gpu_reports_status():
@@ -57,5 +57,5 @@ def test_invalid_arguments_rejected_before_device_use():
     rc = lib.cxg_plan_create(None, None, 0, C.byref(out))
     assert rc == _lib.CXG_ERR_INVALID_ARGUMENT
     assert lib.cxg_last_error()
-    rc = lib.cxg_element_stiffness(0, 1, None, None, None, 0, None, None)  # C3D4 unsupported
+    rc = lib.cxg_element_stiffness(8, 1, None, None, None, 0, None, None)  # no such element type
     assert rc == _lib.CXG_ERR_UNSUPPORTED

@@ -90,7 +90,7 @@ def test_autograd_matches_central_differences(cuda):
         assert abs(fd - g) <= 1e-5 * max(abs(g), 1e-3 * float(gX.abs().max())), (node, comp, fd, g)
 
 
-@pytest.mark.parametrize("etype", [mg.C3D20, mg.C3D20R, mg.C3D6, mg.C3D15])
+@pytest.mark.parametrize("etype", [mg.C3D20, mg.C3D20R, mg.C3D6, mg.C3D15, mg.C3D4, mg.C3D10])
 def test_dcdX_all_families_against_element_differences(cuda, port, etype):
     model = box_model(etype, 2, 2, 2, jitter=0.08, seed=etype)
     plan = Plan(model)

@@ -13,7 +13,8 @@ from calculixpp_b200 import meshgen as mg
 from oracle.oracle import make_material
 from tests.helpers import ALL_TYPES, ISO_TABLE, unit_element
 
-VOL = {mg.C3D8: 1.0, mg.C3D8R: 1.0, mg.C3D20: 1.0, mg.C3D20R: 1.0, mg.C3D6: 0.5, mg.C3D15: 0.5}
+VOL = {mg.C3D8: 1.0, mg.C3D8R: 1.0, mg.C3D20: 1.0, mg.C3D20R: 1.0, mg.C3D6: 0.5, mg.C3D15: 0.5,
+       mg.C3D4: 1.0 / 6.0, mg.C3D10: 1.0 / 6.0}  # unit cube, wedge half, Kuhn tetrahedron
 
 
 @pytest.mark.parametrize("etype", ALL_TYPES)
