@@ -326,3 +326,17 @@ def adjoint_cantilever(nx=96, ny=96, nz=48, seed=0, E0=210000.0, nu=0.3, load=-1
     tip = face_nodes(m, 0, float(nx))
     return {"mesh": m, "spc": spc, "cloads": (tip, np.full(tip.size, 2), np.full(tip.size, load / tip.size)),
             "rho": rho}
+
+
+def thermal_dof_map(n_nodes, tbc_node, tbc_val):
+    """Scalar temperature DOF map (build_thermal_dof_map, src/fem/thermal.cpp:71-90):
+    prescribed nodes get -1 and their value (last writer wins), the others are numbered
+    in node order. Returns (t_dof_eq[N], t_prescribed[N], n_free)."""
+    fixed = np.zeros(n_nodes, dtype=bool)
+    pre = np.zeros(n_nodes)
+    for node, val in zip(np.asarray(tbc_node, dtype=np.int64), np.asarray(tbc_val, dtype=np.float64)):
+        fixed[node] = True
+        pre[node] = val
+    deq = np.full(n_nodes, -1, dtype=np.int32)
+    deq[~fixed] = np.arange(int((~fixed).sum()), dtype=np.int32)
+    return deq, pre, int((~fixed).sum())

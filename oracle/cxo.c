@@ -1059,6 +1059,70 @@ error2:
   return NULL;
 }
 
+/* ---- heat conduction: element_conduction (element.cpp:745-765) and
+ * assemble_conduction (src/fem/thermal.cpp:92-141) without films: one temperature DOF
+ * per node, prescribed temperatures eliminated into the rhs, nodal flux added at the
+ * free nodes. */
+int cxo_element_conduction(int type, const double* x, double k, double* Kt) {
+  const int n = cxo_nodes_per_element(type);
+  if (n == 0) return fail("unsupported element type");
+  memset(Kt, 0, sizeof(double) * (size_t)n * (size_t)n);
+  double gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det;
+  const int ng = cxo_gauss_rule(type, gp);
+  for (int q = 0; q < ng; ++q) {
+    cxo_shape(type, gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
+    if (gradients_from_shape(n, dN, x, g, &det)) return -1;
+    const double scale = k * det * gp[4 * q + 3];
+    for (int a = 0; a < n; ++a)
+      for (int b = 0; b < n; ++b) {
+        const double dot = g[3 * a] * g[3 * b] + g[3 * a + 1] * g[3 * b + 1] + g[3 * a + 2] * g[3 * b + 2];
+        Kt[a * n + b] += scale * dot;
+      }
+  }
+  return 0;
+}
+
+cxo_system* cxo_assemble_conduction(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                                    const int64_t* conn_ptr, const int32_t* conn, const double* conductivity,
+                                    const int32_t* t_dof_eq, const double* t_prescribed, int32_t n_free,
+                                    const double* flux) {
+  triplets_t t = {0};
+  double* rhs = calloc((size_t)n_free + 1, sizeof(double));
+  double x[3 * MAXN], Kt[MAXN * MAXN];
+  int64_t gd[MAXN];
+  for (int64_t e = 0; e < n_elems; ++e) {
+    const int n = cxo_nodes_per_element(types[e]);
+    const int32_t* c = conn + conn_ptr[e];
+    if (n == 0 || conn_ptr[e + 1] - conn_ptr[e] != n) {
+      fail("unsupported element type or bad connectivity length");
+      goto error;
+    }
+    for (int k = 0; k < n; ++k) {
+      if (c[k] < 0 || c[k] >= n_nodes) {
+        fail("element references unknown node");
+        goto error;
+      }
+      gd[k] = c[k];
+      for (int d = 0; d < 3; ++d) x[3 * k + d] = coords[3 * (int64_t)c[k] + d];
+    }
+    if (cxo_element_conduction(types[e], x, conductivity[e], Kt)) goto error;
+    if (scatter(Kt, n, gd, t_dof_eq, t_prescribed, n_free, &t, rhs)) goto error;
+  }
+  if (flux)
+    for (int64_t i = 0; i < n_nodes; ++i)
+      if (t_dof_eq[i] >= 0) rhs[t_dof_eq[i]] += flux[i];
+  {
+    cxo_system* s = finish(&t, n_free, rhs);
+    if (!s) goto error;
+    return s;
+  }
+error:
+  free(t.key);
+  free(t.val);
+  free(rhs);
+  return NULL;
+}
+
 /* ---- field recovery: src/fem/stress.cpp (elastic, no thermal strain) ------------- */
 /* strain_stress_at, stress.cpp:19-42 (eps_th = 0): du[i][j] = sum_k g_k[j] u_k[i],
  * engineering strain, sigma = D eps. */

@@ -105,6 +105,14 @@ int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, c
                        const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
                        const double* u, const double* f_ext, double* strain, double* stress, double* reaction);
 
+/* element_conduction (n x n) and assemble_conduction without films (src/fem/thermal.cpp:
+ * 92-141): t_dof_eq[N] / t_prescribed[N] scalar temperature DOF map, flux[N] may be NULL. */
+int cxo_element_conduction(int type, const double* coords, double k, double* Kt);
+cxo_system* cxo_assemble_conduction(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                                    const int64_t* conn_ptr, const int32_t* conn, const double* conductivity,
+                                    const int32_t* t_dof_eq, const double* t_prescribed, int32_t n_free,
+                                    const double* flux);
+
 int cxo_system_info(const cxo_system* s, int32_t* n_free, int64_t* nnz);
 int cxo_system_copy(const cxo_system* s, int64_t* row_ptr, int32_t* col_idx,
                     double* vals, double* rhs);

@@ -146,6 +146,15 @@ class _Base:
         self._check(f(int(etype), _p(_f64(coords)), _p(_f64(gp_stress)), _p(K)))
         return K.reshape(3 * n, 3 * n)
 
+    def element_conduction(self, etype, coords, k):
+        """element_conduction (element.hpp:73-74): (n, n)."""
+        n = NODES[etype]
+        K = np.zeros(n * n)
+        f = self._fn("element_conduction")
+        f.argtypes = [C.c_int, _vp, C.c_double, _vp]
+        self._check(f(int(etype), _p(_f64(coords)), float(k), _p(K)))
+        return K.reshape(n, n)
+
     def material_evaluate(self, mat, strain, committed=None):
         committed = np.zeros(13) if committed is None else _f64(committed)
         trial = np.zeros(13)
@@ -272,6 +281,18 @@ class Port(_Base):
                       _p(None if f_ext is None else _f64(f_ext)), _p(st), _p(ss), _p(rf)))
         return st.reshape(N, 6), ss.reshape(N, 6), rf.reshape(N, 3)
 
+    def assemble_conduction(self, mesh, conductivity, t_dof_eq, t_prescribed, n_free, flux=None):
+        """assemble_conduction without films (src/fem/thermal.cpp:92-141): (rp, ci, vals, rhs)."""
+        E = mesh.n_elems
+        n = mesh.conn.shape[1]
+        f = self._fn("assemble_conduction")
+        f.restype = _vp
+        f.argtypes = [C.c_int64, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32, _vp]
+        s = f(mesh.n_nodes, _p(_f64(mesh.coords)), E, _p(np.full(E, mesh.etype, dtype=np.int32)),
+              _p(np.arange(E + 1, dtype=np.int64) * n), _p(_i32(mesh.conn.ravel())), _p(_f64(conductivity)),
+              _p(_i32(t_dof_eq)), _p(_f64(t_prescribed)), int(n_free), _p(None if flux is None else _f64(flux)))
+        return self._system(s)
+
     def element_compliance_grad_fd(self, etype, coords, ue, E, nu, h):
         n = NODES[etype]
         out = np.zeros(3 * n)
@@ -385,6 +406,14 @@ class RefModel:
     def assemble_linear_static(self):
         """Returns the reference LinearSystem (COO in hash-map order) as a dict."""
         return self._take(self.ref._fn("assemble_linear_static")(_vp(self.h)))
+
+    def assemble_conduction(self, k_per_material, tbc_node, tbc_val):
+        k = _f64(k_per_material)
+        tn, tv = _i32(tbc_node), _f64(tbc_val)
+        f = self.ref._fn("assemble_conduction")
+        f.restype = _vp
+        f.argtypes = [_vp, C.c_int32, _vp, C.c_int64, _vp, _vp]
+        return self._take(f(_vp(self.h), k.size, _p(k), tn.size, _p(tn), _p(tv)))
 
     def recover_gauss_stress(self, u):
         out = np.zeros(6 * self.mesh.n_elems * NGP[self.mesh.etype])

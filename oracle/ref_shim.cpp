@@ -31,6 +31,7 @@
 #include "calculixpp/core/model.hpp"
 #include "calculixpp/fem/assembly.hpp"
 #include "calculixpp/fem/stress.hpp"
+#include "calculixpp/fem/thermal.hpp"
 #include "calculixpp/fem/element.hpp"
 #include "calculixpp/fem/material_model.hpp"
 #include "calculixpp/numerics/sensitivity.hpp"
@@ -422,6 +423,48 @@ int ref_recover_fields(void* model, const double* u, double* strain, double* str
     return 0;
   } catch (const std::exception& e) {
     return fail(e);
+  }
+}
+
+// element_conduction (element.hpp:73-74): Kt[n * n].
+int ref_element_conduction(int type, const double* coords, double k, double* Kt) {
+  try {
+    const ElementType t = static_cast<ElementType>(type);
+    const int n = nodes_per_element(t);
+    std::vector<Vec3> x(static_cast<std::size_t>(n));
+    for (int i = 0; i < n; ++i) x[static_cast<std::size_t>(i)] = {coords[3 * i], coords[3 * i + 1], coords[3 * i + 2]};
+    const std::vector<Real> K = element_conduction(t, x, k);
+    std::memcpy(Kt, K.data(), K.size() * sizeof(double));
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// assemble_conduction (thermal.cpp:92-141) on a model built by ref_model_create, with
+// per-material conductivity and prescribed temperatures (0-based nodes).
+void* ref_assemble_conduction(void* model, int32_t n_mats, const double* k, int64_t n_tbc, const int32_t* tbc_node,
+                              const double* tbc_val) {
+  try {
+    Model& m = static_cast<RefModel*>(model)->model;
+    for (int32_t i = 0; i < n_mats; ++i) {
+      auto it = m.materials.find("M" + std::to_string(i));
+      if (it == m.materials.end()) continue;
+      Thermal th;
+      th.conductivity = PropertyTable(k[i]);
+      it->second.thermal = th;
+    }
+    m.temp_bcs.clear();
+    for (int64_t i = 0; i < n_tbc; ++i) {
+      TempBc bc;
+      bc.node_id = tbc_node[i] + 1;
+      bc.value = tbc_val[i];
+      m.temp_bcs.push_back(bc);
+    }
+    return new LinearSystem(assemble_conduction(m));
+  } catch (const std::exception& e) {
+    fail(e);
+    return nullptr;
   }
 }
 

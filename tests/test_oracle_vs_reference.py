@@ -190,3 +190,29 @@ def test_recover_stress_and_fields_identical(port, ref, etype):
     b = rm.recover_fields(u)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("etype", ALL_TYPES)
+def test_conduction_identical(port, ref, etype):
+    """element_conduction and assemble_conduction (src/fem/thermal.cpp:92-141) with
+    prescribed temperatures on one face, against the reference."""
+    for x in distorted_elements(etype, 3, seed=etype + 60, amp=0.1):
+        assert np.array_equal(port.element_conduction(etype, x, 45.0), ref.element_conduction(etype, x, 45.0))
+    quad = etype in (mg.C3D20, mg.C3D20R, mg.C3D15, mg.C3D10)
+    dims = (2, 2, 1) if quad else (3, 2, 2)
+    model = box_model(etype, *dims, jitter=0.1, seed=etype)
+    m = model.mesh
+    mats, em = per_element_materials(model)
+    k_mat = 40.0 + 5.0 * np.arange(len(mats))
+    hot = mg.face_nodes(m, 0, 0.0)
+    cold = mg.face_nodes(m, 0, float(dims[0]))
+    tn = np.concatenate([hot, cold])
+    tv = np.concatenate([np.full(hot.size, 100.0), np.full(cold.size, 20.0)])
+    rm = ref.model(m, mats, em, model.spc, model.cloads)
+    s = rm.assemble_conduction(k_mat, tn, tv)
+    deq, pre, nf = mg.thermal_dof_map(m.n_nodes, tn, tv)
+    assert np.array_equal(s["dof_eq"][:m.n_nodes], deq) and s["n_free"] == nf
+    rp, ci, v = coo_to_csr(s["n_free"], s["rows"], s["cols"], s["vals"])
+    rp2, ci2, v2, rhs2 = port.assemble_conduction(m, k_mat[em], deq, pre, nf)
+    assert np.array_equal(rp, rp2) and np.array_equal(ci, ci2) and np.array_equal(v, v2)
+    assert np.array_equal(s["rhs"], rhs2)
