@@ -8,11 +8,11 @@ system) runs in the CUDA kernels of libcxg.so, reached through its C ABI
 """
 from . import meshgen
 from ._lib import CxgError, load as load_library
-from .assembly import (LinearSystem, Material, MaterialPoints, Model, Plan, assemble_linear_static,
+from .assembly import (LinearSystem, Material, MaterialPoints, Model, Plan, ThermalPlan, assemble_linear_static,
                        assemble_material_tangent, element_stiffness, element_tangent_force,
                        make_material_points)
 from .batch import Batch
 
-__all__ = ["meshgen", "Batch", "CxgError", "load_library", "LinearSystem", "Material", "MaterialPoints", "Model",
+__all__ = ["meshgen", "Batch", "ThermalPlan", "CxgError", "load_library", "LinearSystem", "Material", "MaterialPoints", "Model",
            "Plan", "assemble_linear_static", "assemble_material_tangent", "element_stiffness",
            "element_tangent_force", "make_material_points"]

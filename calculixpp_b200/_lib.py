@@ -89,6 +89,8 @@ SIGNATURES = {
     "cxg_assemble_tangent": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cxg_assemble_mass": (C.c_int, [_vp, _vp, C.c_int32, _vp, _vp]),
     "cxg_assemble_geometric": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "cxg_thermal_plan_create": (C.c_int, [C.POINTER(CxgMeshDesc), _vp, _vp, C.c_int32, C.POINTER(_vp)]),
+    "cxg_assemble_conduction": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "cxg_recover_gauss_stress": (C.c_int, [_vp, _vp, _vp, _vp]),
     "cxg_recover_fields": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cxg_state_get": (C.c_int, [_vp, C.c_int32, _vp]),

@@ -363,6 +363,51 @@ class Plan:
 
 # ---- the reference's function names ---------------------------------------------------
 
+class ThermalPlan(Plan):
+    """A temperature plan for heat conduction (assemble_conduction, src/fem/thermal.cpp:
+    92-141): one DOF per node, prescribed temperatures tbc (node, value) eliminated."""
+
+    def __init__(self, mesh, tbc_node=(), tbc_val=(), device=None):
+        from .meshgen import thermal_dof_map
+        self.lib = _lib.load()
+        if not torch.cuda.is_available():
+            raise _lib.CxgError(_lib.CXG_ERR_NO_GPU, "no CUDA device")
+        self.device = torch.device(device or f"cuda:{torch.cuda.current_device()}")
+        self.model = Model(mesh, [Material(1.0, 0.3)])
+        deq, pre, nf = thermal_dof_map(mesh.n_nodes, tbc_node, tbc_val)
+        self.t_dof_eq, self.t_prescribed, self.n_free = deq, pre, nf
+        keep = []
+        mats = (_lib.CxgMaterial * 1)(_c_material(Material(1.0, 0.3), keep))
+        coords = _dev(mesh.coords, torch.float64, self.device)
+        conn = _dev(mesh.conn.reshape(-1), torch.int32, self.device)
+        desc = _lib.CxgMeshDesc(mesh.n_nodes, mesh.n_elems, mesh.etype, _ptr(coords), _ptr(conn), None, None, None, 1,
+                                C.cast(mats, _vp))
+        handle = _vp()
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_thermal_plan_create(C.byref(desc), _vp(deq.ctypes.data), _vp(pre.ctypes.data), nf,
+                                                        C.byref(handle)))
+        self.h = handle
+        info = _lib.CxgPlanInfo()
+        _lib.check(self.lib.cxg_plan_get_info(self.h, C.byref(info)))
+        self.info = info
+        self.nnz = int(info.nnz)
+        self.n_gauss = int(info.n_gauss_points)
+        self._pattern = None
+
+    def assemble_conduction(self, conductivity, flux=None, vals=None, rhs=None, check=True):
+        """(Kt_ff values, rhs = q_f - Kt_fc T_c); conductivity per element, flux per node."""
+        dev = self.device
+        vals = torch.empty(self.nnz, dtype=torch.float64, device=dev) if vals is None else vals
+        rhs = torch.empty(self.n_free, dtype=torch.float64, device=dev) if rhs is None else rhs
+        k = _dev(conductivity, torch.float64, dev)
+        q = None if flux is None else _dev(flux, torch.float64, dev)
+        with torch.cuda.device(dev):
+            _lib.check(self.lib.cxg_assemble_conduction(self.h, _ptr(k), _ptr(q), _ptr(vals), _ptr(rhs), _stream()))
+            if check:
+                self.check()
+        return vals, rhs
+
+
 def assemble_linear_static(model: Model, precision: str = "fp64", plan: Plan | None = None) -> LinearSystem:
     """K_ff u_f = T^T f_ext - K_fc u_c (assembly.hpp:40-42)."""
     plan = plan or Plan(model, precision)

@@ -549,6 +549,80 @@ int cxg_assemble_geometric(cxg_plan* p, const double* gp_stress, double* vals, v
   return assemble_scalar(p, 3, gp_stress, sizeof(double) * 6 * static_cast<size_t>(p->n_gauss), vals, stream);
 }
 
+int cxg_thermal_plan_create(const cxg_mesh_desc* m, const int32_t* t_dof_eq, const double* t_prescribed,
+                            int32_t n_free, cxg_plan** out) {
+  if (!m || !t_dof_eq || !t_prescribed || !out || m->n_nodes <= 0)
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "mesh, temperature DOF map and output are required");
+  const size_t N = static_cast<size_t>(m->n_nodes);
+  std::vector<int32_t> teq(N);
+  std::vector<double> tpre(N);
+  CHECK_CUDA(cudaMemcpy(teq.data(), t_dof_eq, 4 * N, cudaMemcpyDefault), "temperature DOF map");
+  CHECK_CUDA(cudaMemcpy(tpre.data(), t_prescribed, 8 * N, cudaMemcpyDefault), "prescribed temperatures");
+  // the temperature is component 0 of every node; components 1 and 2 are fixed at 0
+  std::vector<int32_t> deq(3 * N, -1);
+  std::vector<double> pre(3 * N, 0.0);
+  for (size_t a = 0; a < N; ++a) {
+    deq[3 * a] = teq[a];
+    pre[3 * a] = teq[a] < 0 ? tpre[a] : 0.0;
+  }
+  cxg_dofmap_desc d{deq.data(), pre.data(), n_free};
+  int rc = cxg_plan_create(m, &d, CXG_FP64, out);
+  if (rc) return rc;
+  (*out)->thermal = true;
+  return CXG_OK;
+}
+
+int cxg_assemble_conduction(cxg_plan* p, const double* conductivity, const double* flux, double* vals, double* rhs,
+                            void* stream) {
+  if (!p || !conductivity || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, conductivity and vals are required");
+  if (!p->thermal) return set_err(CXG_ERR_INVALID_ARGUMENT, "conduction needs a plan from cxg_thermal_plan_create");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
+  const size_t rb = sizeof(double) * static_cast<size_t>(p->n_free);
+  const size_t N = static_cast<size_t>(p->n_nodes);
+  void *dv, *dr, *dk, *df = nullptr;
+  int rc = staged(p, 0, vals, vb, false, s, &dv);
+  if (!rc) rc = staged(p, 1, rhs, rb, false, s, &dr);
+  if (!rc) rc = staged(p, 5, conductivity, sizeof(double) * static_cast<size_t>(p->n_elems), true, s, &dk);
+  if (rc) return rc;
+  if (flux) {
+    // nodal flux into component 0 of a 3N load vector (plan staging slot 2)
+    if (p->stage_bytes[2] < 24 * N) {
+      cudaFree(p->stage[2]);
+      p->stage[2] = nullptr;
+      p->stage_bytes[2] = 0;
+      CHECK_CUDA(cudaMalloc(&p->stage[2], 24 * N), "flux staging");
+      p->stage_bytes[2] = 24 * N;
+    }
+    df = p->stage[2];
+    CHECK_CUDA(cudaMemsetAsync(df, 0, 24 * N, s), "flux staging");
+    CHECK_CUDA(cudaMemcpy2DAsync(df, 24, flux, 8, 8, N, cudaMemcpyDefault, s), "flux upload");
+  }
+  const size_t need = v2_edata_bytes(p->type, p->n_elems, CXG_FP64);
+  if (p->edata_bytes < need) {
+    cudaFree(p->edata);
+    p->edata = nullptr;
+    p->device_bytes -= static_cast<int64_t>(p->edata_bytes);
+    p->edata_bytes = 0;
+    CHECK_CUDA(cudaMalloc(&p->edata, std::max<size_t>(need, 16)), "element buffer");
+    p->edata_bytes = need;
+    p->device_bytes += static_cast<int64_t>(need);
+  }
+  ElemArgs a = base_args(p);
+  a.vals = static_cast<double*>(dv);
+  a.rhs = static_cast<double*>(dr);
+  const V2Args v = v2_args(p, static_cast<const double*>(df), false);
+  CHECK_CUDA(launch_scalar_pass(p->type, 4, a, v, static_cast<const double*>(dk), nullptr, s), "element pass");
+  LaunchCfg gather_only;
+  gather_only.passes = 2;
+  CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, CXG_FP64, a, v, s, gather_only), "row gather");
+  if ((rc = copy_out(vals, dv, vb, s))) return rc;
+  if ((rc = copy_out(rhs, dr, rb, s))) return rc;
+  if (dv != vals || (rhs && dr != rhs)) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
+  return CXG_OK;
+}
+
 int cxg_recover_gauss_stress(cxg_plan* p, const double* u, double* gp_stress, void* stream) {
   if (!p || !u || !gp_stress) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, u and gp_stress are required");
   if (p->has_plastic) return set_err(CXG_ERR_UNSUPPORTED, "Gauss-point stress recovery is for linear elasticity");

@@ -115,8 +115,9 @@ struct LaunchCfg {
 size_t v2_edata_bytes(int elem_type, int64_t n_elems, int precision);
 // Element pass of the scalar-block operators (every 3x3 block is a scalar times I):
 // kind 1 consistent mass rho N_a N_b, 2 lumped mass (row sums on the diagonal), 3
-// geometric stiffness g_a . sigma . g_b. Writes FP64 blocks for the FP64 row gather.
-// density[E] (kinds 1, 2), gp_stress[6 G] (kind 3).
+// geometric stiffness g_a . sigma . g_b, 4 conduction k g_a . g_b. Writes FP64 blocks
+// for the FP64 row gather. density[E] is rho (kinds 1, 2) or k (kind 4), gp_stress[6 G]
+// (kind 3).
 cudaError_t launch_scalar_pass(int elem_type, int kind, const ElemArgs& a, const V2Args& v, const double* density,
                                const double* gp_stress, cudaStream_t s);
 cudaError_t launch_v2(int elem_type, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s,

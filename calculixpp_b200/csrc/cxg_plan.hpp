@@ -36,6 +36,7 @@ struct cxg_plan {
   size_t stage_bytes[6] = {0, 0, 0, 0, 0, 0};
   cxg::LaunchCfg cfg[2];   // launch shape of the linear passes per precision (FP64, mixed)
   cxg::LaunchCfg tcfg[2];  // launch shape of the material-point (tangent) passes
+  bool thermal = false;    // temperature plan: DOF 0 of every node, components 1 and 2 fixed
 };
 
 

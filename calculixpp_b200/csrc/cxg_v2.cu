@@ -874,20 +874,22 @@ cudaError_t launch_v2_type(int mode, int precision, const ElemArgs& a, const V2A
 // (element_geometric_stiffness + accumulate_kgeo, element.cpp:482-508, 833-854). One
 // warp per element: lanes take Gauss points for detJ (and the gradients), then node
 // pairs (a <= b) for the scalar sums; the blocks go to the FP64 element buffer the row
-// gather reads.
+// gather reads. The conduction matrix k_ab = sum_q k detJ w g_a . g_b
+// (element_conduction, element.cpp:745-765) has the same shape and takes kind 4; its
+// plan carries the temperature as component 0 of every node.
 constexpr int kScalarWarps = 4;
 
 template <int ET, int KIND>
 constexpr int scalar_warp_doubles() {
   constexpr int n = nodes_of(ET), nq = gauss_of(ET);
-  return 3 * n + nq + (KIND == 3 ? nq * n * 3 + nq * 6 : 0);
+  return 3 * n + nq + (KIND >= 3 ? nq * n * 3 : 0) + (KIND == 3 ? nq * 6 : 0);
 }
 
 template <int ET, int KIND>
 __global__ void __launch_bounds__(kScalarWarps * 32) scalar_kernel(ElemArgs A, V2Args V, const double* density,
                                                                    const double* gp_stress) {
   constexpr int n = nodes_of(ET), nq = gauss_of(ET), NB = n * (n + 1) / 2;
-  constexpr bool GEO = KIND == 3;
+  constexpr bool GEO = KIND == 3, GRAD = KIND >= 3;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned char s_pa[NB], s_pb[NB];
   for (int p = threadIdx.x; p < NB; p += blockDim.x) {
@@ -902,7 +904,7 @@ __global__ void __launch_bounds__(kScalarWarps * 32) scalar_kernel(ElemArgs A, V
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* x = reinterpret_cast<double*>(smem) + warp * scalar_warp_doubles<ET, KIND>();
-  double* sq = x + 3 * n;   // [nq] rho detJ w (mass) or detJ w (geometric)
+  double* sq = x + 3 * n;   // [nq] rho detJ w (mass), detJ w (geometric), k detJ w (conduction)
   double* g = sq + nq;      // [nq][n][3] physical gradients (geometric)
   double* sig = g + nq * n * 3;  // [nq][6] stress (geometric)
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * kScalarWarps + warp;
@@ -923,10 +925,10 @@ __global__ void __launch_bounds__(kScalarWarps * 32) scalar_kernel(ElemArgs A, V
         atomicCAS(&A.status->code, 0, 4);
         atomicMin(&A.status->bad_elem, static_cast<unsigned long long>(e));
       }
-      if (!GEO) {
+      if (!GRAD) {
         sq[q] = density[e] * det * c_w[ET][q];
       } else {
-        sq[q] = det * c_w[ET][q];
+        sq[q] = GEO ? det * c_w[ET][q] : density[e] * det * c_w[ET][q];
         const double inv = 1.0 / det;
         const double it[3][3] = {
             {c00 * inv, c01 * inv, c02 * inv},
@@ -939,7 +941,8 @@ __global__ void __launch_bounds__(kScalarWarps * 32) scalar_kernel(ElemArgs A, V
                        d2 = c_dN[dn_offset(ET) + (3 * k + 2) * nq + q];
           for (int i = 0; i < 3; ++i) g[(q * n + k) * 3 + i] = it[i][0] * d0 + it[i][1] * d1 + it[i][2] * d2;
         }
-        for (int c = 0; c < 6; ++c) sig[q * 6 + c] = gp_stress ? gp_stress[(e * nq + q) * 6 + c] : 0.0;
+        if (GEO)
+          for (int c = 0; c < 6; ++c) sig[q * 6 + c] = gp_stress ? gp_stress[(e * nq + q) * 6 + c] : 0.0;
       }
     }
     __syncwarp();
@@ -957,6 +960,12 @@ __global__ void __launch_bounds__(kScalarWarps * 32) scalar_kernel(ElemArgs A, V
               m += sq[q] * c_N[nn_offset(ET) + a * nq + q] * c_N[nn_offset(ET) + bb * nq + q];
             val += m;
           }
+      } else if (KIND == 4) {
+        for (int q = 0; q < nq; ++q) {
+          const double* ga = g + (q * n + a) * 3;
+          const double* gb = g + (q * n + b) * 3;
+          val += sq[q] * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+        }
       } else {
         for (int q = 0; q < nq; ++q) {
           const double* ga = g + (q * n + a) * 3;
@@ -998,6 +1007,7 @@ cudaError_t launch_scalar_type(int kind, const ElemArgs& a, const V2Args& v, con
     case 1: return launch_scalar_t<ET, 1>(a, v, density, gp_stress, s);
     case 2: return launch_scalar_t<ET, 2>(a, v, density, gp_stress, s);
     case 3: return launch_scalar_t<ET, 3>(a, v, density, gp_stress, s);
+    case 4: return launch_scalar_t<ET, 4>(a, v, density, gp_stress, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -189,6 +189,18 @@ CXG_API int cxg_assemble_mass(cxg_plan* plan, const double* density, int32_t lum
  * order then the Gauss rule's order; NULL means a zero field. */
 CXG_API int cxg_assemble_geometric(cxg_plan* plan, const double* gp_stress, double* vals, void* stream);
 
+/* ---- heat conduction (assemble_conduction, src/fem/thermal.cpp:92-141, without films)
+ * A temperature plan carries one DOF per node: t_dof_eq[n_nodes] (free equation or -1,
+ * free nodes numbered in node order, build_thermal_dof_map, thermal.cpp:71-90) and
+ * t_prescribed[n_nodes]; its pattern is the scalar conduction pattern. The mesh's
+ * materials are not used. cxg_assemble_conduction writes Kt_ff (element_conduction,
+ * element.cpp:745-765: k detJ w g_a . g_b) and rhs = q_f - Kt_fc T_c; conductivity is
+ * per element, flux[n_nodes] (may be NULL) is added at the free nodes. */
+CXG_API int cxg_thermal_plan_create(const cxg_mesh_desc* mesh, const int32_t* t_dof_eq, const double* t_prescribed,
+                                    int32_t n_free, cxg_plan** out);
+CXG_API int cxg_assemble_conduction(cxg_plan* plan, const double* conductivity, const double* flux, double* vals,
+                                    double* rhs, void* stream);
+
 /* ---- field recovery from a displacement field u[3*n_nodes] (linear elasticity) -------
  * recover_gauss_stress (src/fem/stress.cpp:147-187): gp_stress[6 * n_gauss_points],
  * sigma = D B u_e per Gauss point (Voigt, engineering shear), element order. */
