@@ -239,6 +239,42 @@ def j2_newton(args, world, dev, stream):
     return res
 
 
+def plain_fp64_per_model(models, args, dev, stream):
+    """The plain FP64 drop-in path on the batched workload: one plan and one assembly
+    call per model (no batching, no graph), each model's assembly timed with CUDA events
+    (median of args.steps after args.warmup), summed over the models. Plans are built one
+    at a time so device memory stays bounded."""
+    import torch
+
+    from calculixpp_b200 import Plan
+    total = 0.0
+    elems = 0
+    for model in models:
+        plan = Plan(model, "fp64")
+        f = torch.as_tensor(model.external_load_vector(), device=dev)
+        vals = torch.empty(plan.nnz, dtype=torch.float64, device=dev)
+        rhs = torch.empty(plan.n_free, dtype=torch.float64, device=dev)
+        for _ in range(args.warmup):
+            plan.assemble_linear(f, vals=vals, rhs=rhs, check=False)
+        plan.check()
+        times = []
+        for _ in range(max(args.steps, 1)):
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            plan.assemble_linear(f, vals=vals, rhs=rhs, check=False)
+            s1.record(stream)
+            s1.synchronize()
+            times.append(s0.elapsed_time(s1))
+        plan.check()
+        total += sorted(times)[len(times) // 2]
+        elems += model.mesh.n_elems
+        del vals, rhs, f
+        plan.close()
+    torch.cuda.empty_cache()
+    return {"value": elems / (total * 1e-3), "ms_total": total,
+            "how": "one FP64 plan per model, one assembly call each, per-model median event time summed"}
+
+
 def batched(args, world, rank, dev, stream):
     """Batched mixed-element models: the autotuned batch replayed as one CUDA graph per
     step (all groups as parallel branches), mixed precision; FP64 on the same batch when
@@ -267,6 +303,12 @@ def batched(args, world, rank, dev, stream):
                 raise
             models = models[: len(models) // 2]
     E_tot = sum(m.mesh.n_elems for m in models)
+    E_all = E_tot  # elements over all ranks (each rank draws its own models)
+    if world > 1:
+        import torch.distributed as dist
+        e = torch.tensor([float(E_tot)], dtype=torch.float64, device=dev)
+        dist.all_reduce(e, op=dist.ReduceOp.SUM)
+        E_all = float(e.item())
     by_type = {}
     for m in models:
         name = mg.TYPE_NAMES[m.mesh.etype]
@@ -288,7 +330,7 @@ def batched(args, world, rank, dev, stream):
         barrier(world)
         t = max_over_ranks(time_steps(step, args.steps, stream), world)
         b.check()
-        return {"value": world * E_tot * args.steps / t, "ms_per_step": t / args.steps * 1e3,
+        return {"value": E_all * args.steps / t, "ms_per_step": t / args.steps * 1e3,
                 "tune_s": t_tune, "group_configs": cfg}
 
     res = {"workload": f"{len(models)} independent boxes, element counts log-uniform in [1e3, 2e5], types "
@@ -297,6 +339,7 @@ def batched(args, world, rank, dev, stream):
                        "parallel branches)",
            "models": len(models), "elements": E_tot, "elements_by_type": by_type, "nnz": b.nnz,
            "n_free": b.n_free, "plan_build_s": t_build}
+    plain = plain_fp64_per_model(models, args, dev, stream) if world == 1 else None
     res["mixed"] = run("mixed")
     keep = vals.clone() if b.nnz * 8 < 0.2 * torch.cuda.mem_get_info()[0] else None
     free = torch.cuda.mem_get_info()[0]
@@ -304,7 +347,13 @@ def batched(args, world, rank, dev, stream):
     # released before its FP64 successor is allocated)
     # (padded 3x3 blocks: 80 B in FP64, 48 B in FP32)
     fp64_extra = sum(m.mesh.n_elems * (m.mesh.conn.shape[1] * (m.mesh.conn.shape[1] + 1) // 2) * 80 for m in models)
-    if free + fp64_extra * 0.6 > 1.05 * fp64_extra + 4e9:
+    fits = free + fp64_extra * 0.6 > 1.05 * fp64_extra + 4e9
+    if world > 1:  # every rank takes the same branch (the FP64 run holds collectives)
+        import torch.distributed as dist
+        flag = torch.tensor([1.0 if fits else 0.0], device=dev)
+        dist.all_reduce(flag, op=dist.ReduceOp.MIN)
+        fits = bool(flag.item() > 0.5)
+    if fits:
         res["fp64"] = run("fp64")
         res["speedup_mixed_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
         if keep is not None:
@@ -312,6 +361,9 @@ def batched(args, world, rank, dev, stream):
     else:
         res["fp64"] = {"skipped": f"FP64 element buffers ({fp64_extra / 1e9:.1f} GB) exceed free device memory "
                                   f"({free / 1e9:.1f} GB) plus the FP32 buffers they replace"}
+    if plain is not None:
+        res["plain_fp64_per_model"] = plain
+        res["speedup_batched_mixed_vs_plain_fp64"] = plain["ms_total"] / res["mixed"]["ms_per_step"]
     del keep, vals, rhs, f
     b.close()
     torch.cuda.empty_cache()
