@@ -225,17 +225,34 @@ struct Vec4<double> {
 // slot(k) = k/2 for even k and npad/2 + k/2 for odd k, so the row nodes 2r + i of the
 // lanes' tiles occupy consecutive slots. FP32 vectors are float4 per slot; FP64 vectors
 // are split in two half planes of double2 (x,y | z,0) so consecutive slots are 16 bytes
-// apart. Either way one warp-wide vector load touches distinct banks.
+// apart. Either way one warp-wide vector load touches distinct banks. The plane block of
+// each (element, Gauss point) is followed by 16 bytes of padding: the blocks then start
+// 16 (mod 128) bytes apart, so the lanes of the Gauss-point phase, one block each,
+// store their vectors into 8 distinct 16-byte bank groups instead of one.
 __host__ __device__ constexpr int node_slot(int k, int npad) { return (k & 1) ? npad / 2 + (k >> 1) : (k >> 1); }
 
 template <typename R, int NPAD>
 struct VecIdx {
-  // flat index of component c of the vector in `slot` of plane block b (b = element*nq + q)
+  // elements of one plane block (b = element*nq + q), padding included
+  static constexpr int kBlock = NPAD * 4 + (sizeof(R) == 4 ? 4 : 2);
+  // flat index of component c of the vector in `slot` of plane block b
   __device__ __forceinline__ static int at(int b, int slot, int c) {
-    if (sizeof(R) == 4) return (b * NPAD + slot) * 4 + c;
-    return ((b * 2 + (c >> 1)) * NPAD + slot) * 2 + (c & 1);
+    if (sizeof(R) == 4) return b * kBlock + slot * 4 + c;
+    return b * kBlock + (c >> 1) * (NPAD * 2) + slot * 2 + (c & 1);
   }
 };
+
+// one vector store (x, y, z, 0) of a node vector
+template <typename R, int NPAD>
+__device__ __forceinline__ void st3(R* base, int b, int slot, double x, double y, double z) {
+  if constexpr (sizeof(R) == 4) {
+    *reinterpret_cast<float4*>(base + VecIdx<R, NPAD>::at(b, slot, 0)) =
+        make_float4(static_cast<float>(x), static_cast<float>(y), static_cast<float>(z), 0.f);
+  } else {
+    *reinterpret_cast<double2*>(base + VecIdx<R, NPAD>::at(b, slot, 0)) = make_double2(x, y);
+    *reinterpret_cast<double2*>(base + VecIdx<R, NPAD>::at(b, slot, 2)) = make_double2(z, 0.0);
+  }
+}
 
 template <typename R, int NPAD>
 __device__ __forceinline__ void ld3(const R* base, int b, int slot, R& x, R& y, R& z) {
@@ -258,19 +275,21 @@ struct P1Smem {
   using G = Geo<ET, TILE>;
   static constexpr int n = G::n, nq = G::nq, npad = G::npad, EPW = G::EPW;
   static constexpr bool T = MODE == MODE_TANGENT;
-  R g[EPW * nq * npad * 4];                       // node vectors, see VecIdx
-  R m[T ? EPW * nq * npad * 4 : 4];
+  static constexpr int kVec = EPW * nq * VecIdx<R, npad>::kBlock;
+  static constexpr int HG = ET == C3D8R ? EPW : 1;  // hourglass data (C3D8R only)
+  R g[kVec];                                      // node vectors, see VecIdx
+  R m[T ? kVec : 4];
   R s[EPW][nq];
   R dp[T ? EPW : 1][T ? nq : 1][4];
   double x[EPW][3 * n];
   double u[T ? EPW : 1][T ? 3 * n : 1];
   double sig[T ? EPW : 1][T ? nq : 1][6];
   double lam[EPW], mu[EPW], mu_j2[EPW];
-  double gam[EPW][32];
-  double kappa[EPW];
-  double gc[EPW][3 * n];
-  double vol[EPW];
-  double mu_hg[EPW];
+  double gam[HG][32];
+  double kappa[HG];
+  double gc[HG][3 * n];
+  double vol[HG];
+  double mu_hg[HG];
   int plastic[EPW];
 };
 
@@ -317,7 +336,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
     }
   }
   // zero the padded gradient slots once; they are never written afterwards
-  for (int t = lane; t < EPW * nq * npad * 4; t += 32) {
+  for (int t = lane; t < WS::kVec; t += 32) {
     W.g[t] = R(0);
     if (TAN) W.m[t % (sizeof(W.m) / sizeof(R))] = R(0);
   }
@@ -380,16 +399,16 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
            (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * inv}};
       const double sq = det * sw[q];
       W.s[ei][q] = static_cast<R>(sq);
-      if (ET == C3D8R) W.vol[ei] = sq;
+      if constexpr (ET == C3D8R) W.vol[ei] = sq;
       double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
       for (int k = 0; k < n; ++k) {
         const double d0 = sdN[(3 * k) * nq + q], d1 = sdN[(3 * k + 1) * nq + q], d2 = sdN[(3 * k + 2) * nq + q];
         double gk[3];
         for (int i = 0; i < 3; ++i) {
           gk[i] = it[i][0] * d0 + it[i][1] * d1 + it[i][2] * d2;
-          W.g[VecIdx<R, npad>::at(ei * nq + q, node_slot(k, npad), i)] = static_cast<R>(gk[i]);
-          if (ET == C3D8R) W.gc[ei][i * n + k] = gk[i];
+          if constexpr (ET == C3D8R) W.gc[ei][i * n + k] = gk[i];
         }
+        st3<R, npad>(W.g, ei * nq + q, node_slot(k, npad), gk[0], gk[1], gk[2]);
         if (TAN)
           for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j) H[i][j] = fma(W.u[ei][3 * k + i], gk[j], H[i][j]);
@@ -411,19 +430,21 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
           W.plastic[ei] = 1;
           for (int k = 0; k < n; ++k) {
             const int b = ei * nq + q, sl = node_slot(k, npad);
-            const double gx = W.g[VecIdx<R, npad>::at(b, sl, 0)], gy = W.g[VecIdx<R, npad>::at(b, sl, 1)],
-                         gz = W.g[VecIdx<R, npad>::at(b, sl, 2)];
-            W.m[VecIdx<R, npad>::at(b, sl, 0)] = static_cast<R>(nv[0] * gx + nv[3] * gy + nv[4] * gz);
-            W.m[VecIdx<R, npad>::at(b, sl, 1)] = static_cast<R>(nv[3] * gx + nv[1] * gy + nv[5] * gz);
-            W.m[VecIdx<R, npad>::at(b, sl, 2)] = static_cast<R>(nv[4] * gx + nv[5] * gy + nv[2] * gz);
+            R rx, ry, rz;
+            ld3<R, npad>(W.g, b, sl, rx, ry, rz);
+            const double gx = rx, gy = ry, gz = rz;
+            st3<R, npad>(W.m, b, sl, nv[0] * gx + nv[3] * gy + nv[4] * gz, nv[3] * gx + nv[1] * gy + nv[5] * gz,
+                         nv[4] * gx + nv[5] * gy + nv[2] * gz);
           }
         }
-        if (q == nq - 1) W.mu_hg[ei] = mhg;
+        if constexpr (ET == C3D8R) {
+          if (q == nq - 1) W.mu_hg[ei] = mhg;
+        }
       }
     }
     __syncwarp();
     // ---- C3D8R hourglass vectors (src/fem/element.cpp:545-579) ------------------------
-    if (ET == C3D8R) {
+    if constexpr (ET == C3D8R) {
       for (int t = lane; t < EPW * 4; t += 32) {
         const int ei = t / 4, al = t % 4;
         double gx[3] = {0, 0, 0};
@@ -543,7 +564,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
             const int a = a0 + i, b = b0 + j;
             if (a < n && b < n && a <= b) {
               R h = R(0);
-              if (ET == C3D8R) {
+              if constexpr (ET == C3D8R) {
                 double hd = 0.0;
                 for (int al = 0; al < 4; ++al) hd += W.gam[ei][al * 8 + a] * W.gam[ei][al * 8 + b];
                 h = static_cast<R>(hd * W.kappa[ei]);
@@ -565,14 +586,14 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
         double f[3] = {0, 0, 0};
         for (int q = 0; q < nq; ++q) {
           const double* S = W.sig[ei][q];
-          const int gb_ = ei * nq + q, sl = node_slot(a, npad);
-          const double gx = W.g[VecIdx<R, npad>::at(gb_, sl, 0)], gy = W.g[VecIdx<R, npad>::at(gb_, sl, 1)],
-                       gz = W.g[VecIdx<R, npad>::at(gb_, sl, 2)];
+          R rx, ry, rz;
+          ld3<R, npad>(W.g, ei * nq + q, node_slot(a, npad), rx, ry, rz);
+          const double gx = rx, gy = ry, gz = rz;
           f[0] += S[0] * gx + S[3] * gy + S[4] * gz;
           f[1] += S[3] * gx + S[1] * gy + S[5] * gz;
           f[2] += S[4] * gx + S[5] * gy + S[2] * gz;
         }
-        if (ET == C3D8R) {
+        if constexpr (ET == C3D8R) {
           for (int al = 0; al < 4; ++al) {
             double gu[3] = {0, 0, 0};
             for (int j = 0; j < 8; ++j)
