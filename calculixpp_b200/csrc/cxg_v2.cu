@@ -669,8 +669,8 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   constexpr int GS = P2Geo<ET>::GS, EG = P2Geo<ET>::EG;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t stride = V.row_stride;
-  double* buf = reinterpret_cast<double*>(smem) + static_cast<int64_t>(warp) * (EG * stride);
+  const int stride = static_cast<int>(V.row_stride);  // shared-memory offsets are 32-bit
+  double* buf = reinterpret_cast<double*>(smem) + warp * (EG * stride);
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   const R* ed = reinterpret_cast<const R*>(V.edata);
@@ -680,13 +680,16 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   for (int64_t a = gwarp; a < A.n_nodes; a += nwarps) {
     const int ma = A.node_mask[a];
     const int nf = __popc(ma);
-    const int64_t L = A.node_rowlen[a];
-    const int64_t total = nf * L;
-    const int64_t base = A.node_base[a];
+    const int L = static_cast<int>(A.node_rowlen[a]);
+    const int total = nf * L;
+    double* vout = A.vals + A.node_base[a];
     const int64_t i0 = V.inc_ptr[a], i1 = V.inc_ptr[a + 1];
+    // offset of row i (free component i of node a) in the row buffer
+    int row_off[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) row_off[i] = __popc(ma & ((1 << i) - 1)) * L;
     for (int g = 0; g < EG; ++g)
-      for (int64_t t = lane; t < total; t += 32)
-        buf[g * stride + t] = (g == 0 && V.accumulate) ? A.vals[base + t] : 0.0;
+      for (int t = lane; t < total; t += 32) buf[g * stride + t] = (g == 0 && V.accumulate) ? vout[t] : 0.0;
     __syncwarp();
     double rr[3] = {0.0, 0.0, 0.0};
     double fs[3] = {0.0, 0.0, 0.0};
@@ -701,19 +704,31 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
         P2Pass<R> cur;
         p2_fetch<ET, R>(A, ed, __shfl_sync(0xffffffffu, code_l, (k + sub) & 31), lane_ok && k + sub < cnt, lb, cur);
         if (cur.active && (!DIAGFIX || lb != cur.la)) {
-          int64_t nb = -1;
+          double* col = mine + cur.slotv;
+          if (cur.mb == 7) {  // every component of the column node is free
 #pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            if (!((ma >> i) & 1)) continue;
-            const int64_t row = __popc(ma & ((1 << i) - 1)) * L + cur.slotv;
+            for (int i = 0; i < 3; ++i) {
+              if ((ma >> i) & 1) {
+                double* r = col + row_off[i];
+                r[0] += cur.v[3 * i];
+                r[1] += cur.v[3 * i + 1];
+                r[2] += cur.v[3 * i + 2];
+              }
+            }
+          } else {
+            int64_t nb = -1;
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-              if ((cur.mb >> j) & 1) {
-                mine[row + __popc(cur.mb & ((1 << j) - 1))] += cur.v[3 * i + j];
-              } else {
-                if (nb < 0) nb = A.conn[cur.e * n + lb];
-                const double pv = A.prescribed[3 * nb + j];
-                if (pv != 0.0) rr[i] -= cur.v[3 * i + j] * pv;
+            for (int i = 0; i < 3; ++i) {
+              if (!((ma >> i) & 1)) continue;
+#pragma unroll
+              for (int j = 0; j < 3; ++j) {
+                if ((cur.mb >> j) & 1) {
+                  col[row_off[i] + __popc(cur.mb & ((1 << j) - 1))] += cur.v[3 * i + j];
+                } else {
+                  if (nb < 0) nb = A.conn[cur.e * n + lb];
+                  const double pv = A.prescribed[3 * nb + j];
+                  if (pv != 0.0) rr[i] -= cur.v[3 * i + j] * pv;
+                }
               }
             }
           }
@@ -753,7 +768,8 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
           if (q == lane) d = d9[q];
         if ((ma >> i) & 1) {
           if ((ma >> j) & 1) {
-            buf[__popc(ma & ((1 << i) - 1)) * L + slot_aa + __popc(ma & ((1 << j) - 1))] += d;
+            const int ro = i == 0 ? row_off[0] : (i == 1 ? row_off[1] : row_off[2]);
+            buf[ro + slot_aa + __popc(ma & ((1 << j) - 1))] += d;
           } else {
             const double pv = A.prescribed[3 * a + j];
             if (pv != 0.0) rr[i] -= d * pv;
@@ -782,11 +798,11 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
         if (lane == 0) A.f_int[3 * a + d] = (V.accumulate ? A.f_int[3 * a + d] : 0.0) + v;
       }
     }
-    for (int64_t t = lane; t < total; t += 32) {
+    for (int t = lane; t < total; t += 32) {
       double v = buf[t];
 #pragma unroll
       for (int g = 1; g < EG; ++g) v += buf[g * stride + t];
-      A.vals[base + t] = v;
+      vout[t] = v;
     }
     __syncwarp();
   }
