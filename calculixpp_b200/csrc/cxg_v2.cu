@@ -610,9 +610,14 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 }
 
 // ---- P2: row gather ------------------------------------------------------------------
-// One warp per node a. Lanes form EG groups of GS lanes (GS = n rounded up to a power of
-// two); lane lb of group s handles column node lb of incident element k + s, so EG
-// elements are applied per pass. Each group adds into its own copy of the node's rows
+// One warp per node a. Lanes form EG groups of GS lanes (GS = 16 for elements of at
+// most 16 nodes, else 32; 8 for the <= 8-node families in mixed precision); lane lb of
+// group s handles column node lb of incident element k + s, so EG elements are applied
+// per pass. Every group copy of the rows is zeroed and read once per node, which for the
+// short rows of the <= 8-node families in FP64 costs more shared-memory traffic than
+// the idle lanes of two 16-lane groups (measured: the FP64 C3D8 tangent gather is 10 %
+// faster with two groups than with four, the mixed one 3 % slower, so it keeps four).
+// Each group adds into its own copy of the node's rows
 // in shared memory (within one element every target is distinct, so plain adds, no
 // atomics); the copies are summed in a fixed order when the rows are stored. The
 // node's incident-element codes come in with one coalesced load per 32 elements and
@@ -623,10 +628,10 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 // its element rows: every lane keeps a running sum of the blocks it adds, and one
 // butterfly over the warp per node forms the block, so rigid translations stay in the
 // null space of the assembled rows to FP64 accuracy.
-template <int ET>
+template <int ET, bool DIAGFIX>
 struct P2Geo {
   static constexpr int n = nodes_of(ET);
-  static constexpr int GS = n <= 8 ? 8 : (n <= 16 ? 16 : 32);
+  static constexpr int GS = (DIAGFIX && n <= 8) ? 8 : (n <= 16 ? 16 : 32);
   static constexpr int EG = 32 / GS;
 };
 
@@ -666,7 +671,7 @@ __device__ __forceinline__ void p2_fetch(const ElemArgs& A, const R* ed, int cod
 template <int ET, bool TAN, typename R, bool DIAGFIX>
 __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   constexpr int n = nodes_of(ET);
-  constexpr int GS = P2Geo<ET>::GS, EG = P2Geo<ET>::EG;
+  constexpr int GS = P2Geo<ET, DIAGFIX>::GS, EG = P2Geo<ET, DIAGFIX>::EG;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int stride = static_cast<int>(V.row_stride);  // shared-memory offsets are 32-bit
@@ -871,7 +876,7 @@ cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaS
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
   // configured count when it fits)
   const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
-  const int64_t wbytes = P2Geo<ET>::EG * stride * 8;
+  const int64_t wbytes = P2Geo<ET, DF>::EG * stride * 8;
   int warps = cfg.p2_warps > 0 ? std::min(cfg.p2_warps, 8) : 8;
   while (warps > 1 && warps * wbytes > 160 * 1024) warps /= 2;
   const size_t smem = static_cast<size_t>(warps) * wbytes;

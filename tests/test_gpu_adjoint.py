@@ -3,7 +3,8 @@
 * dc/dX of the 4x2x2 C3D8 cantilever against the reference's own solve_sensitivity
   output (tests/golden, semi-analytic central differences with h = 1e-4): 1e-6 relative.
 * dc/dE and dc/dX against central finite differences (step 1e-6, 64 random components)
-  through the differentiable forward (device assembly + device CG at rtol 1e-13).
+  through the differentiable forward (device assembly + device CG at rtol 1e-12); the
+  dc/dX bar adds the difference quotient's CG noise, about rtol*|c|/h.
 * every full-integration family: dc/dX against the oracle's per-element central
   differences of K_e.
 * the device CG against scipy's direct solve; non-convergence reported as an error."""
@@ -78,6 +79,11 @@ def test_autograd_matches_central_differences(cuda):
         Em[k] -= h
         fd = (c_at(Ep, X.detach()) - c_at(Em, X.detach())) / (2 * h)
         assert abs(fd - float(gE[k])) <= 1e-5 * abs(float(gE[k])) + 1e-12 * abs(float(c)), (k, fd, float(gE[k]))
+    # each compliance evaluation carries the CG's own error (the forward's CG stops at
+    # rtol 1e-12, about rtol*|c|); the two evaluations of a central difference take
+    # different CG paths, so the quotient carries up to ~rtol*|c|/h of noise on top of
+    # the 1e-5 relative bar
+    cg_noise = 4 * 1e-12 * abs(float(c))
     for k in range(32):
         node = int(rng.choice(free_nodes))
         comp = int(rng.integers(3))
@@ -87,7 +93,8 @@ def test_autograd_matches_central_differences(cuda):
         Xm[node, comp] -= h
         fd = (c_at(E.detach(), Xp) - c_at(E.detach(), Xm)) / (2 * h)
         g = float(gX[node, comp])
-        assert abs(fd - g) <= 1e-5 * max(abs(g), 1e-3 * float(gX.abs().max())), (node, comp, fd, g)
+        tol = 1e-5 * max(abs(g), 1e-3 * float(gX.abs().max())) + cg_noise / h
+        assert abs(fd - g) <= tol, (node, comp, fd, g, tol)
 
 
 @pytest.mark.parametrize("etype", [mg.C3D20, mg.C3D20R, mg.C3D6, mg.C3D15, mg.C3D4, mg.C3D10])
