@@ -464,12 +464,21 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
       __syncwarp();
     }
     // ---- phase C: TR x TC node-pair tiles ---------------------------------------------
+    // Staged stores (FP64 linear mode, one tile per lane, the element's blocks fit the
+    // gradient area): once every tile is done the gradient vectors are dead, so the lanes
+    // put their blocks there unpadded and the warp writes the padded element buffer with
+    // consecutive 16-byte stores, instead of every lane writing its own 80-byte blocks
+    // across the element's buffer (about one cache line per lane and store instruction).
+    // Measured on C3D20 64^3: FP64 6.25 -> 6.10 ms per assembly; in FP32 the staging
+    // raised the 2x4 tile's registers from 126 to 168 and lost, so FP32 stores directly.
+    constexpr bool STAGE =
+        MODE == MODE_LINEAR && sizeof(R) == 8 && EPW * NT <= 32 && EPW * NB * 9 <= WS::kVec;
+    R acc[TR][TC][9];
     for (int task = lane; task < EPW * NT; task += 32) {
       const int ei = task / NT, ti = task % NT;
       const int64_t e = e0 + ei;
       if (e < A.n_elems) {
         const int a0 = TR * s_tr[ti], b0 = TC * s_tc[ti];
-        R acc[TR][TC][9];
 #pragma unroll
         for (int i = 0; i < TR; ++i)
 #pragma unroll
@@ -556,26 +565,71 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
             }
           }
         }
-        R* out = reinterpret_cast<R*>(V.edata) + e * (NB * blk_stride<R>());
+        if constexpr (!STAGE) {
+          R* out = reinterpret_cast<R*>(V.edata) + e * (NB * blk_stride<R>());
 #pragma unroll
-        for (int i = 0; i < TR; ++i)
+          for (int i = 0; i < TR; ++i)
 #pragma unroll
-          for (int j = 0; j < TC; ++j) {
-            const int a = a0 + i, b = b0 + j;
-            if (a < n && b < n && a <= b) {
-              R h = R(0);
-              if constexpr (ET == C3D8R) {
-                double hd = 0.0;
-                for (int al = 0; al < 4; ++al) hd += W.gam[ei][al * 8 + a] * W.gam[ei][al * 8 + b];
-                h = static_cast<R>(hd * W.kappa[ei]);
+            for (int j = 0; j < TC; ++j) {
+              const int a = a0 + i, b = b0 + j;
+              if (a < n && b < n && a <= b) {
+                R h = R(0);
+                if constexpr (ET == C3D8R) {
+                  double hd = 0.0;
+                  for (int al = 0; al < 4; ++al) hd += W.gam[ei][al * 8 + a] * W.gam[ei][al * 8 + b];
+                  h = static_cast<R>(hd * W.kappa[ei]);
+                }
+                R bv[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) bv[k] = acc[i][j][k] + ((k % 4 == 0) ? h : R(0));
+                store_block<R>(out + blk_index(n, a, b) * blk_stride<R>(), bv);
               }
-              R bv[9];
-#pragma unroll
-              for (int k = 0; k < 9; ++k) bv[k] = acc[i][j][k] + ((k % 4 == 0) ? h : R(0));
-              store_block<R>(out + blk_index(n, a, b) * blk_stride<R>(), bv);
             }
-          }
+        }
       }
+    }
+    if constexpr (STAGE) {
+      static_assert(ET != C3D8R, "staged stores carry no hourglass term");
+      constexpr int BS = blk_stride<R>(), PER = 16 / static_cast<int>(sizeof(R)), CPB = BS / PER;
+      __syncwarp();  // every lane is done reading the gradient vectors
+      R* stg = W.g;  // EPW x NB blocks of 9 values
+      if (lane < EPW * NT) {
+        const int ei = lane / NT, ti = lane % NT;
+        if (e0 + ei < A.n_elems) {
+          const int a0 = TR * s_tr[ti], b0 = TC * s_tc[ti];
+#pragma unroll
+          for (int i = 0; i < TR; ++i)
+#pragma unroll
+            for (int j = 0; j < TC; ++j) {
+              const int a = a0 + i, b = b0 + j;
+              if (a < n && b < n && a <= b) {
+                R* d = stg + (ei * NB + blk_index(n, a, b)) * 9;
+#pragma unroll
+                for (int k = 0; k < 9; ++k) d[k] = acc[i][j][k];
+              }
+            }
+        }
+      }
+      __syncwarp();
+      for (int ei = 0; ei < EPW && e0 + ei < A.n_elems; ++ei) {
+        R* out = reinterpret_cast<R*>(V.edata) + (e0 + ei) * (NB * BS);
+        const R* sb = stg + ei * NB * 9;
+        for (int pc = lane; pc < NB * CPB; pc += 32) {
+          const int k = pc / CPB, part = pc % CPB;
+          R v[4];
+#pragma unroll
+          for (int t = 0; t < PER; ++t) {
+            const int j = part * PER + t;
+            v[t] = j < 9 ? sb[k * 9 + j] : R(0);
+          }
+          if constexpr (sizeof(R) == 4) {
+            *reinterpret_cast<float4*>(out + k * BS + part * PER) = make_float4(v[0], v[1], v[2], v[3]);
+          } else {
+            *reinterpret_cast<double2*>(out + k * BS + part * PER) = make_double2(v[0], v[1]);
+          }
+        }
+      }
+      __syncwarp();  // the next elements' Gauss-point phase rewrites the gradient area
     }
     // ---- phase D: internal force per element (material-point mode) --------------------
     if (TAN) {
