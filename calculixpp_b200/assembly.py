@@ -192,31 +192,40 @@ class Plan:
 
     def tune(self, step, tangent=False, reps=3):
         """Time `step()` (one assembly through this plan) with CUDA events for every tile
-        and element-pass grid shape of the current precision, keep the fastest and return
-        it with its time in ms."""
-        tiles = (0, 1) if tangent else (0, 1, 2)
-        best = None
-        for tile in tiles:
-            for bps in (0, 1, 2):
-                try:
-                    self.set_launch_config(tangent, tile, bps, 0)
-                except _lib.CxgError:
-                    continue
+        and element-pass grid shape of the current precision, then for the row gather's
+        warps per block (8, 4, 2) at the kept element-pass shape; keep the fastest and
+        return it with its time in ms."""
+
+        def timed(tile, bps, warps):
+            try:
+                self.set_launch_config(tangent, tile, bps, warps)
+            except _lib.CxgError:
+                return None
+            step()
+            torch.cuda.synchronize(self.device)
+            t = []
+            for _ in range(reps):
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record()
                 step()
-                torch.cuda.synchronize(self.device)
-                t = []
-                for _ in range(reps):
-                    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    s.record()
-                    step()
-                    e.record()
-                    e.synchronize()
-                    t.append(s.elapsed_time(e))
-                ms = sorted(t)[len(t) // 2]
-                if best is None or ms < best[0]:
-                    best = (ms, tile, bps)
-        self.set_launch_config(tangent, best[1], best[2], 0)
-        return {"tile": {0: "2x4", 1: "2x2", 2: "4x4"}[best[1]], "p1_blocks_per_sm": best[2], "ms": best[0]}
+                e.record()
+                e.synchronize()
+                t.append(s.elapsed_time(e))
+            return sorted(t)[len(t) // 2]
+
+        best = None
+        for tile in ((0, 1) if tangent else (0, 1, 2)):
+            for bps in (0, 1, 2):
+                ms = timed(tile, bps, 0)
+                if ms is not None and (best is None or ms < best[0]):
+                    best = (ms, tile, bps, 0)
+        for warps in (4, 2):
+            ms = timed(best[1], best[2], warps)
+            if ms is not None and ms < best[0]:
+                best = (ms, best[1], best[2], warps)
+        self.set_launch_config(tangent, best[1], best[2], best[3])
+        return {"tile": {0: "2x4", 1: "2x2", 2: "4x4"}[best[1]], "p1_blocks_per_sm": best[2],
+                "p2_warps": best[3] or 8, "ms": best[0]}
 
     # -- assembly --------------------------------------------------------------------
     def assemble_linear(self, f_ext=None, vals=None, rhs=None, check=True):
