@@ -502,7 +502,7 @@ def host_pattern(mesh, dof_eq):
     return rp, cols.astype(np.int32)
 
 
-def cpu_baseline(seconds, seed=0):
+def cpu_baseline(seconds, seed=0, as_shipped=True):
     from oracle.oracle import Port, Ref
     threads = len(os.sched_getaffinity(0))
     n = 12
@@ -519,9 +519,28 @@ def cpu_baseline(seconds, seed=0):
             if time.perf_counter() - t0 >= seconds:
                 break
         dt = time.perf_counter() - t0
-        return {"value": elems / dt, "unit": "element-integrations/s", "cores": threads, "kind": "reference",
-                "sample": f"C3D20 {n}^3 block ({m.n_elems} elements) x {elems // m.n_elems} passes: reference "
-                          f"element_stiffness (src/fem/element.cpp) on {threads} threads + exact CSR scatter"}
+        out = {"value": elems / dt, "unit": "element-integrations/s", "cores": threads, "kind": "reference",
+               "sample": f"C3D20 {n}^3 block ({m.n_elems} elements) x {elems // m.n_elems} passes: reference "
+                         f"element_stiffness (src/fem/element.cpp) on {threads} threads + exact CSR scatter"}
+        if not as_shipped:
+            return out
+        # beside it, the reference's own assembly driver as shipped: one thread, its hash-map
+        # scatter and unordered COO flush (assemble_linear_static, src/fem/assembly.cpp:225-257)
+        try:
+            from oracle.oracle import make_material
+            n2 = 8
+            model2, _ = c3d20_model(n2, seed)
+            m2 = model2.mesh
+            mats = [make_material(float(E), 0.3) for E in m2.young]
+            rm = ref.model(m2, mats, np.arange(m2.n_elems, dtype=np.int32), model2.spc, model2.cloads)
+            calls, dt2 = rm.time_linear_static(max(1.0, seconds / 3))
+            out["as_shipped"] = {"value": calls * m2.n_elems / dt2, "unit": "element-integrations/s", "cores": 1,
+                                 "sample": f"C3D20 {n2}^3 block ({m2.n_elems} elements) x {calls} calls of the "
+                                           "reference's assemble_linear_static (src/fem/assembly.cpp:225-257), "
+                                           "single-threaded"}
+        except Exception as exc:  # the threaded figure above stands on its own
+            out["as_shipped"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
+        return out
     port = Port()
     from oracle.oracle import make_material
     mats = [make_material(float(E), 0.3) for E in m.young]
@@ -544,7 +563,7 @@ def reference_arm(args, rank, world):
     out = None
     t_all = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(max(1.0, args.cpu_seconds / 4), seed=0)
+        r = cpu_baseline(max(1.0, args.cpu_seconds / 4), seed=0, as_shipped=False)
         if i >= args.warmup:
             t_all.append(r["value"])
         out = r

@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import time
 
 import numpy as np
 
@@ -406,6 +407,19 @@ class RefModel:
     def assemble_linear_static(self):
         """Returns the reference LinearSystem (COO in hash-map order) as a dict."""
         return self._take(self.ref._fn("assemble_linear_static")(_vp(self.h)))
+
+    def time_linear_static(self, seconds):
+        """Calls the reference's assemble_linear_static as shipped (one thread) until
+        `seconds` have passed; returns (calls, elapsed seconds). The systems are freed
+        untouched, so only the reference call is timed."""
+        fn, free = self.ref._fn("assemble_linear_static"), self.ref.lib.ref_sys_free
+        calls, t0 = 0, time.perf_counter()
+        while True:
+            free(_vp(fn(_vp(self.h))))
+            calls += 1
+            dt = time.perf_counter() - t0
+            if dt >= seconds:
+                return calls, dt
 
     def assemble_conduction(self, k_per_material, tbc_node, tbc_val):
         k = _f64(k_per_material)
