@@ -122,3 +122,21 @@ def test_launch_shapes_give_identical_bits(cuda, etype, precision):
                 assert all(bool((a == b).all()) for a, b in zip(plan.assemble_tangent(u), ref_t)), (tile, bps, warps)
     with pytest.raises(Exception):
         plan.set_launch_config(tangent=True, tile=2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_plan_tune_keeps_a_shape_and_the_bits(cuda, precision):
+    """Plan.tune times the element-pass shapes, then the row gather's block sizes at the
+    kept shape; what it keeps is one of those shapes, and the assembly through it (linear
+    and tangent) is bit-identical to the default shape's."""
+    model = box_model(mg.C3D20, 3, 2, 2, jitter=0.08, seed=3, materials=[J2_STEEL], load=False)
+    plan = Plan(model, precision)
+    u = displacement_field(model, 0.0012)
+    ref_l = [t.clone() for t in plan.assemble_linear()]
+    ref_t = [t.clone() for t in plan.assemble_tangent(u)]
+    for tangent, step in ((False, lambda: plan.assemble_linear(check=False)), (True, lambda: plan.assemble_tangent(u))):
+        shape = plan.tune(step, tangent=tangent, reps=2)
+        assert shape["tile"] in (("2x4", "2x2") if tangent else ("2x4", "2x2", "4x4"))
+        assert shape["p1_blocks_per_sm"] in (0, 1, 2) and shape["p2_warps"] in (2, 4, 8) and shape["ms"] > 0
+    assert all(bool((a == b).all()) for a, b in zip(plan.assemble_linear(), ref_l))
+    assert all(bool((a == b).all()) for a, b in zip(plan.assemble_tangent(u), ref_t))
