@@ -72,21 +72,102 @@ class OracleError(RuntimeError):
     pass
 
 
+_i = C.c_int
+_d = C.c_double
+_i32t = C.c_int32
+_i64t = C.c_int64
+
+# Signatures of every entry point, (restype, argtypes). Handles come back as c_void_p so
+# they keep all 64 bits; messages as c_char_p. Entries shared by both libraries first.
+_COMMON = {
+    "last_error": (C.c_char_p, []),
+    "gauss_rule": (_i, [_i, _vp]),
+    "shape": (_i, [_i, _d, _d, _d, _vp, _vp]),
+    "physical_gradients": (_i, [_i, _d, _d, _d, _vp, _vp, _vp]),
+    "element_volume": (_i, [_i, _vp, _vp]),
+    "element_stiffness": (_i, [_i, _vp, _d, _d, _vp]),
+    "material_evaluate": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "element_tangent_force": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "element_geometric_stiffness": (_i, [_i, _vp, _vp, _vp]),
+    "element_conduction": (_i, [_i, _vp, _d, _vp]),
+}
+
+PORT_SIGS = dict(_COMMON, **{
+    "nodes_per_element": (_i, [_i]),
+    "dof_map": (_i32t, [_i64t, _i64t, _vp, _vp, _vp, _vp, _vp]),
+    "assemble_linear": (_vp, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32t, _vp]),
+    "assemble_tangent": (_vp, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32t, _vp, _vp, _vp,
+                               _vp, _vp]),
+    "element_mass": (_i, [_i, _vp, _d, _vp]),
+    "element_mass_lumped": (_i, [_i, _vp, _d, _vp]),
+    "assemble_scalar": (_vp, [_i, _i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32t]),
+    "recover_gauss_stress": (_i, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "recover_fields": (_i, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "assemble_conduction": (_vp, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _i32t, _vp]),
+    "system_info": (_i, [_vp, _vp, _vp]),
+    "system_copy": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "system_free": (None, [_vp]),
+    "element_compliance_grad_fd": (_i, [_i, _vp, _vp, _d, _d, _d, _vp]),
+})
+
+REF_SIGS = dict(_COMMON, **{
+    "model_create": (_vp, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _i32t, _vp, _i64t, _vp, _vp, _vp, _i64t,
+                           _vp, _vp, _vp]),
+    "model_free": (None, [_vp]),
+    "element_mass": (_i, [_i, _vp, _d, _i, _vp]),
+    "model_set_density": (_i, [_vp, _i32t, _vp]),
+    "assemble_mass": (_vp, [_vp, _i]),
+    "assemble_geometric": (_vp, [_vp, _vp]),
+    "recover_gauss_stress": (_i, [_vp, _vp, _vp]),
+    "recover_fields": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "assemble_conduction": (_vp, [_vp, _i32t, _vp, _i64t, _vp, _vp]),
+    "assemble_linear_static": (_vp, [_vp]),
+    "sys_info": (_i, [_vp, _vp, _vp]),
+    "sys_copy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "sys_free": (None, [_vp]),
+    "mp_create": (_vp, [_vp]),
+    "mp_free": (None, [_vp]),
+    "mp_num_points": (_i64t, [_vp]),
+    "mp_get_state": (_i, [_vp, _i, _vp]),
+    "mp_set_state": (_i, [_vp, _i, _vp]),
+    "mp_commit": (None, [_vp]),
+    "assemble_material_tangent": (_vp, [_vp, _vp, _vp, _vp]),
+    "sensitivity_compliance": (_i, [_vp, _i64t, _vp, _vp, _d, _vp, _vp]),
+    "assemble_csr_threads": (_i, [_i, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i]),
+})
+
+
 class _Base:
     prefix = ""
+    sigs: dict = {}
 
     def __init__(self, path):
         if not os.path.exists(path):
             raise OracleError(f"oracle library missing: {path} (run make -C oracle)")
         self.lib = C.CDLL(path)
-        self.lib[f"{self.prefix}_last_error"].restype = C.c_char_p
+        # Every entry point is looked up once and configured once. CDLL.__getitem__
+        # builds a new function object on each call, so settings made on one are lost;
+        # the objects kept here carry their restype/argtypes for the library's lifetime.
+        self._fns = {}
+        for name, (res, args) in self.sigs.items():
+            f = getattr(self.lib, f"{self.prefix}_{name}")
+            f.restype = res
+            f.argtypes = args
+            self._fns[name] = f
 
     def _fn(self, name):
-        return self.lib[f"{self.prefix}_{name}"]
+        try:
+            return self._fns[name]
+        except KeyError:
+            raise OracleError(f"{self.prefix}_{name} has no declared signature") from None
+
+    def last_error(self):
+        msg = self._fn("last_error")()
+        return msg.decode() if msg else ""
 
     def _check(self, rc):
         if rc != 0:
-            raise OracleError(self._fn("last_error")().decode())
+            raise OracleError(self.last_error())
 
     # ---- element level (same signatures in both libraries) -----------------------
     def gauss_rule(self, etype):
@@ -98,7 +179,6 @@ class _Base:
         N = np.zeros(20)
         dN = np.zeros(60)
         f = self._fn("shape")
-        f.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _vp, _vp]
         n = f(int(etype), xi, et, ze, _p(N), _p(dN))
         return N[:n].copy(), dN[: 3 * n].reshape(n, 3).copy()
 
@@ -107,7 +187,6 @@ class _Base:
         g = np.zeros(3 * n)
         det = C.c_double()
         f = self._fn("physical_gradients")
-        f.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp]
         self._check(f(int(etype), xi, et, ze, _p(_f64(coords)), _p(g), C.byref(det)))
         return g.reshape(n, 3), det.value
 
@@ -120,7 +199,6 @@ class _Base:
         n = NODES[etype]
         Ke = np.zeros((3 * n) * (3 * n))
         f = self._fn("element_stiffness")
-        f.argtypes = [C.c_int, _vp, C.c_double, C.c_double, _vp]
         self._check(f(int(etype), _p(_f64(coords)), float(E), float(nu), _p(Ke)))
         return Ke.reshape(3 * n, 3 * n)
 
@@ -130,11 +208,9 @@ class _Base:
         M = np.zeros((3 * n) ** 2)
         if self.prefix == "ref":
             f = self._fn("element_mass")
-            f.argtypes = [C.c_int, _vp, C.c_double, C.c_int, _vp]
             self._check(f(int(etype), _p(_f64(coords)), float(rho), int(lumped), _p(M)))
         else:
             f = self._fn("element_mass_lumped" if lumped else "element_mass")
-            f.argtypes = [C.c_int, _vp, C.c_double, _vp]
             self._check(f(int(etype), _p(_f64(coords)), float(rho), _p(M)))
         return M.reshape(3 * n, 3 * n)
 
@@ -143,7 +219,6 @@ class _Base:
         n = NODES[etype]
         K = np.zeros((3 * n) ** 2)
         f = self._fn("element_geometric_stiffness")
-        f.argtypes = [C.c_int, _vp, _vp, _vp]
         self._check(f(int(etype), _p(_f64(coords)), _p(_f64(gp_stress)), _p(K)))
         return K.reshape(3 * n, 3 * n)
 
@@ -152,7 +227,6 @@ class _Base:
         n = NODES[etype]
         K = np.zeros(n * n)
         f = self._fn("element_conduction")
-        f.argtypes = [C.c_int, _vp, C.c_double, _vp]
         self._check(f(int(etype), _p(_f64(coords)), float(k), _p(K)))
         return K.reshape(n, n)
 
@@ -182,25 +256,23 @@ class Port(_Base):
     """The C restatement (oracle/cxo.c)."""
 
     prefix = "cxo"
+    sigs = PORT_SIGS
 
     def __init__(self, path=PORT_SO):
         super().__init__(path)
-        for name in ("assemble_linear", "assemble_tangent"):
-            self._fn(name).restype = _vp
-        self.lib.cxo_dof_map.restype = C.c_int32
 
     def _system(self, s):
         if not s:
-            raise OracleError(self._fn("last_error")().decode())
+            raise OracleError(self.last_error())
         n_free = C.c_int32()
         nnz = C.c_int64()
-        self.lib.cxo_system_info(_vp(s), C.byref(n_free), C.byref(nnz))
+        self._fn("system_info")(_vp(s), C.byref(n_free), C.byref(nnz))
         rp = np.zeros(n_free.value + 1, dtype=np.int64)
         ci = np.zeros(nnz.value, dtype=np.int32)
         v = np.zeros(nnz.value)
         rhs = np.zeros(n_free.value)
-        self.lib.cxo_system_copy(_vp(s), _p(rp), _p(ci), _p(v), _p(rhs))
-        self.lib.cxo_system_free(_vp(s))
+        self._fn("system_copy")(_vp(s), _p(rp), _p(ci), _p(v), _p(rhs))
+        self._fn("system_free")(_vp(s))
         return rp, ci, v, rhs
 
     @staticmethod
@@ -248,8 +320,6 @@ class Port(_Base):
         types = np.full(E, mesh.etype, dtype=np.int32)
         conn_ptr = np.arange(E + 1, dtype=np.int64) * n
         f = self._fn("assemble_scalar")
-        f.restype = _vp
-        f.argtypes = [C.c_int, C.c_int64, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32]
         code = {"mass": 1, "lumped": 2, "geometric": 3}[kind]
         s = f(code, mesh.n_nodes, _p(_f64(mesh.coords)), E, _p(types), _p(conn_ptr), _p(_i32(mesh.conn.ravel())),
               _p(None if density is None else _f64(density)), _p(None if gp_stress is None else _f64(gp_stress)),
@@ -268,7 +338,6 @@ class Port(_Base):
         """recover_gauss_stress (src/fem/stress.cpp:147-187): (G, 6)."""
         out = np.zeros(6 * mesh.n_elems * NGP[mesh.etype])
         f = self._fn("recover_gauss_stress")
-        f.argtypes = [C.c_int64, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
         self._check(f(*self._recover_args(mesh, young, poisson), _p(_f64(u)), _p(out)))
         return out.reshape(-1, 6)
 
@@ -277,7 +346,6 @@ class Port(_Base):
         N = mesh.n_nodes
         st, ss, rf = np.zeros(6 * N), np.zeros(6 * N), np.zeros(3 * N)
         f = self._fn("recover_fields")
-        f.argtypes = [C.c_int64, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
         self._check(f(*self._recover_args(mesh, young, poisson), _p(_f64(u)),
                       _p(None if f_ext is None else _f64(f_ext)), _p(st), _p(ss), _p(rf)))
         return st.reshape(N, 6), ss.reshape(N, 6), rf.reshape(N, 3)
@@ -287,8 +355,6 @@ class Port(_Base):
         E = mesh.n_elems
         n = mesh.conn.shape[1]
         f = self._fn("assemble_conduction")
-        f.restype = _vp
-        f.argtypes = [C.c_int64, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32, _vp]
         s = f(mesh.n_nodes, _p(_f64(mesh.coords)), E, _p(np.full(E, mesh.etype, dtype=np.int32)),
               _p(np.arange(E + 1, dtype=np.int64) * n), _p(_i32(mesh.conn.ravel())), _p(_f64(conductivity)),
               _p(_i32(t_dof_eq)), _p(_f64(t_prescribed)), int(n_free), _p(None if flux is None else _f64(flux)))
@@ -298,7 +364,6 @@ class Port(_Base):
         n = NODES[etype]
         out = np.zeros(3 * n)
         f = self._fn("element_compliance_grad_fd")
-        f.argtypes = [C.c_int, _vp, _vp, C.c_double, C.c_double, C.c_double, _vp]
         self._check(f(int(etype), _p(_f64(coords)), _p(_f64(ue)), E, nu, h, _p(out)))
         return out.reshape(n, 3)
 
@@ -324,13 +389,10 @@ class Ref(_Base):
     """The reference itself (oracle/_ref/libcxpp_ref.so)."""
 
     prefix = "ref"
+    sigs = REF_SIGS
 
     def __init__(self, path=REF_SO):
         super().__init__(path)
-        for name in ("model_create", "assemble_linear_static", "mp_create",
-                     "assemble_material_tangent"):
-            self._fn(name).restype = _vp
-        self.lib.ref_mp_num_points.restype = C.c_int64
 
     @staticmethod
     def available(path=REF_SO):
@@ -353,15 +415,15 @@ class Ref(_Base):
             C.c_int64(sn.size), _p(sn), _p(sc), _p(sv), C.c_int64(cn.size), _p(cn),
             _p(cc), _p(cv))
         if not h:
-            raise OracleError(self._fn("last_error")().decode())
+            raise OracleError(self.last_error())
         return RefModel(self, h, mesh)
 
     def _sys(self, s):
         if not s:
-            raise OracleError(self._fn("last_error")().decode())
+            raise OracleError(self.last_error())
         n_free = C.c_int64()
         nnz = C.c_int64()
-        self.lib.ref_sys_info(_vp(s), C.byref(n_free), C.byref(nnz))
+        self._fn("sys_info")(_vp(s), C.byref(n_free), C.byref(nnz))
         rows = np.zeros(nnz.value, dtype=np.int32)
         cols = np.zeros(nnz.value, dtype=np.int32)
         vals = np.zeros(nnz.value)
@@ -372,8 +434,6 @@ class Ref(_Base):
         vals = np.zeros(col_idx.size)
         rhs = np.zeros(row_ptr.size - 1)
         f = self._fn("assemble_csr_threads")
-        f.argtypes = [C.c_int, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                      _vp, C.c_int]
         self._check(f(int(mesh.etype), _p(_f64(mesh.coords)), mesh.n_elems,
                       _p(_i32(mesh.conn.ravel())), _p(_f64(mesh.young)),
                       _p(_f64(mesh.poisson)), _p(_i32(dof_eq)), _p(_f64(prescribed)),
@@ -390,17 +450,16 @@ class RefModel:
     def __del__(self):
         try:
             if self.mp:
-                self.ref.lib.ref_mp_free(_vp(self.mp))
-            self.ref.lib.ref_model_free(_vp(self.h))
+                self.ref._fn("mp_free")(_vp(self.mp))
+            self.ref._fn("model_free")(_vp(self.h))
         except Exception:
             pass
 
     def _take(self, s):
-        lib = self.ref.lib
         n_free, rows, cols, vals, rhs, s = self.ref._sys(s)
         dof_eq = np.zeros(3 * self.mesh.n_nodes, dtype=np.int32)
-        lib.ref_sys_copy(_vp(s), _p(rows), _p(cols), _p(vals), _p(rhs), _p(dof_eq))
-        lib.ref_sys_free(_vp(s))
+        self.ref._fn("sys_copy")(_vp(s), _p(rows), _p(cols), _p(vals), _p(rhs), _p(dof_eq))
+        self.ref._fn("sys_free")(_vp(s))
         return {"n_free": n_free, "rows": rows, "cols": cols, "vals": vals, "rhs": rhs,
                 "dof_eq": dof_eq}
 
@@ -412,7 +471,7 @@ class RefModel:
         """Calls the reference's assemble_linear_static as shipped (one thread) until
         `seconds` have passed; returns (calls, elapsed seconds). The systems are freed
         untouched, so only the reference call is timed."""
-        fn, free = self.ref._fn("assemble_linear_static"), self.ref.lib.ref_sys_free
+        fn, free = self.ref._fn("assemble_linear_static"), self.ref._fn("sys_free")
         calls, t0 = 0, time.perf_counter()
         while True:
             free(_vp(fn(_vp(self.h))))
@@ -425,58 +484,51 @@ class RefModel:
         k = _f64(k_per_material)
         tn, tv = _i32(tbc_node), _f64(tbc_val)
         f = self.ref._fn("assemble_conduction")
-        f.restype = _vp
-        f.argtypes = [_vp, C.c_int32, _vp, C.c_int64, _vp, _vp]
         return self._take(f(_vp(self.h), k.size, _p(k), tn.size, _p(tn), _p(tv)))
 
     def recover_gauss_stress(self, u):
         out = np.zeros(6 * self.mesh.n_elems * NGP[self.mesh.etype])
-        self.ref._check(self.ref.lib.ref_recover_gauss_stress(_vp(self.h), _p(_f64(u)), _p(out)))
+        self.ref._check(self.ref._fn("recover_gauss_stress")(_vp(self.h), _p(_f64(u)), _p(out)))
         return out.reshape(-1, 6)
 
     def recover_fields(self, u):
         N = self.mesh.n_nodes
         st, ss, rf = np.zeros(6 * N), np.zeros(6 * N), np.zeros(3 * N)
-        self.ref._check(self.ref.lib.ref_recover_fields(_vp(self.h), _p(_f64(u)), _p(st), _p(ss), _p(rf)))
+        self.ref._check(self.ref._fn("recover_fields")(_vp(self.h), _p(_f64(u)), _p(st), _p(ss), _p(rf)))
         return st.reshape(N, 6), ss.reshape(N, 6), rf.reshape(N, 3)
 
     def set_density(self, rho_per_material):
         rho = _f64(rho_per_material)
-        self.ref._check(self.ref.lib.ref_model_set_density(_vp(self.h), C.c_int32(rho.size), _p(rho)))
+        self.ref._check(self.ref._fn("model_set_density")(_vp(self.h), C.c_int32(rho.size), _p(rho)))
 
     def assemble_mass(self, lumped=False):
         f = self.ref._fn("assemble_mass")
-        f.restype = _vp
-        f.argtypes = [_vp, C.c_int]
         return self._take(f(_vp(self.h), int(lumped)))
 
     def assemble_geometric(self, gp_stress):
         f = self.ref._fn("assemble_geometric")
-        f.restype = _vp
-        f.argtypes = [_vp, _vp]
         return self._take(f(_vp(self.h), _p(_f64(gp_stress))))
 
     def material_points(self):
-        lib = self.ref.lib
         if self.mp is None:
-            self.mp = lib.ref_mp_create(_vp(self.h))
+            self.mp = self.ref._fn("mp_create")(_vp(self.h))
             if not self.mp:
-                raise OracleError(lib.ref_last_error().decode())
+                raise OracleError(self.ref.last_error())
         return self.mp
 
     def state(self, committed=True):
         mp = self.material_points()
-        g = self.ref.lib.ref_mp_num_points(_vp(mp))
+        g = self.ref._fn("mp_num_points")(_vp(mp))
         out = np.zeros(13 * g)
-        self.ref.lib.ref_mp_get_state(_vp(mp), int(committed), _p(out))
+        self.ref._fn("mp_get_state")(_vp(mp), int(committed), _p(out))
         return out
 
     def set_state(self, state, committed=True):
         mp = self.material_points()
-        self.ref.lib.ref_mp_set_state(_vp(mp), int(committed), _p(_f64(state)))
+        self.ref._fn("mp_set_state")(_vp(mp), int(committed), _p(_f64(state)))
 
     def commit(self):
-        self.ref.lib.ref_mp_commit(_vp(self.material_points()))
+        self.ref._fn("mp_commit")(_vp(self.material_points()))
 
     def assemble_material_tangent(self, u):
         mp = self.material_points()
@@ -492,7 +544,6 @@ class RefModel:
         dg = np.zeros(var_node.size)
         obj = C.c_double()
         f = self.ref._fn("sensitivity_compliance")
-        f.argtypes = [_vp, C.c_int64, _vp, _vp, C.c_double, _vp, _vp]
         self.ref._check(f(_vp(self.h), var_node.size, _p(var_node), _p(var_comp), h,
                           _p(dg), C.byref(obj)))
         return dg, obj.value
