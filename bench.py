@@ -209,7 +209,7 @@ def j2_newton(args, world, dev, stream):
         plan.check()
         keep[prec] = (vals.clone(), f_int.clone(), plan.state(committed=False).clone())
         out[prec] = {"value": world * m.n_elems * args.steps / t, "ms_per_step": t / args.steps * 1e3,
-                     "launch_shape": shapes[prec]}
+                     "launch_shape": shapes[prec], "windows_and_ring": plan.windows(tangent=True)}
     (v64, f64, s64), (vm, fm, sm) = keep["fp64"], keep["mixed"]
     yielded = float((s64[:, 6] > 0).double().mean())
     B = j2_algorithmic_bytes(plan, model)
@@ -627,7 +627,7 @@ def main():
         barrier(world)
         t = max_over_ranks(t, world)
         plan.check()
-        results[prec] = {"t": t, "launch_shape": shapes[prec]}
+        results[prec] = {"t": t, "launch_shape": shapes[prec], "windows_and_ring": plan.windows()}
 
     # e2e through the C ABI with host buffers (pinned): load vector in, K_ff + rhs out.
     h_f = torch.as_tensor(f_ext).pin_memory()
@@ -708,9 +708,11 @@ def main():
                                           "generator (same element type, rule and scatter), reported beside "
                                           "the 64^3 GPU figure"},
         "launch_shape": mix["launch_shape"],
+        "windows_and_ring": mix["windows_and_ring"],
         "targets": targets(j2, batch),
         "fp64": {"value": world * E * args.steps / f64["t"], "ms_per_step": f64["t"] / args.steps * 1e3,
                  "launch_shape": f64["launch_shape"],
+                 "windows_and_ring": f64["windows_and_ring"],
                  "fp64_pipe": {"achieved_tflops": FLOPS_PER_ELEM_C3D20 * E / (f64["t"] / args.steps) / 1e12,
                                "peak_tflops": pipe.get("fp64_tflops"),
                                "peak_kind": "cuBLAS DGEMM 8192^3 measured in this run"}},

@@ -118,6 +118,7 @@ class Plan:
             raise _lib.CxgError(_lib.CXG_ERR_NO_GPU, "no CUDA device")
         self.device = torch.device(device or f"cuda:{torch.cuda.current_device()}")
         self.model = model
+        self.precision = precision
         m = model.mesh
         dev = self.device
         dof_eq, prescribed, n_free = model.dof_map()
@@ -180,6 +181,7 @@ class Plan:
 
     def set_precision(self, precision: str):
         _lib.check(self.lib.cxg_plan_set_precision(self.h, _lib.MIXED if precision == "mixed" else _lib.FP64))
+        self.precision = precision
 
     def check(self):
         bad = C.c_int64()
@@ -189,6 +191,18 @@ class Plan:
         """Launch shape of the current precision's linear (or tangent) passes; tile 0 = 2x4,
         1 = 2x2, 2 = 4x4. Results do not depend on it."""
         _lib.check(self.lib.cxg_plan_set_launch_config(self.h, int(tangent), tile, p1_blocks_per_sm, p2_warps))
+
+    def set_ring_bytes(self, nbytes: int):
+        """Element-buffer budget of the windowed assembly (cxg_plan_set_ring_bytes):
+        0 = default share of L2, < 0 = one window over the whole mesh."""
+        _lib.check(self.lib.cxg_plan_set_ring_bytes(self.h, int(nbytes)))
+
+    def windows(self, tangent=False):
+        """(windows, elements held by the element buffers) of the last assembly of the
+        current precision in this mode."""
+        nw, ring = C.c_int32(), C.c_int64()
+        _lib.check(self.lib.cxg_plan_get_windows(self.h, int(tangent), C.byref(nw), C.byref(ring)))
+        return int(nw.value), int(ring.value)
 
     def tune(self, step, tangent=False, reps=3):
         """Time `step()` (one assembly through this plan) with CUDA events for every tile

@@ -162,6 +162,9 @@ int plan_status(cxg_plan* p, int64_t* bad) {
 
 namespace {
 
+// History components an assembly must carry (see cxg_plan::back_stress_zero).
+int state_comps(const cxg_plan* p) { return (p->back_stress_zero && !p->kinematic) ? 7 : kStateDoubles; }
+
 int ensure_state(cxg_plan* p, cudaStream_t s) {
   if (p->state[0]) return CXG_OK;
   const size_t bytes = sizeof(double) * kStateDoubles * static_cast<size_t>(std::max<int64_t>(p->n_gauss, 1));
@@ -177,8 +180,93 @@ int ensure_state(cxg_plan* p, cudaStream_t s) {
 
 namespace cxg {
 namespace api {
+namespace windows {
+
+__global__ void node_span_kernel(const int64_t* inc_ptr, const int32_t* inc_code, int n, int64_t n_nodes,
+                                 int32_t* first, int32_t* last) {
+  for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a < n_nodes;
+       a += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i0 = inc_ptr[a], i1 = inc_ptr[a + 1];
+    first[a] = i1 > i0 ? inc_code[i0] / n : -1;
+    last[a] = i1 > i0 ? inc_code[i1 - 1] / n : -1;
+  }
+}
+
+// Smallest window worth a launch pair under the default budget: a few waves of the
+// element pass. An explicit budget (cxg_plan_set_ring_bytes) is taken as given, down to
+// windows of 32 elements.
+constexpr int64_t kMinWindow = 8192;
+
+// Window schedule for `bpe` bytes of element buffer per element (see cxg::WinSched).
+// Window size W: the ring holds W + span elements, span being the largest distance
+// between a node's first and last incident element, within the plan's budget. Node a
+// is gathered in window last(a) / W; every element it needs is then among the last
+// W + span elements integrated, which the ring still holds.
+int build_schedule(cxg_plan* p, size_t bpe, WinSched& w) {
+  w.built = true;
+  w.ring = std::max<int64_t>(p->n_elems, 1);
+  w.win_e.clear();
+  w.win_n.clear();
+  const int64_t min_w = p->ring_bytes > 0 ? 32 : kMinWindow, grain = p->ring_bytes > 0 ? 32 : 1024;
+  if (p->ring_bytes < 0 || p->n_elems < 2 * min_w) return CXG_OK;
+  if (p->node_first.empty()) {
+    int32_t* d = nullptr;
+    CHECK_CUDA(cudaMalloc(&d, sizeof(int32_t) * 2 * static_cast<size_t>(p->n_nodes)), "node spans");
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>((p->n_nodes + 255) / 256, 4096));
+    node_span_kernel<<<grid, 256>>>(p->pat.inc_ptr, p->pat.inc_code, nodes_of(p->type), p->n_nodes, d,
+                                    d + p->n_nodes);
+    cudaError_t e = cudaGetLastError();
+    p->node_first.resize(static_cast<size_t>(p->n_nodes));
+    p->node_last.resize(static_cast<size_t>(p->n_nodes));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->node_first.data(), d, sizeof(int32_t) * p->n_nodes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->node_last.data(), d + p->n_nodes, sizeof(int32_t) * p->n_nodes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) p->node_first.clear();
+    CHECK_CUDA(e, "node spans");
+  }
+  int64_t span = 1;
+  for (int64_t a = 0; a < p->n_nodes; ++a)
+    if (p->node_last[a] >= 0) span = std::max<int64_t>(span, p->node_last[a] - p->node_first[a] + 1);
+  int64_t budget = p->ring_bytes;
+  if (budget == 0) {
+    int l2 = 0;
+    CHECK_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, p->device), "L2 size");
+    budget = static_cast<int64_t>(l2) * 5 / 8;
+  }
+  const int64_t W = (budget / static_cast<int64_t>(bpe) - span) / grain * grain;
+  if (W < min_w || W * 2 > p->n_elems) return CXG_OK;
+  const int64_t n_win = (p->n_elems + W - 1) / W;
+  std::vector<int64_t> count(static_cast<size_t>(n_win) + 1, 0);
+  for (int64_t a = 0; a < p->n_nodes; ++a) ++count[static_cast<size_t>(std::max(p->node_last[a], 0) / W) + 1];
+  w.win_n.assign(static_cast<size_t>(n_win) + 1, 0);
+  for (int64_t k = 0; k < n_win; ++k) w.win_n[k + 1] = w.win_n[k] + count[k + 1];
+  std::vector<int32_t> order(static_cast<size_t>(p->n_nodes));
+  std::vector<int64_t> pos(w.win_n.begin(), w.win_n.end() - 1);
+  for (int64_t a = 0; a < p->n_nodes; ++a)
+    order[static_cast<size_t>(pos[static_cast<size_t>(std::max(p->node_last[a], 0) / W)]++)] = static_cast<int32_t>(a);
+  if (!w.node_order) {
+    CHECK_CUDA(cudaMalloc(&w.node_order, sizeof(int32_t) * static_cast<size_t>(p->n_nodes)), "node order");
+    p->device_bytes += static_cast<int64_t>(sizeof(int32_t) * p->n_nodes);
+  }
+  CHECK_CUDA(cudaMemcpy(w.node_order, order.data(), sizeof(int32_t) * p->n_nodes, cudaMemcpyHostToDevice),
+             "node order");
+  w.win_e.resize(static_cast<size_t>(n_win) + 1);
+  for (int64_t k = 0; k <= n_win; ++k) w.win_e[static_cast<size_t>(k)] = std::min(k * W, p->n_elems);
+  w.ring = W + span;
+  return CXG_OK;
+}
+
+}  // namespace windows
+
 int ensure_v2(cxg_plan* p, bool tangent) {
-  const size_t need = v2_edata_bytes(p->type, p->n_elems, p->precision);
+  WinSched& w = p->sched[p->precision][tangent ? 1 : 0];
+  if (!w.built) {
+    const int rc = windows::build_schedule(p, v2_bytes_per_element(p->type, p->precision, tangent), w);
+    if (rc) return rc;
+  }
+  const size_t need = v2_edata_bytes(p->type, w.ring, p->precision);
   if (p->edata_bytes < need) {
     cudaFree(p->edata);
     p->edata = nullptr;
@@ -188,12 +276,27 @@ int ensure_v2(cxg_plan* p, bool tangent) {
     p->edata_bytes = need;
     p->device_bytes += static_cast<int64_t>(need);
   }
-  if (tangent && !p->fdata) {
-    const size_t fb = sizeof(double) * 3 * nodes_of(p->type) * static_cast<size_t>(std::max<int64_t>(p->n_elems, 1));
+  const size_t fb = sizeof(double) * 3 * nodes_of(p->type) * static_cast<size_t>(w.ring);
+  if (tangent && p->fdata_bytes < fb) {
+    cudaFree(p->fdata);
+    p->fdata = nullptr;
+    p->device_bytes -= static_cast<int64_t>(p->fdata_bytes);
+    p->fdata_bytes = 0;
     CHECK_CUDA(cudaMalloc(&p->fdata, fb), "force buffer");
+    p->fdata_bytes = fb;
     p->device_bytes += static_cast<int64_t>(fb);
   }
   return CXG_OK;
+}
+
+void apply_windows(const cxg_plan* p, bool tangent, V2Args& v) {
+  const WinSched& w = p->sched[p->precision][tangent ? 1 : 0];
+  if (!w.built || w.win_e.size() < 3) return;
+  v.ring = w.ring;
+  v.node_order = w.node_order;
+  v.n_win = static_cast<int32_t>(w.win_e.size() - 1);
+  v.win_e = w.win_e.data();
+  v.win_n = w.win_n.data();
 }
 
 V2Args v2_args(cxg_plan* p, const double* f_ext, bool accumulate) {
@@ -205,6 +308,13 @@ V2Args v2_args(cxg_plan* p, const double* f_ext, bool accumulate) {
   v.f_ext = f_ext;
   v.max_row = p->pat.max_row;
   v.accumulate = accumulate ? 1 : 0;
+  v.e_begin = 0;
+  v.e_end = p->n_elems;
+  v.ring = std::max<int64_t>(p->n_elems, 1);
+  v.node_order = nullptr;
+  v.n_begin = 0;
+  v.n_end = p->n_nodes;
+  v.n_win = 0;
   return v;
 }
 
@@ -281,6 +391,7 @@ int cxg_plan_create(const cxg_mesh_desc* m, const cxg_dofmap_desc* d, int32_t pr
   p->n_gauss = m->n_elems * gauss_of(m->elem_type);
   p->n_mats = m->n_materials;
   p->has_plastic = plastic;
+  for (const J2Mat& jm : mats) p->kinematic = p->kinematic || jm.h_kin != 0.0;
   const int npe = nodes_of(m->elem_type);
   cudaStream_t s = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -358,6 +469,8 @@ int cxg_plan_destroy(cxg_plan* p) {
                   p->pat.node_eq0, p->pat.slot, p->pat.conn_mask, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
                   p->status, p->edata, p->fdata};
   for (void* b : bufs) cudaFree(b);
+  for (auto& row : p->sched)
+    for (WinSched& w : row) cudaFree(w.node_order);
   for (void* b : p->stage) cudaFree(b);
   delete p;
   return CXG_OK;
@@ -428,6 +541,24 @@ int cxg_plan_set_launch_config(cxg_plan* p, int32_t mode, int32_t tile, int32_t 
   return CXG_OK;
 }
 
+int cxg_plan_set_ring_bytes(cxg_plan* p, int64_t bytes) {
+  if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
+  if (p->last_stream) CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");
+  p->ring_bytes = bytes;
+  for (auto& row : p->sched)
+    for (WinSched& w : row) w.built = false;  // rebuilt at the next assembly
+  return CXG_OK;
+}
+
+int cxg_plan_get_windows(const cxg_plan* p, int32_t mode, int32_t* n_windows, int64_t* ring_elems) {
+  if (!p || (mode != 0 && mode != 1) || !n_windows || !ring_elems)
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");
+  const WinSched& w = p->sched[p->precision][mode];
+  *n_windows = !w.built ? 0 : (w.win_e.size() < 3 ? 1 : static_cast<int32_t>(w.win_e.size() - 1));
+  *ring_elems = w.built ? w.ring : 0;
+  return CXG_OK;
+}
+
 int cxg_plan_check(cxg_plan* p, int64_t* bad) {
   if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
   return plan_status(p, bad);
@@ -455,9 +586,9 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
   ElemArgs a = base_args(p);
   a.vals = static_cast<double*>(dv);
   a.rhs = static_cast<double*>(dr);
-  CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, p->precision, a, v2_args(p, static_cast<const double*>(df), accumulate), s,
-                       p->cfg[p->precision]),
-             "assembly kernels");
+  V2Args v = v2_args(p, static_cast<const double*>(df), accumulate);
+  apply_windows(p, false, v);
+  CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, p->precision, a, v, s, p->cfg[p->precision]), "assembly kernels");
   if ((rc = copy_out(vals, dv, vb, s))) return rc;
   if ((rc = copy_out(rhs, dr, rb, s))) return rc;
   if (dv != vals || (rhs && dr != rhs)) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
@@ -489,9 +620,10 @@ int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_i
   a.u = static_cast<const double*>(du);
   a.state_c = p->state[0];
   a.state_t = p->state[1];
-  CHECK_CUDA(launch_v2(p->type, MODE_TANGENT, p->precision, a, v2_args(p, static_cast<const double*>(df), false), s,
-                       p->tcfg[p->precision]),
-             "assembly kernels");
+  a.state_comps = state_comps(p);
+  V2Args v = v2_args(p, static_cast<const double*>(df), false);
+  apply_windows(p, true, v);
+  CHECK_CUDA(launch_v2(p->type, MODE_TANGENT, p->precision, a, v, s, p->tcfg[p->precision]), "assembly kernels");
   if ((rc = copy_out(vals, dv, vb, s))) return rc;
   if ((rc = copy_out(rhs, dr, rb, s))) return rc;
   if ((rc = copy_out(f_int, dfi, fb, s))) return rc;
@@ -711,6 +843,7 @@ int cxg_state_set(cxg_plan* p, int32_t slot, const double* in) {
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   cudaFree(tmp);
   CHECK_CUDA(e, "state write");
+  p->back_stress_zero = false;  // the caller may have set a back stress
   return CXG_OK;
 }
 
@@ -720,7 +853,8 @@ int cxg_state_commit(cxg_plan* p, void* stream) {
   int rc = ensure_state(p, s);
   if (rc) return rc;
   p->last_stream = s;
-  CHECK_CUDA(cudaMemcpyAsync(p->state[0], p->state[1], sizeof(double) * kStateDoubles * static_cast<size_t>(p->n_gauss),
+  // SoA layout: the first state_comps components are the leading state_comps*G doubles
+  CHECK_CUDA(cudaMemcpyAsync(p->state[0], p->state[1], sizeof(double) * state_comps(p) * static_cast<size_t>(p->n_gauss),
                              cudaMemcpyDeviceToDevice, s), "commit");
   return CXG_OK;
 }

@@ -116,7 +116,8 @@ cudaError_t launch_group(cxg_batch* b, Group& g, double* vals, double* rhs, cons
   ElemArgs a = base_args(p);
   a.vals = vals + g.vals0;
   a.rhs = rhs ? rhs + g.rhs0 : nullptr;
-  const V2Args v = v2_args(p, f_ext ? f_ext + 3 * g.node0 : nullptr, false);
+  V2Args v = v2_args(p, f_ext ? f_ext + 3 * g.node0 : nullptr, false);
+  apply_windows(p, false, v);
   return launch_v2(p->type, MODE_LINEAR, b->precision, a, v, s, override_cfg ? *override_cfg : p->cfg[b->precision]);
 }
 

@@ -78,6 +78,11 @@ struct ElemArgs {
   const double* state_c;
   double* state_t;
   int64_t n_gauss;
+  // history components the element pass reads and writes: 13, or 7 (plastic strain and
+  // equivalent plastic strain) when the back stress is zero in both buffers and no
+  // material moves it (every kinematic modulus is 0); components 7..12 are then zero
+  // and left untouched
+  int state_comps;
   // displacement (tangent mode)
   const double* u;           // [3N] (mesh) or [E*n*3] (dense)
   // outputs
@@ -99,6 +104,19 @@ struct V2Args {
   int64_t max_row;          // largest (free rows x row length) of any node
   int64_t row_stride;       // set by the launcher
   int accumulate;           // add into vals / rhs / f_int instead of overwriting
+  // The window of one element-pass + row-gather pair: the element pass integrates
+  // elements [e_begin, e_end), the row gather the nodes node_order[n_begin..n_end)
+  // (node_order null: nodes n_begin..n_end in mesh order). The element buffers hold
+  // `ring` elements; element e lives in slot e mod ring.
+  int64_t e_begin, e_end, ring;
+  const int32_t* node_order;
+  int64_t n_begin, n_end;
+  // Window schedule read by the launcher (host arrays): n_win windows with element
+  // offsets win_e[0..n_win] and node-list offsets win_n[0..n_win]; n_win <= 1 runs the
+  // whole mesh as one window.
+  int32_t n_win;
+  const int64_t* win_e;
+  const int64_t* win_n;
 };
 // Launch shape of the two passes. tile: element-pass node-pair tile (0 = 2x4, 1 = 2x2,
 // 2 = 4x4, the last in the linear pass with FP32 accumulators only);
@@ -113,6 +131,8 @@ struct LaunchCfg {
   int passes = 3;
 };
 size_t v2_edata_bytes(int elem_type, int64_t n_elems, int precision);
+// Bytes of element buffer per element (blocks, plus the internal force in tangent mode).
+size_t v2_bytes_per_element(int elem_type, int precision, bool tangent);
 // Element pass of the scalar-block operators (every 3x3 block is a scalar times I):
 // kind 1 consistent mass rho N_a N_b, 2 lumped mass (row sums on the diagonal), 3
 // geometric stiffness g_a . sigma . g_b, 4 conduction k g_a . g_b. Writes FP64 blocks

@@ -5,9 +5,25 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/cxg.h"
 #include "cxg_internal.cuh"
+
+namespace cxg {
+// Window schedule of the two-pass assembly for one element-buffer footprint: windows of
+// consecutive elements, each followed by the row gather of the nodes whose last
+// incident element it holds, with element buffers of `ring` elements (slot e mod ring)
+// sized to stay in L2 between the two passes. One window (ring = n_elems) when the
+// mesh ordering does not allow a ring that small.
+struct WinSched {
+  bool built = false;
+  int64_t ring = 0;
+  std::vector<int64_t> win_e;      // [n_win + 1] element offsets
+  std::vector<int64_t> win_n;      // [n_win + 1] offsets into node_order
+  int32_t* node_order = nullptr;   // device [n_nodes]: nodes by window, mesh order within
+};
+}  // namespace cxg
 
 struct cxg_plan {
   int device = 0;
@@ -25,10 +41,19 @@ struct cxg_plan {
   double* prescribed = nullptr;
   cxg::PatternOut pat;
   double* state[2] = {nullptr, nullptr};  // SoA [13][G]: committed, trial
+  // The back stress (components 7..12) is zero in both buffers and no material has a
+  // kinematic modulus, so it stays zero: the element pass and commit move only the
+  // first 7 components. Cleared for good by cxg_state_set.
+  bool back_stress_zero = true;
+  bool kinematic = false;  // some material has h_kin != 0
   cxg::DevStatus* status = nullptr;
   void* edata = nullptr;      // per-element K blocks of the two-pass assembly
   size_t edata_bytes = 0;
   double* fdata = nullptr;    // per-element internal force (material-point mode)
+  size_t fdata_bytes = 0;
+  cxg::WinSched sched[2][2];  // [precision][tangent]
+  int64_t ring_bytes = 0;     // element-buffer budget: 0 default share of L2, < 0 one window
+  std::vector<int32_t> node_first, node_last;  // first / last incident element per node
   cudaStream_t last_stream = nullptr;
   int64_t device_bytes = 0;
   // staging buffers for host pointers, grown on demand and reused
@@ -49,8 +74,13 @@ bool on_device(const void* p);
 // Synchronise the plan's last stream and turn an in-kernel error into a status.
 int plan_status(cxg_plan* p, int64_t* bad);
 // Allocate the per-element buffers of the two-pass assembly.
+// Allocate the per-element buffers of the two-pass assembly (ring-sized when the plan's
+// window schedule for this precision and mode has more than one window).
 int ensure_v2(cxg_plan* p, bool tangent);
+// Arguments of one whole-mesh assembly; apply_windows adds the plan's window schedule
+// for the current precision and mode (built by ensure_v2).
 V2Args v2_args(cxg_plan* p, const double* f_ext, bool accumulate);
+void apply_windows(const cxg_plan* p, bool tangent, V2Args& v);
 ElemArgs base_args(cxg_plan* p);
 
 }  // namespace api

@@ -83,6 +83,13 @@ __host__ __device__ constexpr int blk_index(int n, int a, int b) { return a * n 
 template <typename R>
 __host__ __device__ constexpr int blk_stride() { return sizeof(R) == 8 ? 10 : 12; }
 
+// Slot of element e in the element buffer: a ring of `ring` elements (the whole mesh when
+// the assembly runs as one window). Element indices fit 31 bits (incidence codes are
+// e*n + local index in int32), so the modulo is 32-bit.
+__device__ __forceinline__ int64_t ring_slot(int64_t e, int64_t ring) {
+  return static_cast<int64_t>(static_cast<uint32_t>(e) % static_cast<uint32_t>(ring));
+}
+
 template <typename R>
 __device__ __forceinline__ void store_block(R* dst, const R (&v)[9]) {
   if constexpr (sizeof(R) == 8) {
@@ -344,12 +351,13 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * kW1 + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kW1;
-  for (int64_t e0 = gwarp * EPW; e0 < A.n_elems; e0 += nwarps * EPW) {
+  const int64_t e_end = V.e_end;  // elements [V.e_begin, V.e_end) of this window
+  for (int64_t e0 = V.e_begin + gwarp * EPW; e0 < e_end; e0 += nwarps * EPW) {
     // ---- phase A ---------------------------------------------------------------
     for (int t = lane; t < EPW * n; t += 32) {
       const int ei = t / n, k = t % n;
       const int64_t e = e0 + ei;
-      if (e < A.n_elems) {
+      if (e < e_end) {
         const int node = A.conn[e * n + k];
         for (int d = 0; d < 3; ++d) {
           W.x[ei][3 * k + d] = A.coords[3 * static_cast<int64_t>(node) + d];
@@ -359,7 +367,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
     }
     if (lane < EPW) {
       const int64_t e = e0 + lane;
-      const double E = e < A.n_elems ? A.young[e] : 1.0, nu = e < A.n_elems ? A.poisson[e] : 0.0;
+      const double E = e < e_end ? A.young[e] : 1.0, nu = e < e_end ? A.poisson[e] : 0.0;
       const double um2 = E / (1.0 + nu);
       W.lam[lane] = nu * um2 / (1.0 - 2.0 * nu);
       W.mu[lane] = um2 / 2.0;
@@ -371,7 +379,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
     for (int t = lane; t < EPW * nq; t += 32) {
       const int ei = t / nq, q = t % nq;
       const int64_t e = e0 + ei;
-      if (e >= A.n_elems) continue;
+      if (e >= e_end) continue;
       double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
       for (int k = 0; k < n; ++k) {
         const double d0 = sdN[(3 * k) * nq + q], d1 = sdN[(3 * k + 1) * nq + q], d2 = sdN[(3 * k + 2) * nq + q];
@@ -418,10 +426,14 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
         const int mat = A.elem_mat ? A.elem_mat[e] : 0;
         const int64_t gidx = e * nq + q;
         double cs[kStateDoubles], ts[kStateDoubles], sig[6], nv[6] = {0, 0, 0, 0, 0, 0};
-        for (int c = 0; c < kStateDoubles; ++c) cs[c] = A.state_c[c * A.n_gauss + gidx];
+        const int ncomp = A.state_comps;
+#pragma unroll
+        for (int c = 0; c < kStateDoubles; ++c) cs[c] = c < ncomp ? A.state_c[c * A.n_gauss + gidx] : 0.0;
         double lt, mt, ct, mhg;
         const bool pl = j2_point(A.mats[mat], W.lam[ei], W.mu[ei], W.mu_j2[ei], eps, cs, ts, sig, lt, mt, ct, nv, mhg);
-        for (int c = 0; c < kStateDoubles; ++c) A.state_t[c * A.n_gauss + gidx] = ts[c];
+#pragma unroll
+        for (int c = 0; c < kStateDoubles; ++c)
+          if (c < ncomp) A.state_t[c * A.n_gauss + gidx] = ts[c];
         for (int c = 0; c < 6; ++c) W.sig[ei][q][c] = sq * sig[c];
         W.dp[ei][q][0] = static_cast<R>(sq * lt);
         W.dp[ei][q][1] = static_cast<R>(sq * mt);
@@ -477,7 +489,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
     for (int task = lane; task < EPW * NT; task += 32) {
       const int ei = task / NT, ti = task % NT;
       const int64_t e = e0 + ei;
-      if (e < A.n_elems) {
+      if (e < e_end) {
         const int a0 = TR * s_tr[ti], b0 = TC * s_tc[ti];
 #pragma unroll
         for (int i = 0; i < TR; ++i)
@@ -566,7 +578,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
           }
         }
         if constexpr (!STAGE) {
-          R* out = reinterpret_cast<R*>(V.edata) + e * (NB * blk_stride<R>());
+          R* out = reinterpret_cast<R*>(V.edata) + ring_slot(e, V.ring) * (NB * blk_stride<R>());
 #pragma unroll
           for (int i = 0; i < TR; ++i)
 #pragma unroll
@@ -595,7 +607,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
       R* stg = W.g;  // EPW x NB blocks of 9 values
       if (lane < EPW * NT) {
         const int ei = lane / NT, ti = lane % NT;
-        if (e0 + ei < A.n_elems) {
+        if (e0 + ei < e_end) {
           const int a0 = TR * s_tr[ti], b0 = TC * s_tc[ti];
 #pragma unroll
           for (int i = 0; i < TR; ++i)
@@ -611,8 +623,8 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
         }
       }
       __syncwarp();
-      for (int ei = 0; ei < EPW && e0 + ei < A.n_elems; ++ei) {
-        R* out = reinterpret_cast<R*>(V.edata) + (e0 + ei) * (NB * BS);
+      for (int ei = 0; ei < EPW && e0 + ei < e_end; ++ei) {
+        R* out = reinterpret_cast<R*>(V.edata) + ring_slot(e0 + ei, V.ring) * (NB * BS);
         const R* sb = stg + ei * NB * 9;
         for (int pc = lane; pc < NB * CPB; pc += 32) {
           const int k = pc / CPB, part = pc % CPB;
@@ -636,7 +648,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
       for (int t = lane; t < EPW * n; t += 32) {
         const int ei = t / n, a = t % n;
         const int64_t e = e0 + ei;
-        if (e >= A.n_elems) continue;
+        if (e >= e_end) continue;
         double f[3] = {0, 0, 0};
         for (int q = 0; q < nq; ++q) {
           const double* S = W.sig[ei][q];
@@ -656,7 +668,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
             for (int d = 0; d < 3; ++d) f[d] += ka * gu[d];
           }
         }
-        for (int d = 0; d < 3; ++d) V.fdata[e * (3 * n) + 3 * a + d] = f[d];
+        for (int d = 0; d < 3; ++d) V.fdata[ring_slot(e, V.ring) * (3 * n) + 3 * a + d] = f[d];
       }
     }
     __syncwarp();
@@ -664,146 +676,133 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 }
 
 // ---- P2: row gather ------------------------------------------------------------------
-// One warp per node a. Lanes form EG groups of GS lanes (GS = 16 for elements of at
-// most 16 nodes, else 32; 8 for the <= 8-node families in mixed precision); lane lb of
-// group s handles column node lb of incident element k + s, so EG elements are applied
-// per pass. Every group copy of the rows is zeroed and read once per node, which for the
-// short rows of the <= 8-node families in FP64 costs more shared-memory traffic than
-// the idle lanes of two 16-lane groups (measured: the FP64 C3D8 tangent gather is 10 %
-// faster with two groups than with four, the mixed one 3 % slower, so it keeps four).
-// Each group adds into its own copy of the node's rows
-// in shared memory (within one element every target is distinct, so plain adds, no
-// atomics); the copies are summed in a fixed order when the rows are stored. The
-// node's incident-element codes come in with one coalesced load per 32 elements and
-// are handed out by shuffles; the free-component mask of each column node comes from
-// the per-element-node mask array, so a pass waits for one round of independent loads.
-// The connectivity is read only for constrained columns. In mixed precision the
-// diagonal 3x3 block of node a is minus the FP64 sum of all off-diagonal FP32 blocks of
-// its element rows: every lane keeps a running sum of the blocks it adds, and one
-// butterfly over the warp per node forms the block, so rigid translations stay in the
-// null space of the assembled rows to FP64 accuracy.
-template <int ET, bool DIAGFIX>
+// One warp per node a. It walks the node's incident elements in element order; for each
+// it reads row a of the element's upper-block buffer value by value: the 9n values of
+// the row (n column blocks of 9) are spread over the lanes in memory order, so a warp's
+// load covers consecutive values (the blocks (a, b >= a) are one contiguous run, each
+// block (b < a, a) a contiguous 9-value piece read transposed) instead of every lane
+// fetching a whole block of its own. Each value is added into the node's rows held in
+// shared memory (one copy per warp; within one element every target is distinct, so
+// plain adds, no atomics), so every CSR value is the sum of its contributions in
+// element order, as in the reference's scatter (src/fem/assembly.cpp:76-100).
+// Prescribed columns go into the rhs (-K_fc u_c, src/fem/assembly.cpp:95-96), the load
+// vector and the internal forces are added, and the rows are stored once with
+// coalesced writes. The node's row length L is padded to L' = 3 (mod 16) doubles in
+// the buffer, so the 3 rows x 3 components of one block fall into distinct banks.
+// The incident-element codes come in with one coalesced load per 32 elements and are
+// handed out by shuffles; the column masks and slots of the element's nodes are loaded
+// once per element by lanes 0..n-1 and shuffled to the lanes that use them.
+// In mixed precision the diagonal 3x3 block of node a is minus the FP64 sum of all
+// off-diagonal FP32 blocks of its element rows: every lane keeps running sums of the
+// values it adds (one per iteration and orientation, so the target component is fixed
+// per lane), and nine butterflies over the warp form the block, so rigid translations
+// stay in the null space of the assembled rows to FP64 accuracy.
+template <int ET>
 struct P2Geo {
   static constexpr int n = nodes_of(ET);
-  static constexpr int GS = (DIAGFIX && n <= 8) ? 8 : (n <= 16 ? 16 : 32);
-  static constexpr int EG = 32 / GS;
+  static constexpr int NB = n * (n + 1) / 2;
+  static constexpr int NV = 9 * n;              // values of one element row
+  static constexpr int IT = (NV + 31) / 32;     // lane iterations per element row
 };
 
+// start of block row x in the upper-block numbering: blk_index(n, x, b) = row0(x) + b
+__host__ __device__ constexpr int blk_row0(int n, int x) { return x * n - x * (x - 1) / 2 - x; }
 
 template <typename R>
-struct P2Pass {
-  double v[9];
-  int64_t e;
-  int la, mb, slotv;
-  bool active;
-};
-
-template <int ET, typename R>
-__device__ __forceinline__ void p2_fetch(const ElemArgs& A, const R* ed, int code, bool active, int lb, P2Pass<R>& p) {
-  constexpr int n = nodes_of(ET), NB = n * (n + 1) / 2;
-  p.active = active;
-  p.e = code / n;
-  p.la = code % n;
-  if (active) {
-    p.mb = __ldg(A.conn_mask + p.e * n + lb);
-    p.slotv = __ldg(A.slot + (p.e * n + p.la) * n + lb);
-    const bool tr = lb < p.la;
-    double raw[9];
-    load_block<R>(ed + p.e * (NB * blk_stride<R>()) +
-                      (tr ? blk_index(n, lb, p.la) : blk_index(n, p.la, lb)) * blk_stride<R>(),
-                  raw);
-#pragma unroll
-    for (int q = 0; q < 9; ++q) p.v[q] = tr ? raw[3 * (q % 3) + q / 3] : raw[q];
-  } else {
-    p.mb = 0;
-    p.slotv = 0;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) p.v[q] = 0.0;
-  }
+__device__ __forceinline__ double ld_val(const R* p) {
+  return static_cast<double>(__ldg(p));
 }
 
 template <int ET, bool TAN, typename R, bool DIAGFIX>
 __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
-  constexpr int n = nodes_of(ET);
-  constexpr int GS = P2Geo<ET, DIAGFIX>::GS, EG = P2Geo<ET, DIAGFIX>::EG;
+  using PG = P2Geo<ET>;
+  constexpr int n = PG::n, NB = PG::NB, NV = PG::NV, IT = PG::IT;
+  constexpr int BS = blk_stride<R>();
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int stride = static_cast<int>(V.row_stride);  // shared-memory offsets are 32-bit
-  double* buf = reinterpret_cast<double*>(smem) + warp * (EG * stride);
+  double* buf = reinterpret_cast<double*>(smem) + warp * stride;
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   const R* ed = reinterpret_cast<const R*>(V.edata);
-  const int sub = lane / GS, lb = lane % GS;
-  const bool lane_ok = lb < n;
-  double* mine = buf + sub * stride;
-  for (int64_t a = gwarp; a < A.n_nodes; a += nwarps) {
+  // per-lane constants of every iteration: column node lb, position p in the block
+  int lbv[IT], pv[IT], r0v[IT];
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int v = lane + 32 * it;
+    lbv[it] = v < NV ? v / 9 : -1;
+    pv[it] = v % 9;
+    r0v[it] = v < NV ? blk_row0(n, v / 9) : 0;
+  }
+  // nodes [V.n_begin, V.n_end) of this window's node list (node_order), or of the mesh
+  for (int64_t idx = V.n_begin + gwarp; idx < V.n_end; idx += nwarps) {
+    const int64_t a = V.node_order ? static_cast<int64_t>(V.node_order[idx]) : idx;
     const int ma = A.node_mask[a];
     const int nf = __popc(ma);
     const int L = static_cast<int>(A.node_rowlen[a]);
-    const int total = nf * L;
+    const int Lp = L + ((3 - L) % 16 + 16) % 16;  // L' = 3 (mod 16)
     double* vout = A.vals + A.node_base[a];
     const int64_t i0 = V.inc_ptr[a], i1 = V.inc_ptr[a + 1];
-    // offset of row i (free component i of node a) in the row buffer
     int row_off[3];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) row_off[i] = __popc(ma & ((1 << i) - 1)) * L;
-    for (int g = 0; g < EG; ++g)
-      for (int t = lane; t < total; t += 32) buf[g * stride + t] = (g == 0 && V.accumulate) ? vout[t] : 0.0;
+    for (int i = 0; i < 3; ++i) row_off[i] = __popc(ma & ((1 << i) - 1)) * Lp;
+    for (int t = lane; t < nf * Lp; t += 32) buf[t] = 0.0;
     __syncwarp();
     double rr[3] = {0.0, 0.0, 0.0};
-    double fs[3] = {0.0, 0.0, 0.0};
-    double dsum[9];  // this lane's FP64 sum of the off-diagonal blocks it added (DIAGFIX)
+    double fsum = 0.0;  // lanes 0..2: component `lane` of the node's internal force
+    double dU[IT], dL[IT];  // DIAGFIX running sums of the upper / transposed values
 #pragma unroll
-    for (int q = 0; q < 9; ++q) dsum[q] = 0.0;
+    for (int it = 0; it < IT; ++it) dU[it] = dL[it] = 0.0;
     int slot_aa = 0;  // column offset of node a in its own rows
     for (int64_t c0 = i0; c0 < i1; c0 += 32) {
       const int cnt = static_cast<int>(i1 - c0 < 32 ? i1 - c0 : 32);
       const int code_l = lane < cnt ? __ldg(V.inc_code + c0 + lane) : 0;
-      for (int k = 0; k < cnt; k += EG) {
-        P2Pass<R> cur;
-        p2_fetch<ET, R>(A, ed, __shfl_sync(0xffffffffu, code_l, (k + sub) & 31), lane_ok && k + sub < cnt, lb, cur);
-        if (cur.active && (!DIAGFIX || lb != cur.la)) {
-          double* col = mine + cur.slotv;
-          if (cur.mb == 7) {  // every component of the column node is free
+      for (int k = 0; k < cnt; ++k) {
+        const int code = __shfl_sync(0xffffffffu, code_l, k);
+        const int64_t e = code / n;
+        const int la = code % n;
+        // column masks and slots of the element's nodes, one lane per node
+        int mb_l = 0, sl_l = 0;
+        if (lane < n) {
+          mb_l = __ldg(A.conn_mask + e * n + lane);
+          sl_l = __ldg(A.slot + (e * n + la) * n + lane);
+        }
+        const int64_t es = ring_slot(e, V.ring);
+        const R* eb = ed + es * (NB * BS);
+        const int r0a = blk_row0(n, la);
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              if ((ma >> i) & 1) {
-                double* r = col + row_off[i];
-                r[0] += cur.v[3 * i];
-                r[1] += cur.v[3 * i + 1];
-                r[2] += cur.v[3 * i + 2];
-              }
+        for (int it = 0; it < IT; ++it) {
+          const int lb = lbv[it];
+          const int mb = __shfl_sync(0xffffffffu, mb_l, lb < 0 ? 0 : lb);
+          const int sl = __shfl_sync(0xffffffffu, sl_l, lb < 0 ? 0 : lb);
+          if (lb < 0) continue;
+          const bool up = lb >= la;
+          const int p = pv[it];
+          const int blk = up ? r0a + lb : r0v[it] + la;
+          const double x = ld_val<R>(eb + blk * BS + p);
+          const int i = up ? p / 3 : p % 3;
+          const int j = up ? p % 3 : p / 3;
+          if (DIAGFIX) {
+            if (lb == la) {
+              slot_aa = sl;
+              continue;
             }
+            if (up) dU[it] += x; else dL[it] += x;
+          }
+          if (!((ma >> i) & 1)) continue;
+          if ((mb >> j) & 1) {
+            const int ro = i == 0 ? row_off[0] : (i == 1 ? row_off[1] : row_off[2]);
+            buf[ro + sl + __popc(mb & ((1 << j) - 1))] += x;
           } else {
-            int64_t nb = -1;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              if (!((ma >> i) & 1)) continue;
-#pragma unroll
-              for (int j = 0; j < 3; ++j) {
-                if ((cur.mb >> j) & 1) {
-                  col[row_off[i] + __popc(cur.mb & ((1 << j) - 1))] += cur.v[3 * i + j];
-                } else {
-                  if (nb < 0) nb = A.conn[cur.e * n + lb];
-                  const double pv = A.prescribed[3 * nb + j];
-                  if (pv != 0.0) rr[i] -= cur.v[3 * i + j] * pv;
-                }
-              }
+            const double pvl = A.prescribed[3 * static_cast<int64_t>(A.conn[e * n + lb]) + j];
+            if (pvl != 0.0) {
+              if (i == 0) rr[0] -= x * pvl;
+              else if (i == 1) rr[1] -= x * pvl;
+              else rr[2] -= x * pvl;
             }
           }
         }
-        if (TAN && cur.active && lb == cur.la) {
-#pragma unroll
-          for (int d = 0; d < 3; ++d) fs[d] += __ldg(V.fdata + cur.e * (3 * n) + 3 * cur.la + d);
-        }
-        if (DIAGFIX && cur.active) {
-          if (lb != cur.la) {
-#pragma unroll
-            for (int q = 0; q < 9; ++q) dsum[q] += cur.v[q];
-          } else {
-            slot_aa = cur.slotv;  // slot(la, la)
-          }
-        }
+        if (TAN && lane < 3) fsum += __ldg(V.fdata + es * (3 * n) + 3 * la + lane);
         __syncwarp();
       }
     }
@@ -813,7 +812,13 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
       double d9[9];
 #pragma unroll
       for (int q = 0; q < 9; ++q) {
-        double x = dsum[q];
+        double x = 0.0;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+          const int p = pv[it];
+          if (p == q) x += dU[it];
+          if ((p % 3) * 3 + p / 3 == q) x += dL[it];
+        }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
         d9[q] = -x;
@@ -830,8 +835,12 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
             const int ro = i == 0 ? row_off[0] : (i == 1 ? row_off[1] : row_off[2]);
             buf[ro + slot_aa + __popc(ma & ((1 << j) - 1))] += d;
           } else {
-            const double pv = A.prescribed[3 * a + j];
-            if (pv != 0.0) rr[i] -= d * pv;
+            const double pvl = A.prescribed[3 * a + j];
+            if (pvl != 0.0) {
+              if (i == 0) rr[0] -= d * pvl;
+              else if (i == 1) rr[1] -= d * pvl;
+              else rr[2] -= d * pvl;
+            }
           }
         }
       }
@@ -849,34 +858,19 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
         }
       }
     }
-    if (TAN && A.f_int) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double v = fs[d];
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if (lane == 0) A.f_int[3 * a + d] = (V.accumulate ? A.f_int[3 * a + d] : 0.0) + v;
-      }
-    }
-    for (int t = lane; t < total; t += 32) {
-      double v = buf[t];
-#pragma unroll
-      for (int g = 1; g < EG; ++g) v += buf[g * stride + t];
-      vout[t] = v;
+    if (TAN && A.f_int && lane < 3) A.f_int[3 * a + lane] = (V.accumulate ? A.f_int[3 * a + lane] : 0.0) + fsum;
+    for (int r = 0; r < nf; ++r) {
+      const double* src = buf + r * Lp;
+      double* dst = vout + static_cast<int64_t>(r) * L;
+      for (int t = lane; t < L; t += 32) dst[t] = V.accumulate ? dst[t] + src[t] : src[t];
     }
     __syncwarp();
   }
 }
 
-// Blocks of at most 8 warps. The mixed-precision gather of the <= 8-node families is
-// compiled for 3 resident blocks per SM (<= 85 registers), which its short rows leave
-// room for in shared memory; the other gathers are compiled without a register budget.
+// Blocks of at most 8 warps.
 template <int ET, bool TAN, typename R, bool DIAGFIX>
-__global__ void p2_kernel(ElemArgs A, V2Args V) {
-  p2_body<ET, TAN, R, DIAGFIX>(A, V);
-}
-
-template <int ET, bool TAN, typename R, bool DIAGFIX>
-__global__ void __launch_bounds__(256, 3) p2_kernel_short(ElemArgs A, V2Args V) {
+__global__ void __launch_bounds__(256) p2_kernel(ElemArgs A, V2Args V) {
   p2_body<ET, TAN, R, DIAGFIX>(A, V);
 }
 
@@ -905,9 +899,10 @@ cudaError_t launch_p1_tile(const ElemArgs& a, const V2Args& v, const LaunchCfg& 
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT1, smem);
   if (err != cudaSuccess) return err;
   constexpr int EPW = Geo<ET, TILE>::EPW;
-  const int64_t need = (a.n_elems + kW1 * EPW - 1) / (kW1 * EPW);
+  const int64_t count = v.e_end - v.e_begin;
+  const int64_t need = (count + kW1 * EPW - 1) / (kW1 * EPW);
   const int64_t grid = persistent_grid(need, per_sm, cfg.p1_blocks_per_sm);
-  if (a.n_elems == 0) return cudaSuccess;
+  if (count <= 0) return cudaSuccess;
   kern<<<static_cast<unsigned>(grid), kT1, smem, s>>>(a, v);
   return cudaGetLastError();
 }
@@ -926,11 +921,12 @@ cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg
 
 template <int ET, bool TAN, typename R, bool DF>
 cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaStream_t s) {
-  auto kern = (DF && nodes_of(ET) <= 8) ? p2_kernel_short<ET, TAN, R, DF> : p2_kernel<ET, TAN, R, DF>;
+  auto kern = p2_kernel<ET, TAN, R, DF>;
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
-  // configured count when it fits)
-  const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
-  const int64_t wbytes = P2Geo<ET, DF>::EG * stride * 8;
+  // configured count when it fits). A node's nf rows padded to L' <= L + 15 take at
+  // most max_row + 45 doubles.
+  const int64_t stride = (v.max_row + 48) / 2 * 2;
+  const int64_t wbytes = stride * 8;
   int warps = cfg.p2_warps > 0 ? std::min(cfg.p2_warps, 8) : 8;
   while (warps > 1 && warps * wbytes > 160 * 1024) warps /= 2;
   const size_t smem = static_cast<size_t>(warps) * wbytes;
@@ -941,14 +937,39 @@ cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaS
   int per_sm = 0;
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
   if (err != cudaSuccess) return err;
-  const int64_t need = (a.n_nodes + warps - 1) / warps;
+  const int64_t count = v.n_end - v.n_begin;
+  if (count <= 0) return cudaSuccess;
+  const int64_t need = (count + warps - 1) / warps;
   const int64_t grid = persistent_grid(need, per_sm, cfg.p2_blocks_per_sm);
   kern<<<static_cast<unsigned>(grid), warps * 32, smem, s>>>(a, v);
   return cudaGetLastError();
 }
 
 template <int ET>
+cudaError_t launch_v2_pair(int mode, int precision, const ElemArgs& a, const V2Args& v, const LaunchCfg& c,
+                           cudaStream_t s);
+
+// Every window's element pass and row gather in order on one stream: the row gather of
+// window w reads element blocks that stay in the ring (and in L2) until the element
+// pass of window w+1 overwrites the slots of elements no later node needs.
+template <int ET>
 cudaError_t launch_v2_type(int mode, int precision, const ElemArgs& a, const V2Args& v, const LaunchCfg& c,
+                           cudaStream_t s) {
+  if (v.n_win <= 1) return launch_v2_pair<ET>(mode, precision, a, v, c, s);
+  V2Args w = v;
+  for (int32_t k = 0; k < v.n_win; ++k) {
+    w.e_begin = v.win_e[k];
+    w.e_end = v.win_e[k + 1];
+    w.n_begin = v.win_n[k];
+    w.n_end = v.win_n[k + 1];
+    const cudaError_t err = launch_v2_pair<ET>(mode, precision, a, w, c, s);
+    if (err != cudaSuccess) return err;
+  }
+  return cudaSuccess;
+}
+
+template <int ET>
+cudaError_t launch_v2_pair(int mode, int precision, const ElemArgs& a, const V2Args& v, const LaunchCfg& c,
                            cudaStream_t s) {
   cudaError_t err = cudaSuccess;
   if (mode == MODE_LINEAR) {
@@ -1109,6 +1130,10 @@ cudaError_t launch_scalar_type(int kind, const ElemArgs& a, const V2Args& v, con
 }
 
 }  // namespace
+
+size_t v2_bytes_per_element(int t, int precision, bool tangent) {
+  return v2_edata_bytes(t, 1, precision) + (tangent ? sizeof(double) * 3 * nodes_of(t) : 0);
+}
 
 size_t v2_edata_bytes(int t, int64_t n_elems, int precision) {
   const int n = nodes_of(t);

@@ -148,6 +148,20 @@ CXG_API int cxg_plan_update_young(cxg_plan* plan, const double* young);
  * do not depend on the shape. */
 CXG_API int cxg_plan_set_launch_config(cxg_plan* plan, int32_t mode, int32_t tile, int32_t p1_blocks_per_sm,
                                        int32_t p2_warps);
+/* No counterpart in the reference (a tuning knob of this library). Device-memory
+ * budget of the element buffers that carry K_e blocks from the element pass to the
+ * row gather. The assembly runs in windows of consecutive elements, each followed by
+ * the row gather of the nodes it completes, with the buffers holding only as many
+ * elements as the budget allows, so that they stay in L2 between the two passes.
+ * 0 (default) = five eighths of the GPU's L2; < 0 = one window over the whole mesh
+ * (buffers for every element). The windows follow from the element ordering: a node
+ * waits for its last incident element, so the ring must also hold the largest
+ * distance between a node's first and last element; when the budget cannot, the
+ * assembly runs as one window. Results do not depend on the budget. */
+CXG_API int cxg_plan_set_ring_bytes(cxg_plan* plan, int64_t bytes);
+/* Windows of the current precision's linear (mode 0) or tangent (mode 1) assembly and
+ * the elements its buffers hold (both from the last assembly of that mode; 0 before). */
+CXG_API int cxg_plan_get_windows(const cxg_plan* plan, int32_t mode, int32_t* n_windows, int64_t* ring_elems);
 /* Synchronise the stream of the last launch and report the first in-kernel error
  * (CXG_ERR_NEGATIVE_JACOBIAN, CXG_ERR_UNKNOWN_NODE) with the offending element. */
 CXG_API int cxg_plan_check(cxg_plan* plan, int64_t* bad_element);
