@@ -20,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_lib", "libcxo.so")
 REF_SO = os.path.join(HERE, "_ref", "libcxpp_ref.so")
+ADAPTER_SO = os.path.join(HERE, "_ref", "libcxg_cxpp_test.so")
 
 NODES = {0: 4, 1: 10, 2: 8, 3: 8, 4: 20, 5: 20, 6: 6, 7: 15}
 NGP = {0: 1, 1: 4, 2: 8, 3: 1, 4: 27, 5: 8, 6: 2, 7: 6}
@@ -135,6 +136,18 @@ REF_SIGS = dict(_COMMON, **{
     "sensitivity_compliance": (_i, [_vp, _i64t, _vp, _vp, _d, _vp, _vp]),
     "assemble_csr_threads": (_i, [_i, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i]),
 })
+
+
+# The reference's drivers with the product's C++ adapter (ref_cuda_shim.cpp).
+ADAPTER_SIGS = {
+    "last_error": (C.c_char_p, []),
+    "solve_linear_static": (_i, [_vp, _i, _i, _vp, _vp]),
+    "assembler_create": (_vp, [_vp, _i]),
+    "assembler_free": (None, [_vp]),
+    "assembler_sizes": (_i, [_vp, _vp, _vp]),
+    "assemble_linear": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "assemble_tangent": (_i, [_vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _i]),
+}
 
 
 class _Base:
@@ -547,3 +560,57 @@ class RefModel:
         self.ref._check(f(_vp(self.h), var_node.size, _p(var_node), _p(var_comp), h,
                           _p(dg), C.byref(obj)))
         return dg, obj.value
+
+
+class RefCuda(_Base):
+    """The reference's linear-static driver and assembly calls with the assembly through
+    the product's C++ adapter (oracle/_ref/libcxg_cxpp_test.so); models come from Ref."""
+
+    prefix = "cuda"
+    sigs = ADAPTER_SIGS
+
+    def __init__(self, path=ADAPTER_SO):
+        super().__init__(path)
+
+    @staticmethod
+    def available(path=ADAPTER_SO):
+        return os.path.exists(path)
+
+    def solve_linear_static(self, ref_model, gpu, precision=0):
+        """(u (N,3), nodal stress (N,6)) of numerics::solve_linear_static with a direct
+        solve; gpu selects the adapter's assembly."""
+        N = ref_model.mesh.n_nodes
+        u, st = np.zeros(3 * N), np.zeros(6 * N)
+        self._check(self._fn("solve_linear_static")(_vp(ref_model.h), int(gpu), int(precision), _p(u), _p(st)))
+        return u.reshape(N, 3), st.reshape(N, 6)
+
+    def assembler(self, ref_model, precision=0):
+        h = self._fn("assembler_create")(_vp(ref_model.h), int(precision))
+        if not h:
+            raise OracleError(self.last_error())
+        return h
+
+    def free(self, h):
+        self._fn("assembler_free")(_vp(h))
+
+    def _arrays(self, h):
+        nnz, nf = C.c_int64(), C.c_int64()
+        self._check(self._fn("assembler_sizes")(_vp(h), C.byref(nnz), C.byref(nf)))
+        n = nnz.value
+        return np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n), np.zeros(nf.value)
+
+    def assemble_linear(self, h):
+        """The adapter's LinearSystem: (rows, cols, vals, rhs), COO in (row, column) order."""
+        rows, cols, vals, rhs = self._arrays(h)
+        self._check(self._fn("assemble_linear")(_vp(h), _p(rows), _p(cols), _p(vals), _p(rhs)))
+        return rows, cols, vals, rhs
+
+    def assemble_tangent(self, h, u, commit=False):
+        """assemble_material_tangent through the adapter at u[3N]: (rows, cols, vals, rhs,
+        f_int); commit afterwards when asked."""
+        u = _f64(u)
+        rows, cols, vals, rhs = self._arrays(h)
+        f_int = np.zeros(u.size)
+        self._check(self._fn("assemble_tangent")(_vp(h), u.size // 3, _p(u), _p(rows), _p(cols), _p(vals), _p(rhs),
+                                                 _p(f_int), int(commit)))
+        return rows, cols, vals, rhs, f_int

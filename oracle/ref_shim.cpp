@@ -309,6 +309,9 @@ void* ref_model_create(int64_t n_nodes, const double* coords, int64_t n_elems,
 
 void ref_model_free(void* model) { delete static_cast<RefModel*>(model); }
 
+// The Model behind a handle, for other harness translation units (ref_cuda_shim.cpp).
+const cxpp::Model* ref_model_get(void* model) { return &static_cast<RefModel*>(model)->model; }
+
 // element_mass (lumped = 0) / element_mass_lumped (lumped = 1), element.hpp:93-102.
 int ref_element_mass(int type, const double* coords, double rho, int lumped, double* Me) {
   try {

@@ -70,3 +70,13 @@ def test_ref_handles_round_trip(ref):
     mp = rm.material_points()
     assert isinstance(mp, int) and mp > 0
     assert rm.state().size == 13 * m.n_elems * mg.NGP[mg.C3D8]
+
+
+def test_adapter_library_loads_with_its_signatures(ref):
+    """The C++ adapter's test library (the product adapter compiled against the
+    reference headers) loads without a GPU and exports every declared entry point."""
+    from oracle.oracle import ADAPTER_SIGS, RefCuda
+    if not RefCuda.available():
+        pytest.skip("adapter library not built here")
+    lib = RefCuda()
+    _check_sigs(lib, ADAPTER_SIGS, ("assembler_create",))
