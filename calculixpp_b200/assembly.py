@@ -207,8 +207,9 @@ class Plan:
     def tune(self, step, tangent=False, reps=3):
         """Time `step()` (one assembly through this plan) with CUDA events for every tile
         and element-pass grid shape of the current precision, then for the row gather's
-        warps per block (8, 4, 2) at the kept element-pass shape; keep the fastest and
-        return it with its time in ms."""
+        warps per block (8, 4, 2) at the kept element-pass shape, then for the
+        element-buffer budget of the windowed assembly (default, one window, 40 % and 85 %
+        of L2); keep the fastest and return it with its time in ms."""
 
         def timed(tile, bps, warps):
             try:
@@ -237,9 +238,19 @@ class Plan:
             ms = timed(best[1], best[2], warps)
             if ms is not None and ms < best[0]:
                 best = (ms, best[1], best[2], warps)
+        # element-buffer budget: one window, or windows whose buffers take a share of L2
+        # (results do not depend on it)
+        l2 = torch.cuda.get_device_properties(self.device).L2_cache_size
+        ring, ring_ms = 0, best[0]
+        for budget in (-1, int(0.4 * l2), int(0.85 * l2)):
+            self.set_ring_bytes(budget)
+            ms = timed(best[1], best[2], best[3])
+            if ms is not None and ms < ring_ms:
+                ring, ring_ms = budget, ms
+        self.set_ring_bytes(ring)
         self.set_launch_config(tangent, best[1], best[2], best[3])
         return {"tile": {0: "2x4", 1: "2x2", 2: "4x4"}[best[1]], "p1_blocks_per_sm": best[2],
-                "p2_warps": best[3] or 8, "ms": best[0]}
+                "p2_warps": best[3] or 8, "ring_bytes": ring, "ms": ring_ms}
 
     # -- assembly --------------------------------------------------------------------
     def assemble_linear(self, f_ext=None, vals=None, rhs=None, check=True):

@@ -210,6 +210,104 @@ __device__ bool j2_point(const J2Mat& M, double lam, double mu_el, double mu, co
   return true;
 }
 
+// Band around the yield surface, as a fraction of the current yield stress, inside which
+// the mixed-precision path decides and returns in FP64.
+constexpr float kYieldBandFp32 = 1e-3f;
+
+// J2 return of the mixed-precision path: the same steps as j2_point
+// (src/fem/plasticity.cpp:90-236) with the trial stress, the local Newton on the plastic
+// multiplier, the stress and history update and the consistent-tangent parameters in
+// FP32. The consistency scalar f = q_tr - sigma_y(ep0) decides the branch in FP32 only
+// when |f| exceeds kYieldBandFp32 * sigma_y, clear of the FP32 rounding of q_tr; points
+// inside the band, and points whose FP32 Newton does not settle, take the FP64 return.
+// The hardening table is read in FP64 (it is indexed by the FP64 history).
+__device__ bool j2_point_mixed(const J2Mat& M, double lam, double mu_el, double mu, const double* eps,
+                               const double* cs, double* ts, double* sig, double& lam_t, double& mu_t,
+                               double& c_t, double* nv, double& mu_hg) {
+  const float l = static_cast<float>(lam), me = static_cast<float>(mu_el), m = static_cast<float>(mu);
+  const float hk = static_cast<float>(M.h_kin);
+  float el[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) el[i] = static_cast<float>(eps[i] - cs[i]);
+  const float l2m = l + 2.0f * me;
+  float st[6];
+  st[0] = l2m * el[0] + l * el[1] + l * el[2];
+  st[1] = l * el[0] + l2m * el[1] + l * el[2];
+  st[2] = l * el[0] + l * el[1] + l2m * el[2];
+  st[3] = me * el[3];
+  st[4] = me * el[4];
+  st[5] = me * el[5];
+  const float p = (st[0] + st[1] + st[2]) / 3.0f;
+  const float s_tr[6] = {st[0] - p, st[1] - p, st[2] - p, st[3], st[4], st[5]};
+  float xi[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) xi[i] = s_tr[i] - static_cast<float>(cs[7 + i]);
+  const float xi_norm = sqrtf(xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2] +
+                              2.0f * (xi[3] * xi[3] + xi[4] * xi[4] + xi[5] * xi[5]));
+  const float sq32 = static_cast<float>(kSqrt3_2v2);
+  const float q_tr = sq32 * xi_norm;
+  double sy0 = 0.0, h0 = 0.0;
+  if (M.plastic) hardening2(M, cs[6], sy0, h0);
+  const float f = q_tr - static_cast<float>(sy0);
+  if (M.plastic && fabsf(f) <= kYieldBandFp32 * static_cast<float>(sy0))
+    return j2_point(M, lam, mu_el, mu, eps, cs, ts, sig, lam_t, mu_t, c_t, nv, mu_hg);
+  if (!M.plastic || f <= 0.0f || xi_norm == 0.0f) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) sig[i] = st[i];
+#pragma unroll
+    for (int i = 0; i < kStateDoubles; ++i) ts[i] = cs[i];
+    lam_t = lam;
+    mu_t = mu_el;
+    c_t = 0.0;
+    mu_hg = mu_el;
+    return false;
+  }
+  const double ep0 = cs[6];
+  float dgamma = 0.0f;
+  bool settled = false;
+  for (int it = 0; it < 50; ++it) {
+    double sy, h_iso;
+    hardening2(M, ep0 + dgamma, sy, h_iso);
+    const float g = q_tr - 3.0f * m * dgamma - hk * dgamma - static_cast<float>(sy);
+    const float dg = -(3.0f * m + hk + static_cast<float>(h_iso));
+    const float step = -g / dg;
+    dgamma += step;
+    if (dgamma < 0.0f) dgamma = 0.0f;
+    if (fabsf(step) <= 4e-7f * dgamma) {
+      settled = true;
+      break;
+    }
+  }
+  if (!settled) return j2_point(M, lam, mu_el, mu, eps, cs, ts, sig, lam_t, mu_t, c_t, nv, mu_hg);
+  float n32[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) n32[i] = xi[i] / xi_norm;
+  const float dev_scale = 2.0f * m * dgamma * sq32;
+  const float alpha_scale = (2.0f / 3.0f) * hk * dgamma * sq32;
+  const float dep_scale = dgamma * sq32;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    nv[i] = n32[i];
+    sig[i] = (s_tr[i] - dev_scale * n32[i]) + (i < 3 ? p : 0.0f);
+    ts[i] = cs[i] + static_cast<double>(dep_scale * n32[i] * (i < 3 ? 1.0f : 2.0f));
+    ts[7 + i] = cs[7 + i] + static_cast<double>(alpha_scale * n32[i]);
+  }
+  ts[6] = ep0 + static_cast<double>(dgamma);
+  double sy, h_iso;
+  hardening2(M, ep0 + dgamma, sy, h_iso);
+  const float theta = 1.0f - dev_scale / xi_norm;
+  const float denom = 1.0f + (static_cast<float>(h_iso) + hk) / (3.0f * m);
+  const float theta_bar = 1.0f / denom - (1.0f - theta);
+  const float lt = l + (2.0f / 3.0f) * (1.0f - theta) * m;
+  const float mt = me - (1.0f - theta) * m;
+  const float ct = 2.0f * m * theta_bar;
+  lam_t = lt;
+  mu_t = mt;
+  c_t = ct;
+  mu_hg = mt - ct * n32[3] * n32[3];
+  return true;
+}
+
 __constant__ double c_hg2[4][8] = {
     {1, 1, -1, -1, -1, -1, 1, 1},
     {1, -1, -1, 1, -1, 1, 1, -1},
@@ -430,7 +528,11 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 #pragma unroll
         for (int c = 0; c < kStateDoubles; ++c) cs[c] = c < ncomp ? A.state_c[c * A.n_gauss + gidx] : 0.0;
         double lt, mt, ct, mhg;
-        const bool pl = j2_point(A.mats[mat], W.lam[ei], W.mu[ei], W.mu_j2[ei], eps, cs, ts, sig, lt, mt, ct, nv, mhg);
+        // FP64 return in the FP64 path; FP32 (with the FP64 band near yield) in mixed precision
+        const bool pl = sizeof(R) == 8
+                            ? j2_point(A.mats[mat], W.lam[ei], W.mu[ei], W.mu_j2[ei], eps, cs, ts, sig, lt, mt, ct, nv, mhg)
+                            : j2_point_mixed(A.mats[mat], W.lam[ei], W.mu[ei], W.mu_j2[ei], eps, cs, ts, sig, lt, mt,
+                                             ct, nv, mhg);
 #pragma unroll
         for (int c = 0; c < kStateDoubles; ++c)
           if (c < ncomp) A.state_t[c * A.n_gauss + gidx] = ts[c];

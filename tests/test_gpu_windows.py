@@ -48,7 +48,7 @@ def test_windowed_linear_equals_one_window(cuda, etype, precision):
     v1, r1 = (to_np(t).copy() for t in one.assemble_linear(f))
     assert one.windows()[0] == 1
     win = Plan(model, precision)
-    win.set_ring_bytes(_ring_budget(win, False, 64))
+    win.set_ring_bytes(_ring_budget(win, False, 32))
     v2, r2 = (to_np(t).copy() for t in win.assemble_linear(f))
     nw, ring = win.windows()
     assert nw > 2 and ring < model.mesh.n_elems, (nw, ring)
@@ -62,7 +62,7 @@ def test_windowed_tangent_equals_one_window(cuda, precision):
     one = Plan(model, precision)
     one.set_ring_bytes(-1)
     win = Plan(model, precision)
-    win.set_ring_bytes(_ring_budget(win, True, 64))
+    win.set_ring_bytes(_ring_budget(win, True, 32))
     x = model.mesh.coords
     for k in range(1, 4):
         u = np.zeros_like(x)

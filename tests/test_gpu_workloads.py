@@ -33,7 +33,7 @@ pytestmark = pytest.mark.gpu
 def _on_oracle_pattern(plan, vals, rp, ci):
     """GPU values restricted to the oracle's pattern; the pattern must contain it and
     the entries the oracle leaves out (every contribution exactly 0.0 there) must be
-    below rounding."""
+    below rounding (FP64 rounding, or FP32 rounding of the blocks in mixed precision)."""
     rpg, cig = (to_np(t) for t in plan.pattern())
     v = to_np(vals)
     if np.array_equal(rpg, rp) and np.array_equal(cig, ci):
@@ -43,7 +43,8 @@ def _on_oracle_pattern(plan, vals, rp, ci):
     ko = np.repeat(np.arange(nf), np.diff(rp)).astype(np.int64) * nf + ci
     keep = np.isin(kg, ko)
     assert keep.sum() == ko.size
-    assert np.abs(v[~keep]).max(initial=0.0) <= 1e-12 * np.abs(v).max()
+    extra = 1e-12 if plan.precision == "fp64" else 1e-6
+    assert np.abs(v[~keep]).max(initial=0.0) <= extra * np.abs(v).max()
     return v[keep]
 
 
@@ -127,7 +128,10 @@ def test_batched_workload_slices(cuda, port, precision):
         keep = np.isin(kb, ko)
         assert keep.sum() == ko.size, k
         v = to_np(vk)
-        assert np.abs(v[~keep]).max(initial=0.0) <= 1e-12 * np.abs(v).max(), k
+        # entries the reference leaves out (all contributions exactly 0.0 there) are zero
+        # to rounding: FP64 rounding, or FP32 rounding of the blocks in mixed precision
+        extra = 1e-12 if precision == "fp64" else 1e-6
+        assert np.abs(v[~keep]).max(initial=0.0) <= extra * np.abs(v).max(), k
         if precision == "fp64":
             assert rel_fro(v[keep], vo) <= 1e-12, k
             assert rel_fro(to_np(rk), rhs_o) <= 1e-12, k
