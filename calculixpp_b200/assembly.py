@@ -197,6 +197,17 @@ class Plan:
         0 = default share of L2, < 0 = one window over the whole mesh."""
         _lib.check(self.lib.cxg_plan_set_ring_bytes(self.h, int(nbytes)))
 
+    def use_reference_pattern(self, enable=True):
+        """Switch the linear assembly to the reference's own CSR pattern (entries whose
+        every element contribution is exactly 0.0 in the reference's arithmetic dropped,
+        cxg_plan_use_reference_pattern) or back to the topological one."""
+        _lib.check(self.lib.cxg_plan_use_reference_pattern(self.h, int(bool(enable))))
+        info = _lib.CxgPlanInfo()
+        _lib.check(self.lib.cxg_plan_get_info(self.h, C.byref(info)))
+        self.info = info
+        self.nnz = int(info.nnz)
+        self._pattern = None
+
     def windows(self, tangent=False):
         """(windows, elements held by the element buffers) of the last assembly of the
         current precision in this mode."""

@@ -14,7 +14,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libcxg.so")
-SOURCES = ["cxg_api.cu", "cxg_kernels.cu", "cxg_pattern.cu", "cxg_v2.cu", "cxg_solve.cu", "cxg_batch.cu", "cxg_recover.cu"]
+SOURCES = ["cxg_api.cu", "cxg_kernels.cu", "cxg_pattern.cu", "cxg_v2.cu", "cxg_solve.cu", "cxg_batch.cu", "cxg_recover.cu",
+           "cxg_refpattern.cu"]
+# Per-file flags: the reference-pattern mask evaluates K_e in the reference's own FP64
+# operation order, so it must not contract multiply-adds.
+EXTRA_FLAGS = {"cxg_refpattern.cu": ["-fmad=false"]}
 HEADERS = ["cxg_internal.cuh", "cxg_elements.hpp", "cxg_plan.hpp", os.path.join("..", "..", "include", "cxg.h")]
 
 NVCC_FLAGS = [
@@ -47,7 +51,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     objs, procs = [], []
     for src in srcs:  # the translation units compile in parallel
         obj = os.path.join(OUT_DIR, os.path.basename(src).replace(".cu", ".o"))
-        cmd = [_nvcc(), *NVCC_FLAGS, "-dc", src, "-o", obj]
+        cmd = [_nvcc(), *NVCC_FLAGS, *EXTRA_FLAGS.get(os.path.basename(src), []), "-dc", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((cmd, subprocess.Popen(cmd)))

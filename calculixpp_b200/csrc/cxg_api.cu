@@ -162,6 +162,18 @@ int plan_status(cxg_plan* p, int64_t* bad) {
 
 namespace {
 
+// The CSR the plan's linear assembly returns: the reference's pattern when the plan uses
+// it (cxg_plan_use_reference_pattern), the topological one otherwise.
+int64_t active_nnz(const cxg_plan* p) { return p->refpat.on ? p->refpat.nnz : p->pat.nnz; }
+const int64_t* active_row_ptr(const cxg_plan* p) { return p->refpat.on ? p->refpat.row_ptr : p->pat.row_ptr; }
+const int32_t* active_col_idx(const cxg_plan* p) { return p->refpat.on ? p->refpat.col_idx : p->pat.col_idx; }
+
+int reject_refpat(const cxg_plan* p) {
+  return p->refpat.on ? set_err(CXG_ERR_UNSUPPORTED,
+                                "the reference pattern covers the linear assembly; switch it off for this operator")
+                      : CXG_OK;
+}
+
 // History components an assembly must carry (see cxg_plan::back_stress_zero).
 int state_comps(const cxg_plan* p) { return (p->back_stress_zero && !p->kinematic) ? 7 : kStateDoubles; }
 
@@ -471,6 +483,9 @@ int cxg_plan_destroy(cxg_plan* p) {
   for (void* b : bufs) cudaFree(b);
   for (auto& row : p->sched)
     for (WinSched& w : row) cudaFree(w.node_order);
+  for (void* b : {static_cast<void*>(p->refpat.row_ptr), static_cast<void*>(p->refpat.col_idx),
+                  static_cast<void*>(p->refpat.src), static_cast<void*>(p->refpat.topo_vals)})
+    cudaFree(b);
   for (void* b : p->stage) cudaFree(b);
   delete p;
   return CXG_OK;
@@ -482,7 +497,7 @@ int cxg_plan_get_info(const cxg_plan* p, cxg_plan_info* info) {
   info->n_elems = p->n_elems;
   info->elem_type = p->type;
   info->n_free = p->n_free;
-  info->nnz = p->pat.nnz;
+  info->nnz = active_nnz(p);
   info->n_gauss_points = p->n_gauss;
   info->precision = p->precision;
   info->device = p->device;
@@ -500,29 +515,33 @@ int cxg_plan_set_precision(cxg_plan* p, int32_t precision) {
 int cxg_plan_get_pattern(const cxg_plan* p, int64_t* row_ptr, int32_t* col_idx) {
   if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
   if (row_ptr)
-    CHECK_CUDA(cudaMemcpy(row_ptr, p->pat.row_ptr, sizeof(int64_t) * (static_cast<size_t>(p->n_free) + 1),
+    CHECK_CUDA(cudaMemcpy(row_ptr, active_row_ptr(p), sizeof(int64_t) * (static_cast<size_t>(p->n_free) + 1),
                           cudaMemcpyDefault), "row_ptr copy");
   if (col_idx)
-    CHECK_CUDA(cudaMemcpy(col_idx, p->pat.col_idx, sizeof(int32_t) * static_cast<size_t>(p->pat.nnz),
+    CHECK_CUDA(cudaMemcpy(col_idx, active_col_idx(p), sizeof(int32_t) * static_cast<size_t>(active_nnz(p)),
                           cudaMemcpyDefault), "col_idx copy");
   return CXG_OK;
 }
 
 int cxg_plan_pattern_device(const cxg_plan* p, const int64_t** row_ptr, const int32_t** col_idx) {
   if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
-  if (row_ptr) *row_ptr = p->pat.row_ptr;
-  if (col_idx) *col_idx = p->pat.col_idx;
+  if (row_ptr) *row_ptr = active_row_ptr(p);
+  if (col_idx) *col_idx = active_col_idx(p);
   return CXG_OK;
 }
 
 int cxg_plan_update_coords(cxg_plan* p, const double* coords) {
   if (!p || !coords) return set_err(CXG_ERR_INVALID_ARGUMENT, "null argument");
+  if (int rc = reject_refpat(p)) return rc;
   CHECK_CUDA(cudaMemcpy(p->coords, coords, sizeof(double) * 3 * static_cast<size_t>(p->n_nodes), cudaMemcpyDefault),
              "coords update");
   return CXG_OK;
 }
 
 int cxg_plan_update_young(cxg_plan* p, const double* young) {
+  if (p) {
+    if (int rc = reject_refpat(p)) return rc;
+  }
   if (!p || !young) return set_err(CXG_ERR_INVALID_ARGUMENT, "null argument");
   CHECK_CUDA(cudaMemcpy(p->young, young, sizeof(double) * static_cast<size_t>(p->n_elems), cudaMemcpyDefault),
              "young update");
@@ -550,6 +569,59 @@ int cxg_plan_set_ring_bytes(cxg_plan* p, int64_t bytes) {
   return CXG_OK;
 }
 
+int cxg_plan_use_reference_pattern(cxg_plan* p, int32_t enable) {
+  if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
+  if (p->thermal) return set_err(CXG_ERR_UNSUPPORTED, "the reference pattern covers the structural linear assembly");
+  if (p->last_stream) CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");
+  RefPattern& r = p->refpat;
+  if (!enable || r.on) {
+    if (!enable && r.on) {
+      for (void* b : {static_cast<void*>(r.row_ptr), static_cast<void*>(r.col_idx), static_cast<void*>(r.src),
+                      static_cast<void*>(r.topo_vals)})
+        cudaFree(b);
+      p->device_bytes -= static_cast<int64_t>(8 * (p->n_free + 1) + 12 * r.nnz + 8 * p->pat.nnz);
+      r = RefPattern{};
+    }
+    return CXG_OK;
+  }
+  cudaStream_t s = nullptr;
+  CHECK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+  double *flags = nullptr, *counts = nullptr;
+  RefPattern nr;
+  cudaError_t e = cudaMalloc(&flags, std::max<size_t>(v2_edata_bytes(p->type, p->n_elems, CXG_FP64), 16));
+  if (e == cudaSuccess) e = cudaMalloc(&counts, sizeof(double) * static_cast<size_t>(std::max<int64_t>(p->pat.nnz, 1)));
+  ElemArgs a = base_args(p);
+  // 1.0 / 0.0 per element-matrix entry: nonzero in the reference's arithmetic or not
+  if (e == cudaSuccess) e = launch_refmask(p->type, a, flags, s);
+  // the FP64 row gather counts, per CSR entry, the elements contributing a nonzero value
+  a.vals = counts;
+  a.rhs = nullptr;
+  V2Args v = v2_args(p, nullptr, false);
+  v.edata = flags;
+  LaunchCfg gather_only;
+  gather_only.passes = 2;
+  if (e == cudaSuccess) e = launch_v2(p->type, MODE_LINEAR, CXG_FP64, a, v, s, gather_only);
+  if (e == cudaSuccess)
+    e = compact_pattern(p->pat.row_ptr, p->pat.col_idx, p->n_free, p->pat.nnz, counts, &nr.row_ptr, &nr.col_idx,
+                        &nr.src, &nr.nnz, s);
+  if (e == cudaSuccess)
+    e = cudaMalloc(&nr.topo_vals, sizeof(double) * static_cast<size_t>(std::max<int64_t>(p->pat.nnz, 1)));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(flags);
+  cudaFree(counts);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) {
+    for (void* b : {static_cast<void*>(nr.row_ptr), static_cast<void*>(nr.col_idx), static_cast<void*>(nr.src),
+                    static_cast<void*>(nr.topo_vals)})
+      cudaFree(b);
+    return cuda_err(e, "reference pattern");
+  }
+  nr.on = true;
+  r = nr;
+  p->device_bytes += static_cast<int64_t>(8 * (p->n_free + 1) + 12 * r.nnz + 8 * p->pat.nnz);
+  return CXG_OK;
+}
+
 int cxg_plan_get_windows(const cxg_plan* p, int32_t mode, int32_t* n_windows, int64_t* ring_elems) {
   if (!p || (mode != 0 && mode != 1) || !n_windows || !ring_elems)
     return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");
@@ -572,9 +644,11 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
                            void* stream) {
   if (!p || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan and vals are required");
   const bool accumulate = (flags & CXG_ACCUMULATE) != 0;
+  if (accumulate && p->refpat.on)
+    return set_err(CXG_ERR_UNSUPPORTED, "CXG_ACCUMULATE works on the topological pattern only");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
-  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
+  const size_t vb = sizeof(double) * static_cast<size_t>(active_nnz(p));
   const size_t rb = sizeof(double) * static_cast<size_t>(p->n_free);
   const size_t fb = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
   void *dv, *dr, *df = nullptr;
@@ -584,11 +658,16 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
   if (rc) return rc;
   if ((rc = ensure_v2(p, false))) return rc;
   ElemArgs a = base_args(p);
-  a.vals = static_cast<double*>(dv);
+  // with the reference's pattern, the assembly runs on the topological pattern and the
+  // kept entries are gathered into the caller's values
+  a.vals = p->refpat.on ? p->refpat.topo_vals : static_cast<double*>(dv);
   a.rhs = static_cast<double*>(dr);
   V2Args v = v2_args(p, static_cast<const double*>(df), accumulate);
   apply_windows(p, false, v);
   CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, p->precision, a, v, s, p->cfg[p->precision]), "assembly kernels");
+  if (p->refpat.on)
+    CHECK_CUDA(gather_values(p->refpat.src, p->refpat.topo_vals, p->refpat.nnz, static_cast<double*>(dv), s),
+               "reference pattern");
   if ((rc = copy_out(vals, dv, vb, s))) return rc;
   if ((rc = copy_out(rhs, dr, rb, s))) return rc;
   if (dv != vals || (rhs && dr != rhs)) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
@@ -598,6 +677,7 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
 int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_int, double* rhs,
                          const double* f_ext, void* stream) {
   if (!p || !u || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, u and vals are required");
+  if (int rc0 = reject_refpat(p)) return rc0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
   int rc = ensure_state(p, s);
@@ -637,6 +717,7 @@ namespace {
 // and the FP64 row gather; the rhs side effect of prescribed columns is discarded, as
 // in the reference (src/fem/assembly.cpp:286-288, 320-322).
 int assemble_scalar(cxg_plan* p, int kind, const double* input, size_t input_bytes, double* vals, void* stream) {
+  if (int rc0 = reject_refpat(p)) return rc0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
   const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
@@ -1042,14 +1123,14 @@ int cxg_spmv(cxg_plan* p, const double* vals, const double* x, double* y, void* 
   if (!p || !vals || !x || !y) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, vals, x, y are required");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
-  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
+  const size_t vb = sizeof(double) * static_cast<size_t>(active_nnz(p));
   const size_t nb = sizeof(double) * static_cast<size_t>(p->n_free);
   void *dv, *dx, *dy;
   int rc = staged(p, 0, vals, vb, true, s, &dv);
   if (!rc) rc = staged(p, 2, x, nb, true, s, &dx);
   if (!rc) rc = staged(p, 1, y, nb, false, s, &dy);
   if (rc) return rc;
-  CHECK_CUDA(launch_spmv(p->n_free, p->pat.row_ptr, p->pat.col_idx, static_cast<const double*>(dv),
+  CHECK_CUDA(launch_spmv(p->n_free, active_row_ptr(p), active_col_idx(p), static_cast<const double*>(dv),
                          static_cast<const double*>(dx), static_cast<double*>(dy), s), "spmv");
   if ((rc = copy_out(y, dy, nb, s))) return rc;
   if (dy != y) CHECK_CUDA(cudaStreamSynchronize(s), "sync");
@@ -1061,7 +1142,7 @@ int cxg_solve_cg(cxg_plan* p, const double* vals, const double* rhs, double* x, 
   if (!p || !vals || !rhs || !x || max_iter < 0) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
-  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
+  const size_t vb = sizeof(double) * static_cast<size_t>(active_nnz(p));
   const size_t nb = sizeof(double) * static_cast<size_t>(p->n_free);
   void *dv, *db, *dx;
   int rc = staged(p, 0, vals, vb, true, s, &dv);
@@ -1078,7 +1159,7 @@ int cxg_solve_cg(cxg_plan* p, const double* vals, const double* rhs, double* x, 
   }
   int it = 0;
   double rel = 0.0;
-  CHECK_CUDA(cg_solve(p->n_free, p->pat.row_ptr, p->pat.col_idx, static_cast<const double*>(dv),
+  CHECK_CUDA(cg_solve(p->n_free, active_row_ptr(p), active_col_idx(p), static_cast<const double*>(dv),
                       static_cast<const double*>(db), static_cast<double*>(dx), rtol, max_iter,
                       static_cast<double*>(p->stage[5]), &it, &rel, s), "cg");
   if ((rc = copy_out(x, dx, nb, s))) return rc;

@@ -143,6 +143,17 @@ cudaError_t launch_scalar_pass(int elem_type, int kind, const ElemArgs& a, const
 cudaError_t launch_v2(int elem_type, int mode, int precision, const ElemArgs& a, const V2Args& v, cudaStream_t s,
                       const LaunchCfg& cfg = LaunchCfg{});
 
+// The reference's own pattern (cxg_refpattern.cu): launch_refmask writes, per element and
+// in the FP64 element-buffer layout, 1.0 where the reference's K_e (its operation order)
+// is nonzero and 0.0 where it is exactly zero; compact_pattern keeps the CSR entries whose
+// gathered count is positive (row_ptr_c, col_idx_c, and src = their topological index);
+// gather_values copies a topological assembly onto the kept entries.
+cudaError_t launch_refmask(int elem_type, const ElemArgs& a, double* out, cudaStream_t s);
+cudaError_t compact_pattern(const int64_t* row_ptr, const int32_t* col_idx, int32_t n_rows, int64_t nnz,
+                            const double* counts, int64_t** row_ptr_c, int32_t** col_idx_c, int64_t** src,
+                            int64_t* nnz_c, cudaStream_t s);
+cudaError_t gather_values(const int64_t* src, const double* topo, int64_t nnz_c, double* out, cudaStream_t s);
+
 // Launchers (cxg_kernels.cu). `precision` 0 = FP64, 1 = mixed.
 cudaError_t launch_element_kernel(int elem_type, int mode, bool dense, int precision,
                                   const ElemArgs& a, cudaStream_t s);

@@ -25,6 +25,20 @@ struct WinSched {
 };
 }  // namespace cxg
 
+namespace cxg {
+// The reference's own sparsity pattern (cxg_plan_use_reference_pattern): the entries of
+// the topological pattern with at least one nonzero element contribution in the
+// reference's arithmetic, and where each sits in the topological pattern.
+struct RefPattern {
+  bool on = false;
+  int64_t nnz = 0;
+  int64_t* row_ptr = nullptr;   // [n_free + 1]
+  int32_t* col_idx = nullptr;   // [nnz]
+  int64_t* src = nullptr;       // [nnz] index of the entry in the topological pattern
+  double* topo_vals = nullptr;  // [pat.nnz] one assembly on the topological pattern
+};
+}  // namespace cxg
+
 struct cxg_plan {
   int device = 0;
   int64_t n_nodes = 0, n_elems = 0, n_gauss = 0;
@@ -54,6 +68,7 @@ struct cxg_plan {
   cxg::WinSched sched[2][2];  // [precision][tangent]
   int64_t ring_bytes = 0;     // element-buffer budget: 0 default share of L2, < 0 one window
   std::vector<int32_t> node_first, node_last;  // first / last incident element per node
+  cxg::RefPattern refpat;
   cudaStream_t last_stream = nullptr;
   int64_t device_bytes = 0;
   // staging buffers for host pointers, grown on demand and reused

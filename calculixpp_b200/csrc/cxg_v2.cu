@@ -87,7 +87,7 @@ __host__ __device__ constexpr int blk_stride() { return sizeof(R) == 8 ? 10 : 12
 // the assembly runs as one window). Element indices fit 31 bits (incidence codes are
 // e*n + local index in int32), so the modulo is 32-bit.
 __device__ __forceinline__ int64_t ring_slot(int64_t e, int64_t ring) {
-  return static_cast<int64_t>(static_cast<uint32_t>(e) % static_cast<uint32_t>(ring));
+  return e < ring ? e : static_cast<int64_t>(static_cast<uint32_t>(e) % static_cast<uint32_t>(ring));
 }
 
 template <typename R>
@@ -778,133 +778,150 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 }
 
 // ---- P2: row gather ------------------------------------------------------------------
-// One warp per node a. It walks the node's incident elements in element order; for each
-// it reads row a of the element's upper-block buffer value by value: the 9n values of
-// the row (n column blocks of 9) are spread over the lanes in memory order, so a warp's
-// load covers consecutive values (the blocks (a, b >= a) are one contiguous run, each
-// block (b < a, a) a contiguous 9-value piece read transposed) instead of every lane
-// fetching a whole block of its own. Each value is added into the node's rows held in
-// shared memory (one copy per warp; within one element every target is distinct, so
-// plain adds, no atomics), so every CSR value is the sum of its contributions in
-// element order, as in the reference's scatter (src/fem/assembly.cpp:76-100).
-// Prescribed columns go into the rhs (-K_fc u_c, src/fem/assembly.cpp:95-96), the load
-// vector and the internal forces are added, and the rows are stored once with
-// coalesced writes. The node's row length L is padded to L' = 3 (mod 16) doubles in
-// the buffer, so the 3 rows x 3 components of one block fall into distinct banks.
-// The incident-element codes come in with one coalesced load per 32 elements and are
-// handed out by shuffles; the column masks and slots of the element's nodes are loaded
-// once per element by lanes 0..n-1 and shuffled to the lanes that use them.
-// In mixed precision the diagonal 3x3 block of node a is minus the FP64 sum of all
-// off-diagonal FP32 blocks of its element rows: every lane keeps running sums of the
-// values it adds (one per iteration and orientation, so the target component is fixed
-// per lane), and nine butterflies over the warp form the block, so rigid translations
-// stay in the null space of the assembled rows to FP64 accuracy.
-template <int ET>
+// One warp per node a. Lanes form EG groups of GS lanes (GS = 16 for elements of at
+// most 16 nodes, else 32; 8 for the <= 8-node families in mixed precision); lane lb of
+// group s handles column node lb of incident element k + s, so EG elements are applied
+// per pass. Every group copy of the rows is zeroed and read once per node, which for the
+// short rows of the <= 8-node families in FP64 costs more shared-memory traffic than
+// the idle lanes of two 16-lane groups (measured: the FP64 C3D8 tangent gather is 10 %
+// faster with two groups than with four, the mixed one 3 % slower, so it keeps four).
+// Each group adds into its own copy of the node's rows
+// in shared memory (within one element every target is distinct, so plain adds, no
+// atomics); the copies are summed in a fixed order when the rows are stored. The
+// node's incident-element codes come in with one coalesced load per 32 elements and
+// are handed out by shuffles; the free-component mask of each column node comes from
+// the per-element-node mask array, so a pass waits for one round of independent loads.
+// The connectivity is read only for constrained columns. In mixed precision the
+// diagonal 3x3 block of node a is minus the FP64 sum of all off-diagonal FP32 blocks of
+// its element rows: every lane keeps a running sum of the blocks it adds, and one
+// butterfly over the warp per node forms the block, so rigid translations stay in the
+// null space of the assembled rows to FP64 accuracy.
+template <int ET, bool DIAGFIX>
 struct P2Geo {
   static constexpr int n = nodes_of(ET);
-  static constexpr int NB = n * (n + 1) / 2;
-  static constexpr int NV = 9 * n;              // values of one element row
-  static constexpr int IT = (NV + 31) / 32;     // lane iterations per element row
+  static constexpr int GS = (DIAGFIX && n <= 8) ? 8 : (n <= 16 ? 16 : 32);
+  static constexpr int EG = 32 / GS;
 };
 
-// start of block row x in the upper-block numbering: blk_index(n, x, b) = row0(x) + b
-__host__ __device__ constexpr int blk_row0(int n, int x) { return x * n - x * (x - 1) / 2 - x; }
 
 template <typename R>
-__device__ __forceinline__ double ld_val(const R* p) {
-  return static_cast<double>(__ldg(p));
+struct P2Pass {
+  double v[9];
+  int64_t e;
+  int la, mb, slotv;
+  bool active;
+};
+
+template <int ET, typename R>
+__device__ __forceinline__ void p2_fetch(const ElemArgs& A, const R* ed, int64_t ring, int code, bool active, int lb,
+                                         P2Pass<R>& p) {
+  constexpr int n = nodes_of(ET), NB = n * (n + 1) / 2;
+  p.active = active;
+  p.e = code / n;
+  p.la = code % n;
+  if (active) {
+    p.mb = __ldg(A.conn_mask + p.e * n + lb);
+    p.slotv = __ldg(A.slot + (p.e * n + p.la) * n + lb);
+    const bool tr = lb < p.la;
+    double raw[9];
+    load_block<R>(ed + ring_slot(p.e, ring) * (NB * blk_stride<R>()) +
+                      (tr ? blk_index(n, lb, p.la) : blk_index(n, p.la, lb)) * blk_stride<R>(),
+                  raw);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p.v[q] = tr ? raw[3 * (q % 3) + q / 3] : raw[q];
+  } else {
+    p.mb = 0;
+    p.slotv = 0;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p.v[q] = 0.0;
+  }
 }
 
 template <int ET, bool TAN, typename R, bool DIAGFIX>
 __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
-  using PG = P2Geo<ET>;
-  constexpr int n = PG::n, NB = PG::NB, NV = PG::NV, IT = PG::IT;
-  constexpr int BS = blk_stride<R>();
+  constexpr int n = nodes_of(ET);
+  constexpr int GS = P2Geo<ET, DIAGFIX>::GS, EG = P2Geo<ET, DIAGFIX>::EG;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int stride = static_cast<int>(V.row_stride);  // shared-memory offsets are 32-bit
-  double* buf = reinterpret_cast<double*>(smem) + warp * stride;
+  double* buf = reinterpret_cast<double*>(smem) + warp * (EG * stride);
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   const R* ed = reinterpret_cast<const R*>(V.edata);
-  // per-lane constants of every iteration: column node lb, position p in the block
-  int lbv[IT], pv[IT], r0v[IT];
-#pragma unroll
-  for (int it = 0; it < IT; ++it) {
-    const int v = lane + 32 * it;
-    lbv[it] = v < NV ? v / 9 : -1;
-    pv[it] = v % 9;
-    r0v[it] = v < NV ? blk_row0(n, v / 9) : 0;
-  }
+  const int sub = lane / GS, lb = lane % GS;
+  const bool lane_ok = lb < n;
+  double* mine = buf + sub * stride;
   // nodes [V.n_begin, V.n_end) of this window's node list (node_order), or of the mesh
   for (int64_t idx = V.n_begin + gwarp; idx < V.n_end; idx += nwarps) {
     const int64_t a = V.node_order ? static_cast<int64_t>(V.node_order[idx]) : idx;
     const int ma = A.node_mask[a];
     const int nf = __popc(ma);
     const int L = static_cast<int>(A.node_rowlen[a]);
-    const int Lp = L + ((3 - L) % 16 + 16) % 16;  // L' = 3 (mod 16)
+    const int total = nf * L;
     double* vout = A.vals + A.node_base[a];
     const int64_t i0 = V.inc_ptr[a], i1 = V.inc_ptr[a + 1];
+    // offset of row i (free component i of node a) in the row buffer
     int row_off[3];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) row_off[i] = __popc(ma & ((1 << i) - 1)) * Lp;
-    for (int t = lane; t < nf * Lp; t += 32) buf[t] = 0.0;
+    for (int i = 0; i < 3; ++i) row_off[i] = __popc(ma & ((1 << i) - 1)) * L;
+    for (int g = 0; g < EG; ++g)
+      for (int t = lane; t < total; t += 32) buf[g * stride + t] = (g == 0 && V.accumulate) ? vout[t] : 0.0;
     __syncwarp();
     double rr[3] = {0.0, 0.0, 0.0};
-    double fsum = 0.0;  // lanes 0..2: component `lane` of the node's internal force
-    double dU[IT], dL[IT];  // DIAGFIX running sums of the upper / transposed values
+    double fs[3] = {0.0, 0.0, 0.0};
+    double dsum[9];  // this lane's FP64 sum of the off-diagonal blocks it added (DIAGFIX)
 #pragma unroll
-    for (int it = 0; it < IT; ++it) dU[it] = dL[it] = 0.0;
+    for (int q = 0; q < 9; ++q) dsum[q] = 0.0;
     int slot_aa = 0;  // column offset of node a in its own rows
     for (int64_t c0 = i0; c0 < i1; c0 += 32) {
       const int cnt = static_cast<int>(i1 - c0 < 32 ? i1 - c0 : 32);
       const int code_l = lane < cnt ? __ldg(V.inc_code + c0 + lane) : 0;
-      for (int k = 0; k < cnt; ++k) {
-        const int code = __shfl_sync(0xffffffffu, code_l, k);
-        const int64_t e = code / n;
-        const int la = code % n;
-        // column masks and slots of the element's nodes, one lane per node
-        int mb_l = 0, sl_l = 0;
-        if (lane < n) {
-          mb_l = __ldg(A.conn_mask + e * n + lane);
-          sl_l = __ldg(A.slot + (e * n + la) * n + lane);
-        }
-        const int64_t es = ring_slot(e, V.ring);
-        const R* eb = ed + es * (NB * BS);
-        const int r0a = blk_row0(n, la);
+      for (int k = 0; k < cnt; k += EG) {
+        P2Pass<R> cur;
+        p2_fetch<ET, R>(A, ed, V.ring, __shfl_sync(0xffffffffu, code_l, (k + sub) & 31), lane_ok && k + sub < cnt, lb,
+                        cur);
+        if (cur.active && (!DIAGFIX || lb != cur.la)) {
+          double* col = mine + cur.slotv;
+          if (cur.mb == 7) {  // every component of the column node is free
 #pragma unroll
-        for (int it = 0; it < IT; ++it) {
-          const int lb = lbv[it];
-          const int mb = __shfl_sync(0xffffffffu, mb_l, lb < 0 ? 0 : lb);
-          const int sl = __shfl_sync(0xffffffffu, sl_l, lb < 0 ? 0 : lb);
-          if (lb < 0) continue;
-          const bool up = lb >= la;
-          const int p = pv[it];
-          const int blk = up ? r0a + lb : r0v[it] + la;
-          const double x = ld_val<R>(eb + blk * BS + p);
-          const int i = up ? p / 3 : p % 3;
-          const int j = up ? p % 3 : p / 3;
-          if (DIAGFIX) {
-            if (lb == la) {
-              slot_aa = sl;
-              continue;
+            for (int i = 0; i < 3; ++i) {
+              if ((ma >> i) & 1) {
+                double* r = col + row_off[i];
+                r[0] += cur.v[3 * i];
+                r[1] += cur.v[3 * i + 1];
+                r[2] += cur.v[3 * i + 2];
+              }
             }
-            if (up) dU[it] += x; else dL[it] += x;
-          }
-          if (!((ma >> i) & 1)) continue;
-          if ((mb >> j) & 1) {
-            const int ro = i == 0 ? row_off[0] : (i == 1 ? row_off[1] : row_off[2]);
-            buf[ro + sl + __popc(mb & ((1 << j) - 1))] += x;
           } else {
-            const double pvl = A.prescribed[3 * static_cast<int64_t>(A.conn[e * n + lb]) + j];
-            if (pvl != 0.0) {
-              if (i == 0) rr[0] -= x * pvl;
-              else if (i == 1) rr[1] -= x * pvl;
-              else rr[2] -= x * pvl;
+            int64_t nb = -1;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+              if (!((ma >> i) & 1)) continue;
+#pragma unroll
+              for (int j = 0; j < 3; ++j) {
+                if ((cur.mb >> j) & 1) {
+                  col[row_off[i] + __popc(cur.mb & ((1 << j) - 1))] += cur.v[3 * i + j];
+                } else {
+                  if (nb < 0) nb = A.conn[cur.e * n + lb];
+                  const double pv = A.prescribed[3 * nb + j];
+                  if (pv != 0.0) rr[i] -= cur.v[3 * i + j] * pv;
+                }
+              }
             }
           }
         }
-        if (TAN && lane < 3) fsum += __ldg(V.fdata + es * (3 * n) + 3 * la + lane);
+        if (TAN && cur.active && lb == cur.la) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) fs[d] += __ldg(V.fdata + ring_slot(cur.e, V.ring) * (3 * n) + 3 * cur.la + d);
+        }
+        if (DIAGFIX && cur.active) {
+          if (lb != cur.la) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) dsum[q] += cur.v[q];
+          } else {
+            slot_aa = cur.slotv;  // slot(la, la)
+          }
+        }
         __syncwarp();
       }
     }
@@ -914,13 +931,7 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
       double d9[9];
 #pragma unroll
       for (int q = 0; q < 9; ++q) {
-        double x = 0.0;
-#pragma unroll
-        for (int it = 0; it < IT; ++it) {
-          const int p = pv[it];
-          if (p == q) x += dU[it];
-          if ((p % 3) * 3 + p / 3 == q) x += dL[it];
-        }
+        double x = dsum[q];
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
         d9[q] = -x;
@@ -937,12 +948,8 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
             const int ro = i == 0 ? row_off[0] : (i == 1 ? row_off[1] : row_off[2]);
             buf[ro + slot_aa + __popc(ma & ((1 << j) - 1))] += d;
           } else {
-            const double pvl = A.prescribed[3 * a + j];
-            if (pvl != 0.0) {
-              if (i == 0) rr[0] -= d * pvl;
-              else if (i == 1) rr[1] -= d * pvl;
-              else rr[2] -= d * pvl;
-            }
+            const double pv = A.prescribed[3 * a + j];
+            if (pv != 0.0) rr[i] -= d * pv;
           }
         }
       }
@@ -960,19 +967,34 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
         }
       }
     }
-    if (TAN && A.f_int && lane < 3) A.f_int[3 * a + lane] = (V.accumulate ? A.f_int[3 * a + lane] : 0.0) + fsum;
-    for (int r = 0; r < nf; ++r) {
-      const double* src = buf + r * Lp;
-      double* dst = vout + static_cast<int64_t>(r) * L;
-      for (int t = lane; t < L; t += 32) dst[t] = V.accumulate ? dst[t] + src[t] : src[t];
+    if (TAN && A.f_int) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double v = fs[d];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) A.f_int[3 * a + d] = (V.accumulate ? A.f_int[3 * a + d] : 0.0) + v;
+      }
+    }
+    for (int t = lane; t < total; t += 32) {
+      double v = buf[t];
+#pragma unroll
+      for (int g = 1; g < EG; ++g) v += buf[g * stride + t];
+      vout[t] = v;
     }
     __syncwarp();
   }
 }
 
-// Blocks of at most 8 warps.
+// Blocks of at most 8 warps. The mixed-precision gather of the <= 8-node families is
+// compiled for 3 resident blocks per SM (<= 85 registers), which its short rows leave
+// room for in shared memory; the other gathers are compiled without a register budget.
 template <int ET, bool TAN, typename R, bool DIAGFIX>
-__global__ void __launch_bounds__(256) p2_kernel(ElemArgs A, V2Args V) {
+__global__ void p2_kernel(ElemArgs A, V2Args V) {
+  p2_body<ET, TAN, R, DIAGFIX>(A, V);
+}
+
+template <int ET, bool TAN, typename R, bool DIAGFIX>
+__global__ void __launch_bounds__(256, 3) p2_kernel_short(ElemArgs A, V2Args V) {
   p2_body<ET, TAN, R, DIAGFIX>(A, V);
 }
 
@@ -1023,12 +1045,11 @@ cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg
 
 template <int ET, bool TAN, typename R, bool DF>
 cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaStream_t s) {
-  auto kern = p2_kernel<ET, TAN, R, DF>;
+  auto kern = (DF && nodes_of(ET) <= 8) ? p2_kernel_short<ET, TAN, R, DF> : p2_kernel<ET, TAN, R, DF>;
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
-  // configured count when it fits). A node's nf rows padded to L' <= L + 15 take at
-  // most max_row + 45 doubles.
-  const int64_t stride = (v.max_row + 48) / 2 * 2;
-  const int64_t wbytes = stride * 8;
+  // configured count when it fits)
+  const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
+  const int64_t wbytes = P2Geo<ET, DF>::EG * stride * 8;
   int warps = cfg.p2_warps > 0 ? std::min(cfg.p2_warps, 8) : 8;
   while (warps > 1 && warps * wbytes > 160 * 1024) warps /= 2;
   const size_t smem = static_cast<size_t>(warps) * wbytes;

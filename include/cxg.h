@@ -159,6 +159,19 @@ CXG_API int cxg_plan_set_launch_config(cxg_plan* plan, int32_t mode, int32_t til
  * distance between a node's first and last element; when the budget cannot, the
  * assembly runs as one window. Results do not depend on the budget. */
 CXG_API int cxg_plan_set_ring_bytes(cxg_plan* plan, int64_t bytes);
+/* The reference's own sparsity pattern for the linear assembly. The reference's scatter
+ * skips every element contribution that is exactly 0.0 (src/fem/assembly.cpp:86-90), so
+ * an entry whose every contribution is exactly zero in its FP64 arithmetic is absent from
+ * its LinearSystem (straight, axis-aligned C3D20 / C3D20R / C3D6 elements have such
+ * entries). enable != 0: evaluates every K_e once in the reference's operation order
+ * (element.cpp:10-102, 160-462, 529-610; no multiply-add contraction), keeps the CSR
+ * entries with at least one nonzero contribution, and from then on cxg_plan_get_info,
+ * cxg_plan_get_pattern, cxg_plan_pattern_device, cxg_assemble_linear, cxg_spmv and
+ * cxg_solve_cg use that pattern (each assembly runs on the topological pattern and copies
+ * the kept entries). The values of the dropped entries are zero to rounding. While it is
+ * on, the other operators, CXG_ACCUMULATE and coordinate / modulus updates return
+ * CXG_ERR_UNSUPPORTED; enable = 0 returns to the topological pattern. */
+CXG_API int cxg_plan_use_reference_pattern(cxg_plan* plan, int32_t enable);
 /* Windows of the current precision's linear (mode 0) or tangent (mode 1) assembly and
  * the elements its buffers hold (both from the last assembly of that mode; 0 before). */
 CXG_API int cxg_plan_get_windows(const cxg_plan* plan, int32_t mode, int32_t* n_windows, int64_t* ring_elems);
