@@ -1,4 +1,4 @@
-"""Batches of independent linear-elastic models assembled together (cxg_batch_*).
+"""Batches of independent models (linear elastic or J2) assembled together (cxg_batch_*).
 
 Models are grouped by element type inside libcxg; each group is one element pass and
 one row gather over the concatenation of its models. Per model the results equal those
@@ -20,7 +20,7 @@ TILES = {0: "2x4", 1: "2x2", 2: "4x4"}
 
 
 class Batch:
-    """A cxg_batch on one GPU. `models` is a list of assembly.Model (linear elastic)."""
+    """A cxg_batch on one GPU. `models` is a list of assembly.Model."""
 
     def __init__(self, models: list[Model], precision: str = "mixed", device=None):
         self.lib = _lib.load()
@@ -144,3 +144,47 @@ class Batch:
 
     def check(self):
         _lib.check(self.lib.cxg_batch_check(self.h))
+
+    # -- material-point (J2) assembly ------------------------------------------------------
+    def displacement_vector(self, us):
+        """Batch displacement vector (batch node order) from per-model full vectors."""
+        u = np.zeros(3 * self.n_nodes)
+        for k, uk in enumerate(us):
+            o = 3 * self.info[k].node_offset
+            uk = np.asarray(uk, dtype=np.float64).reshape(-1)
+            u[o:o + uk.size] = uk
+        return u
+
+    def assemble_tangent(self, u, f_ext=None, vals=None, f_int=None, rhs=None, check=True):
+        """Consistent tangent, internal force and rhs of every model at once
+        (cxg_batch_assemble_tangent); u in batch node order (device or host array)."""
+        dev = self.device
+        if vals is None:
+            vals, rhs = self.buffers()
+        f_int = torch.empty(3 * self.n_nodes, dtype=torch.float64, device=dev) if f_int is None else f_int
+        du = _dev(u, torch.float64, dev)
+        fe = None if f_ext is None else _dev(f_ext, torch.float64, dev)
+        with torch.cuda.device(dev):
+            _lib.check(self.lib.cxg_batch_assemble_tangent(self.h, _ptr(du), _ptr(vals), _ptr(f_int), _ptr(rhs),
+                                                           _ptr(fe), _stream()))
+            if check:
+                self.check()
+        return vals, f_int, rhs
+
+    def commit(self):
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_batch_commit(self.h, _stream()))
+
+    def state(self, k, committed=True):
+        """Model k's history (Gauss points, 13)."""
+        mi = self.info[k]
+        ng = mi.n_elems * _lib.load().cxg_gauss_points_per_element(self.models[k].mesh.etype)
+        out = torch.empty(ng * 13, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_batch_get_state(self.h, k, _lib.COMMITTED if committed else _lib.TRIAL,
+                                                    _ptr(out)))
+        return out.view(ng, 13)
+
+    def f_int_slice(self, k, f_int):
+        o = 3 * self.info[k].node_offset
+        return f_int[o:o + 3 * self.models[k].mesh.n_nodes]

@@ -174,6 +174,11 @@ int reject_refpat(const cxg_plan* p) {
                       : CXG_OK;
 }
 
+}  // namespace
+
+namespace cxg {
+namespace api {
+
 // History components an assembly must carry (see cxg_plan::back_stress_zero).
 int state_comps(const cxg_plan* p) { return (p->back_stress_zero && !p->kinematic) ? 7 : kStateDoubles; }
 
@@ -188,10 +193,6 @@ int ensure_state(cxg_plan* p, cudaStream_t s) {
   return CXG_OK;
 }
 
-}  // namespace
-
-namespace cxg {
-namespace api {
 namespace windows {
 
 __global__ void node_span_kernel(const int64_t* inc_ptr, const int32_t* inc_code, int n, int64_t n_nodes,

@@ -1,4 +1,5 @@
-// Batches of independent linear-elastic models (cxg_batch_* in include/cxg.h).
+// Batches of independent models (cxg_batch_* in include/cxg.h): linear elastic, or J2
+// plastic with a batched material-point (tangent) assembly.
 //
 // Models are grouped by element type. A group is one plan over the disjoint union of
 // its models: node, element and equation numbers of model k are shifted by the totals
@@ -41,6 +42,7 @@ struct Model {
   int64_t n_nodes = 0, n_elems = 0, node0 = 0;  // node0 inside the group
   int32_t n_free = 0, row0 = 0;                  // row0 inside the group
   int64_t nnz = 0, nnz0 = 0;                     // nnz0 inside the group
+  int64_t e0 = 0;                                // first element inside the group
 };
 
 __global__ void shift_kernel(int32_t* v, int64_t n, int32_t add, int only_nonneg) {
@@ -233,8 +235,6 @@ int cxg_batch_create(int32_t n_models, const cxg_mesh_desc* meshes, const cxg_do
       return set_err(CXG_ERR_INVALID_ARGUMENT, "batch mesh needs n_nodes > 0, coords and conn");
     if (m.n_materials < 1 || !m.materials) return set_err(CXG_ERR_INVALID_ARGUMENT, "batch mesh needs >= 1 material");
     for (int32_t i = 0; i < m.n_materials; ++i) {
-      if (m.materials[i].n_plastic > 0)
-        return set_err(CXG_ERR_UNSUPPORTED, "batched assembly covers linear elastic models only");
       if (!(m.materials[i].E > 0.0) || !(m.materials[i].nu > -1.0 && m.materials[i].nu < 0.5))
         return set_err(CXG_ERR_INVALID_ARGUMENT, "material needs E > 0 and -1 < nu < 0.5");
     }
@@ -293,18 +293,32 @@ int cxg_batch_create(int32_t n_models, const cxg_mesh_desc* meshes, const cxg_do
       break;
     }
     double *coords, *young, *poisson, *pres;
-    int32_t *conn, *deq;
+    int32_t *conn, *deq, *gem;
     if (!dalloc(reinterpret_cast<void**>(&coords), 24 * N) || !dalloc(reinterpret_cast<void**>(&pres), 24 * N) ||
         !dalloc(reinterpret_cast<void**>(&deq), 12 * N) || !dalloc(reinterpret_cast<void**>(&conn), 4 * E * npe) ||
-        !dalloc(reinterpret_cast<void**>(&young), 8 * E) || !dalloc(reinterpret_cast<void**>(&poisson), 8 * E))
+        !dalloc(reinterpret_cast<void**>(&young), 8 * E) || !dalloc(reinterpret_cast<void**>(&poisson), 8 * E) ||
+        !dalloc(reinterpret_cast<void**>(&gem), 4 * E))
       break;
+    // the group's materials: every model's list in turn; elem_mat shifted by the model's
+    // offset in that list (E and nu come per element, the *PLASTIC tables from here)
+    std::vector<cxg_material> gmats;
     int* dbad = nullptr;
     if (!dalloc(reinterpret_cast<void**>(&dbad), sizeof(int))) break;
     cudaMemsetAsync(dbad, 0, sizeof(int), s);
     int64_t e_off = 0;
     for (int32_t k : g.models) {
       const cxg_mesh_desc& m = meshes[k];
-      const Model& md = b->models[static_cast<size_t>(k)];
+      Model& md = b->models[static_cast<size_t>(k)];
+      md.e0 = e_off;
+      const int32_t mat0 = static_cast<int32_t>(gmats.size());
+      gmats.insert(gmats.end(), m.materials, m.materials + m.n_materials);
+      if (md.n_elems > 0) {
+        if (m.elem_mat)
+          cudaMemcpyAsync(gem + e_off, m.elem_mat, 4 * md.n_elems, cudaMemcpyDefault, s);
+        else
+          cudaMemsetAsync(gem + e_off, 0, 4 * md.n_elems, s);
+        shift_kernel<<<grid_for(md.n_elems), 256, 0, s>>>(gem + e_off, md.n_elems, mat0, 0);
+      }
       const int64_t n3 = 3 * md.n_nodes;
       cudaMemcpyAsync(coords + 3 * md.node0, m.coords, 8 * n3, cudaMemcpyDefault, s);
       cudaMemcpyAsync(pres + 3 * md.node0, dofs[k].prescribed, 8 * n3, cudaMemcpyDefault, s);
@@ -352,8 +366,8 @@ int cxg_batch_create(int32_t n_models, const cxg_mesh_desc* meshes, const cxg_do
       rc = set_err(CXG_ERR_INVALID_ARGUMENT, "elem_mat index outside [0, n_materials)");
       break;
     }
-    cxg_material placeholder{1.0, 0.3, 0, nullptr, nullptr, 0, 0.0};  // per-element E, nu given
-    cxg_mesh_desc desc{N, E, g.type, coords, conn, young, poisson, nullptr, 1, &placeholder};
+    cxg_mesh_desc desc{N, E, g.type, coords, conn, young, poisson, gem, static_cast<int32_t>(gmats.size()),
+                       gmats.data()};
     cxg_dofmap_desc dd{deq, pres, static_cast<int32_t>(F)};
     rc = cxg_plan_create(&desc, &dd, precision, &g.plan);
     for (void* p : tmp) cudaFree(p);
@@ -635,6 +649,64 @@ int cxg_batch_set_group_config(cxg_batch* b, int32_t gi, int32_t tile, int32_t p
   c.p1_blocks_per_sm = p1;
   c.p2_warps = warps;
   return CXG_OK;
+}
+
+int cxg_batch_assemble_tangent(cxg_batch* b, const double* u, double* vals, double* f_int, double* rhs,
+                               const double* f_ext, void* stream) {
+  if (!b || !u || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "batch, u and vals are required");
+  if (!on_device(u) || !on_device(vals) || (f_int && !on_device(f_int)) || (rhs && !on_device(rhs)) ||
+      (f_ext && !on_device(f_ext)))
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "batched tangent assembly needs device buffers");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (Group& g : b->groups) {
+    cxg_plan* p = g.plan;
+    p->precision = b->precision;
+    p->last_stream = s;
+    int rc = ensure_state(p, s);
+    if (!rc) rc = ensure_v2(p, true);
+    if (rc) return rc;
+    ElemArgs a = base_args(p);
+    a.vals = vals + g.vals0;
+    a.rhs = rhs ? rhs + g.rhs0 : nullptr;
+    a.f_int = f_int ? f_int + 3 * g.node0 : nullptr;
+    a.u = u + 3 * g.node0;
+    a.state_c = p->state[0];
+    a.state_t = p->state[1];
+    a.state_comps = state_comps(p);
+    V2Args v = v2_args(p, f_ext ? f_ext + 3 * g.node0 : nullptr, false);
+    apply_windows(p, true, v);
+    CHECK_CUDA(launch_v2(p->type, MODE_TANGENT, b->precision, a, v, s, p->tcfg[b->precision]), "batch tangent");
+  }
+  return CXG_OK;
+}
+
+int cxg_batch_commit(cxg_batch* b, void* stream) {
+  if (!b) return set_err(CXG_ERR_INVALID_ARGUMENT, "null batch");
+  for (Group& g : b->groups) {
+    const int rc = cxg_state_commit(g.plan, stream);
+    if (rc) return rc;
+  }
+  return CXG_OK;
+}
+
+int cxg_batch_get_state(const cxg_batch* b, int32_t k, int32_t slot, double* out) {
+  if (!b || k < 0 || k >= static_cast<int32_t>(b->models.size()) || !out || (slot != 0 && slot != 1))
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");
+  const Model& md = b->models[static_cast<size_t>(k)];
+  cxg_plan* p = b->groups[static_cast<size_t>(md.group)].plan;
+  const size_t nq = static_cast<size_t>(gauss_of(p->type));
+  const size_t all = static_cast<size_t>(kStateDoubles) * static_cast<size_t>(p->n_gauss);
+  double* tmp = nullptr;
+  CHECK_CUDA(cudaMalloc(&tmp, std::max<size_t>(all, 1) * sizeof(double)), "state staging");
+  int rc = cxg_state_get(p, slot, tmp);
+  if (!rc) {
+    const cudaError_t e = cudaMemcpy(out, tmp + kStateDoubles * nq * static_cast<size_t>(md.e0),
+                                     sizeof(double) * kStateDoubles * nq * static_cast<size_t>(md.n_elems),
+                                     cudaMemcpyDefault);
+    if (e != cudaSuccess) rc = cuda_err(e, "state copy");
+  }
+  cudaFree(tmp);
+  return rc;
 }
 
 }  // extern "C"

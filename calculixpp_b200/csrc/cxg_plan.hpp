@@ -96,6 +96,10 @@ int ensure_v2(cxg_plan* p, bool tangent);
 // for the current precision and mode (built by ensure_v2).
 V2Args v2_args(cxg_plan* p, const double* f_ext, bool accumulate);
 void apply_windows(const cxg_plan* p, bool tangent, V2Args& v);
+// J2 history of the material-point assembly: allocated (zeroed) on first use; the number
+// of components an assembly reads and writes (7 or 13, see back_stress_zero).
+int ensure_state(cxg_plan* p, cudaStream_t s);
+int state_comps(const cxg_plan* p);
 ElemArgs base_args(cxg_plan* p);
 
 }  // namespace api

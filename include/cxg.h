@@ -302,7 +302,7 @@ CXG_API int cxg_element_tangent_force_noalloc(int32_t elem_type, int64_t n_elems
 CXG_API int cxg_adjoint_compliance(cxg_plan* plan, const double* u, double* dc_dE, double* dc_dX,
                            void* stream);
 
-/* ---- batches: many independent linear-elastic models in one launch ------------------
+/* ---- batches: many independent models (elastic or J2) per launch ---------------------
  * No counterpart in the reference, whose drivers assemble one model per call
  * (assemble_linear_static, src/fem/assembly.cpp:225-257); per model the results are
  * those of cxg_assemble_linear on that model alone. A batch groups its models by
@@ -355,6 +355,18 @@ CXG_API int cxg_batch_graph_launch(cxg_batch* batch, double* vals, double* rhs, 
                                    void* stream);
 /* Synchronise and report the first in-kernel error of any group. */
 CXG_API int cxg_batch_check(cxg_batch* batch);
+/* Material-point (J2) assembly of every model of the batch at once: per model
+ * assemble_material_tangent (src/fem/assembly.cpp:385-423) at its slice of u[3 n_nodes]
+ * (batch node order), K_ff into its vals slice, f_int[3 n_nodes] and rhs as
+ * cxg_assemble_tangent writes them; each model's history lives in the batch. Device
+ * buffers only. Per model the results equal cxg_assemble_tangent on a plan of that model. */
+CXG_API int cxg_batch_assemble_tangent(cxg_batch* batch, const double* u, double* vals, double* f_int, double* rhs,
+                                       const double* f_ext, void* stream);
+/* MaterialPoints::commit (include/calculixpp/fem/assembly.hpp:84-87) for every model. */
+CXG_API int cxg_batch_commit(cxg_batch* batch, void* stream);
+/* Model `model`'s history (committed or trial), 13 doubles per Gauss point in its element
+ * order, as cxg_state_get returns a plan's. */
+CXG_API int cxg_batch_get_state(const cxg_batch* batch, int32_t model, int32_t slot, double* out);
 /* Autotuner. For every group and the current precision it times each candidate launch
  * shape on the batch's own data with CUDA events: the element-pass node-pair tile
  * (2x4, 2x2 and, in mixed precision, 4x4), its persistent grid (blocks per SM) and

@@ -1,7 +1,8 @@
 """Batched assembly of many independent models (cxg_batch_*): every model's slice of the
 batch output equals the assembly of that model alone, bit for bit, in FP64 and mixed
 precision, whatever launch shape the groups run with, directly or as a CUDA graph;
-the autotuner's cache round-trips; plastic models are rejected."""
+the autotuner's cache round-trips; J2 models assemble their tangent in the batch with
+the same bits as alone."""
 import json
 
 import numpy as np
@@ -109,8 +110,59 @@ def test_host_buffers_and_rejections(cuda, models):
     dv, dr = b.assemble(torch.as_tensor(f, device=b.device))
     assert torch.equal(hv, dv.cpu()) and torch.equal(hr, dr.cpu())
     b.close()
-    m = models[0]
-    plastic = Model(m.mesh, [Material(2.1e5, 0.3, (np.array([0.0, 1.0]), np.array([250.0, 1250.0])))], None, m.spc)
-    with pytest.raises(CxgError) as exc:
-        Batch([models[1], plastic])
-    assert exc.value.code == 5
+    with pytest.raises(CxgError):
+        b2 = Batch(models[:2], "fp64")
+        b2.assemble_tangent(np.zeros(3 * b2.n_nodes))  # host u: device buffers only
+
+
+J2 = ([0.0, 1.0], [250.0, 1250.0])  # sigma_y 250, linear hardening H = 1000
+
+
+def plastic_models(seed=4):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k, t in enumerate([mg.C3D8, mg.C3D20R, mg.C3D6, mg.C3D8R, mg.C3D15, mg.C3D8]):
+        ne = int(rng.integers(20, 200))
+        E, nu = float(rng.uniform(7e4, 2.1e5)), float(rng.uniform(0.25, 0.35))
+        m, spc, top = mg.batch_box(t, ne, 0.1, seed * 1000 + k, E, nu)
+        mats = [Material(E, nu, J2)] if k % 2 == 0 else [Material(E, nu), Material(E, nu, J2, 2, 3000.0)]
+        em = None if k % 2 == 0 else (np.arange(m.n_elems) % 2).astype(np.int32)
+        out.append(Model(m, mats, em, spc, None))
+    return out
+
+
+def _u(model, scale):
+    x = model.mesh.coords
+    h = x[:, 2].max()
+    u = np.zeros_like(x)
+    u[:, 0] = scale * x[:, 2] * (1.0 + 0.3 * x[:, 0] / max(x[:, 0].max(), 1.0))
+    u[:, 2] = 0.4 * scale * x[:, 2] ** 2 / h
+    return u.reshape(-1)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_plastic_models_equal_single_plans(cuda, precision):
+    """J2 models of several types (isotropic and combined hardening, per-element
+    materials) in one batch: every model's tangent, internal force, rhs and history equal
+    those of a plan of that model alone, bit for bit, over two increments with commits."""
+    models = plastic_models()
+    b = Batch(models, precision)
+    plans = [Plan(m, precision) for m in models]
+    vals, rhs = b.buffers()
+    for step, scale in enumerate((0.004, 0.009)):
+        u = torch.as_tensor(b.displacement_vector([_u(m, scale) for m in models]), device=b.device)
+        vals, f_int, rhs = b.assemble_tangent(u, vals=vals, rhs=rhs)
+        for k, (model, plan) in enumerate(zip(models, plans)):
+            v1, f1, r1 = plan.assemble_tangent(_u(model, scale))
+            vk, rk = b.slices(k, vals, rhs)
+            assert torch.equal(vk, v1), (step, k)
+            assert torch.equal(rk, r1), (step, k)
+            assert torch.equal(b.f_int_slice(k, f_int), f1), (step, k)
+            assert torch.equal(b.state(k, committed=False), plan.state(committed=False)), (step, k)
+        b.commit()
+        for plan in plans:
+            plan.commit()
+    assert any(float(b.state(k)[:, 6].max()) > 0.0 for k in range(len(models)))  # yielded
+    for plan in plans:
+        plan.close()
+    b.close()
