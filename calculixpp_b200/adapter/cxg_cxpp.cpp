@@ -54,8 +54,21 @@ bool same_table(const cxpp::Plastic& a, const cxpp::Plastic& b) {
 CudaAssembler::CudaAssembler(const cxpp::Model& model, Precision precision) : model_(model) {
   const cxpp::Mesh& mesh = model.mesh;
   build_dof_map(model, base_);
-  for (bool slave : base_.transform.is_slave)
-    if (slave) unsupported("*EQUATION / multi-point constraint elimination");
+  // multi-point constraints: the slaves' expansions of the reference's own transform
+  std::vector<int64_t> slave_dof, term_ptr(1, 0);
+  std::vector<int32_t> term_eq;
+  std::vector<double> term_coeff, constant;
+  for (std::size_t g = 0; g < base_.transform.is_slave.size(); ++g) {
+    if (!base_.transform.is_slave[g]) continue;
+    const cxpp::fem::DofExpansion& ex = base_.transform.expansion[g];
+    slave_dof.push_back(static_cast<int64_t>(g));
+    for (const cxpp::fem::DofTerm& t : ex.terms) {
+      term_eq.push_back(t.eq);
+      term_coeff.push_back(t.coeff);
+    }
+    term_ptr.push_back(static_cast<int64_t>(term_eq.size()));
+    constant.push_back(ex.constant);
+  }
   if (!model.springs.empty()) unsupported("*SPRING connectors");
   for (cxpp::Real v : cxpp::fem::thermal_strain_load_vector(model))
     if (v != 0.0) unsupported("a thermal-strain load");
@@ -124,7 +137,9 @@ CudaAssembler::CudaAssembler(const cxpp::Model& model, Precision precision) : mo
                      conn.data(), young.data(), poisson.data(), elem_mat.data(), static_cast<int32_t>(mats.size()),
                      mats.data()};
   cxg_dofmap_desc dmap{dof_eq.data(), base_.prescribed.data(), base_.n_free};
-  check(cxg_plan_create(&desc, &dmap, static_cast<int32_t>(precision), &plan_));
+  const cxg_mpc_desc mpc{static_cast<int64_t>(slave_dof.size()), slave_dof.data(), term_ptr.data(), term_eq.data(),
+                         term_coeff.data(), constant.data()};
+  check(cxg_plan_create_mpc(&desc, &dmap, &mpc, static_cast<int32_t>(precision), &plan_));
   cxg_plan_info info{};
   check(cxg_plan_get_info(plan_, &info));
   row_ptr_.resize(static_cast<std::size_t>(info.n_free) + 1);

@@ -10,9 +10,10 @@
 //   numerics::solve_linear_static    include/calculixpp/numerics/linear_static.hpp
 // Supported: one element type per model (C3D4/C3D10/C3D8/C3D8R/C3D20/C3D20R/C3D6/C3D15),
 // per-element sections and materials (elastic, J2 plasticity), *BOUNDARY single-point
-// constraints, *CLOAD/*DLOAD/*GRAV loads through external_load_vector, deactivated
-// elements (*MODEL CHANGE). Anything else (several element types, *EQUATION / MPC
-// slaves, springs, thermal-strain loads, hyperelastic or user materials) throws
+// constraints, *EQUATION and the other constraints the reference expands into linear
+// equations (through its own constraint transform), *CLOAD/*DLOAD/*GRAV loads through
+// external_load_vector, deactivated elements (*MODEL CHANGE). Anything else (several
+// element types, springs, thermal-strain loads, hyperelastic or user materials) throws
 // std::runtime_error naming the feature, before any GPU work.
 #pragma once
 

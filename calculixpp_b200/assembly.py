@@ -194,7 +194,7 @@ class Plan:
 
     def set_ring_bytes(self, nbytes: int):
         """Element-buffer budget of the windowed assembly (cxg_plan_set_ring_bytes):
-        0 = default share of L2, < 0 = one window over the whole mesh."""
+        0 or < 0 = one window over the whole mesh, > 0 = windows whose buffers fit."""
         _lib.check(self.lib.cxg_plan_set_ring_bytes(self.h, int(nbytes)))
 
     def use_reference_pattern(self, enable=True):
@@ -219,8 +219,8 @@ class Plan:
         """Time `step()` (one assembly through this plan) with CUDA events for every tile
         and element-pass grid shape of the current precision, then for the row gather's
         warps per block (8, 4, 2) at the kept element-pass shape, then for the
-        element-buffer budget of the windowed assembly (default, one window, 40 % and 85 %
-        of L2); keep the fastest and return it with its time in ms."""
+        element-buffer budget of the windowed assembly (one window, 40 % and 85 % of L2);
+        keep the fastest and return it with its time in ms."""
 
         def timed(tile, bps, warps):
             try:
@@ -253,7 +253,7 @@ class Plan:
         # (results do not depend on it)
         l2 = torch.cuda.get_device_properties(self.device).L2_cache_size
         ring, ring_ms = 0, best[0]
-        for budget in (-1, int(0.4 * l2), int(0.85 * l2)):
+        for budget in (int(0.4 * l2), int(0.85 * l2)):
             self.set_ring_bytes(budget)
             ms = timed(best[1], best[2], best[3])
             if ms is not None and ms < ring_ms:

@@ -164,11 +164,39 @@ namespace {
 
 // The CSR the plan's linear assembly returns: the reference's pattern when the plan uses
 // it (cxg_plan_use_reference_pattern), the topological one otherwise.
-int64_t active_nnz(const cxg_plan* p) { return p->refpat.on ? p->refpat.nnz : p->pat.nnz; }
-const int64_t* active_row_ptr(const cxg_plan* p) { return p->refpat.on ? p->refpat.row_ptr : p->pat.row_ptr; }
-const int32_t* active_col_idx(const cxg_plan* p) { return p->refpat.on ? p->refpat.col_idx : p->pat.col_idx; }
+// A plan with multi-point constraints returns the reduced free system.
+int64_t active_nnz(const cxg_plan* p) {
+  return p->mpc.on ? p->mpc.lists.nnz : p->refpat.on ? p->refpat.nnz : p->pat.nnz;
+}
+const int64_t* active_row_ptr(const cxg_plan* p) {
+  return p->mpc.on ? p->mpc.lists.row_ptr : p->refpat.on ? p->refpat.row_ptr : p->pat.row_ptr;
+}
+const int32_t* active_col_idx(const cxg_plan* p) {
+  return p->mpc.on ? p->mpc.lists.col_idx : p->refpat.on ? p->refpat.col_idx : p->pat.col_idx;
+}
+int32_t active_n_free(const cxg_plan* p) { return p->mpc.on ? p->mpc.n_free : p->n_free; }
+
+// K_ff and rhs of a plan with multi-point constraints from its extended assembly
+// (mpc.vals_x, mpc.rhs_x): vals = T^T K_x T, rhs = T^T (rhs_x - K_x c).
+cudaError_t mpc_reduce(cxg_plan* p, double* vals, double* rhs, cudaStream_t s) {
+  const MpcPlan& m = p->mpc;
+  cudaError_t e = mpc_reduce_values(m.lists, m.vals_x, vals, s);
+  if (e != cudaSuccess || !rhs) return e;
+  if (m.c_x) {
+    e = launch_spmv(p->n_free, p->pat.row_ptr, p->pat.col_idx, m.vals_x, m.c_x, m.kc_x, s);
+    if (e != cudaSuccess) return e;
+  }
+  return mpc_reduce_rhs(m.lists, m.rhs_x, m.c_x ? m.kc_x : nullptr, p->n_free, m.tmp_x, m.n_free, rhs, s);
+}
+
+int reject_mpc(const cxg_plan* p) {
+  return p->mpc.on ? set_err(CXG_ERR_UNSUPPORTED,
+                             "plans with multi-point constraints cover the linear and tangent assembly")
+                   : CXG_OK;
+}
 
 int reject_refpat(const cxg_plan* p) {
+  if (p->mpc.on) return reject_mpc(p);
   return p->refpat.on ? set_err(CXG_ERR_UNSUPPORTED,
                                 "the reference pattern covers the linear assembly; switch it off for this operator")
                       : CXG_OK;
@@ -221,7 +249,11 @@ int build_schedule(cxg_plan* p, size_t bpe, WinSched& w) {
   w.win_e.clear();
   w.win_n.clear();
   const int64_t min_w = p->ring_bytes > 0 ? 32 : kMinWindow, grain = p->ring_bytes > 0 ? 32 : 1024;
-  if (p->ring_bytes < 0 || p->n_elems < 2 * min_w) return CXG_OK;
+  // default (0) and negative budgets: one window. Measured on the B200, windows lost at
+  // every budget tried (C3D8 J2 128^3: 11.2 ms one window, 14.2-15.6 ms windowed; C3D20
+  // 64^3 mixed: 6.9 against 7.2 ms): the two passes are not HBM-bound, and every window
+  // adds two launches and a tail. The tuner still tries L2-sized budgets.
+  if (p->ring_bytes <= 0 || p->n_elems < 2 * min_w) return CXG_OK;
   if (p->node_first.empty()) {
     int32_t* d = nullptr;
     CHECK_CUDA(cudaMalloc(&d, sizeof(int32_t) * 2 * static_cast<size_t>(p->n_nodes)), "node spans");
@@ -242,12 +274,7 @@ int build_schedule(cxg_plan* p, size_t bpe, WinSched& w) {
   int64_t span = 1;
   for (int64_t a = 0; a < p->n_nodes; ++a)
     if (p->node_last[a] >= 0) span = std::max<int64_t>(span, p->node_last[a] - p->node_first[a] + 1);
-  int64_t budget = p->ring_bytes;
-  if (budget == 0) {
-    int l2 = 0;
-    CHECK_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, p->device), "L2 size");
-    budget = static_cast<int64_t>(l2) * 5 / 8;
-  }
+  const int64_t budget = p->ring_bytes;
   const int64_t W = (budget / static_cast<int64_t>(bpe) - span) / grain * grain;
   if (W < min_w || W * 2 > p->n_elems) return CXG_OK;
   const int64_t n_win = (p->n_elems + W - 1) / W;
@@ -474,6 +501,98 @@ int cxg_plan_create(const cxg_mesh_desc* m, const cxg_dofmap_desc* d, int32_t pr
   return CXG_OK;
 }
 
+int cxg_plan_create_mpc(const cxg_mesh_desc* m, const cxg_dofmap_desc* d, const cxg_mpc_desc* mpc, int32_t precision,
+                        cxg_plan** out) {
+  if (!m || !d || !mpc || !out) return set_err(CXG_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (mpc->n_slaves < 0) return set_err(CXG_ERR_INVALID_ARGUMENT, "negative slave count");
+  if (mpc->n_slaves == 0) return cxg_plan_create(m, d, precision, out);
+  if (m->n_nodes <= 0 || !d->dof_eq || !d->prescribed || d->n_free < 0 || !mpc->slave_dof || !mpc->term_ptr)
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "bad DOF map or constraint description");
+  const int64_t ndof = 3 * m->n_nodes, ns = mpc->n_slaves;
+  // host copies (the arrays may be host or device memory)
+  std::vector<int32_t> deq(static_cast<size_t>(ndof));
+  std::vector<double> pre(static_cast<size_t>(ndof));
+  std::vector<int64_t> sdof(static_cast<size_t>(ns)), tptr(static_cast<size_t>(ns) + 1);
+  std::vector<double> cst(static_cast<size_t>(ns), 0.0);
+  CHECK_CUDA(cudaMemcpy(deq.data(), d->dof_eq, 4 * ndof, cudaMemcpyDefault), "dof_eq");
+  CHECK_CUDA(cudaMemcpy(pre.data(), d->prescribed, 8 * ndof, cudaMemcpyDefault), "prescribed");
+  CHECK_CUDA(cudaMemcpy(sdof.data(), mpc->slave_dof, 8 * ns, cudaMemcpyDefault), "slave_dof");
+  CHECK_CUDA(cudaMemcpy(tptr.data(), mpc->term_ptr, 8 * (ns + 1), cudaMemcpyDefault), "term_ptr");
+  if (mpc->constant) CHECK_CUDA(cudaMemcpy(cst.data(), mpc->constant, 8 * ns, cudaMemcpyDefault), "constant");
+  const int64_t nt = tptr[static_cast<size_t>(ns)];
+  if (tptr[0] != 0 || nt < 0 || (nt > 0 && (!mpc->term_eq || !mpc->term_coeff)))
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "term_ptr must start at 0 and the term arrays be given");
+  std::vector<int32_t> teq(static_cast<size_t>(nt));
+  std::vector<double> tco(static_cast<size_t>(nt));
+  if (nt > 0) {
+    CHECK_CUDA(cudaMemcpy(teq.data(), mpc->term_eq, 4 * nt, cudaMemcpyDefault), "term_eq");
+    CHECK_CUDA(cudaMemcpy(tco.data(), mpc->term_coeff, 8 * nt, cudaMemcpyDefault), "term_coeff");
+  }
+  for (int64_t k = 0; k < ns; ++k) {
+    const int64_t g = sdof[static_cast<size_t>(k)];
+    if (g < 0 || g >= ndof || (k > 0 && g <= sdof[static_cast<size_t>(k) - 1]) || deq[static_cast<size_t>(g)] >= 0)
+      return set_err(CXG_ERR_INVALID_ARGUMENT, "slave DOFs must be ascending, in range and not free");
+    if (tptr[static_cast<size_t>(k) + 1] < tptr[static_cast<size_t>(k)])
+      return set_err(CXG_ERR_INVALID_ARGUMENT, "term_ptr must not decrease");
+  }
+  for (int32_t e : teq)
+    if (e < 0 || e >= d->n_free) return set_err(CXG_ERR_INVALID_ARGUMENT, "constraint term outside the free equations");
+  // extended numbering: free DOFs and slaves in ascending global DOF order
+  std::vector<int32_t> xeq(static_cast<size_t>(ndof), -1), ext_map;
+  std::vector<double> cx;
+  bool any_c = false;
+  int32_t nx = 0;
+  size_t si = 0;
+  for (int64_t g = 0; g < ndof; ++g) {
+    if (si < sdof.size() && sdof[si] == g) {
+      xeq[static_cast<size_t>(g)] = nx++;
+      ext_map.push_back(-1 - static_cast<int32_t>(si));
+      cx.push_back(cst[si]);
+      any_c = any_c || cst[si] != 0.0;
+      pre[static_cast<size_t>(g)] = 0.0;
+      ++si;
+    } else if (deq[static_cast<size_t>(g)] >= 0) {
+      xeq[static_cast<size_t>(g)] = nx++;
+      ext_map.push_back(deq[static_cast<size_t>(g)]);
+      cx.push_back(0.0);
+    }
+  }
+  const cxg_dofmap_desc xd{xeq.data(), pre.data(), nx};
+  cxg_plan* p = nullptr;
+  int rc = cxg_plan_create(m, &xd, precision, &p);
+  if (rc) return rc;
+  MpcPlan& mp = p->mpc;
+  auto up = [&](void** dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMalloc(dst, std::max<size_t>(bytes, 16));
+    if (e == cudaSuccess && bytes) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    return e;
+  };
+  cudaError_t e = up(reinterpret_cast<void**>(&mp.ext_map), ext_map.data(), 4 * ext_map.size());
+  if (e == cudaSuccess) e = up(reinterpret_cast<void**>(&mp.term_ptr), tptr.data(), 8 * tptr.size());
+  if (e == cudaSuccess) e = up(reinterpret_cast<void**>(&mp.term_eq), teq.data(), 4 * teq.size());
+  if (e == cudaSuccess) e = up(reinterpret_cast<void**>(&mp.term_coeff), tco.data(), 8 * tco.size());
+  if (e == cudaSuccess && any_c) e = up(reinterpret_cast<void**>(&mp.c_x), cx.data(), 8 * cx.size());
+  if (e == cudaSuccess && any_c) e = cudaMalloc(&mp.kc_x, 8 * static_cast<size_t>(std::max(nx, 1)));
+  if (e == cudaSuccess) e = cudaMalloc(&mp.vals_x, 8 * static_cast<size_t>(std::max<int64_t>(p->pat.nnz, 1)));
+  if (e == cudaSuccess) e = cudaMalloc(&mp.rhs_x, 8 * static_cast<size_t>(std::max(nx, 1)));
+  if (e == cudaSuccess) e = cudaMalloc(&mp.tmp_x, 8 * static_cast<size_t>(std::max(nx, 1)));
+  cudaStream_t s = nullptr;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e == cudaSuccess)
+    e = build_mpc_reduce(p->pat.row_ptr, p->pat.col_idx, nx, p->pat.nnz, mp.ext_map, mp.term_ptr, mp.term_eq,
+                         mp.term_coeff, d->n_free, &mp.lists, s);
+  if (s) cudaStreamDestroy(s);
+  if (e != cudaSuccess) {
+    cxg_plan_destroy(p);
+    return cuda_err(e, "constraint reduction");
+  }
+  mp.on = true;
+  mp.n_free = d->n_free;
+  *out = p;
+  return CXG_OK;
+}
+
 int cxg_plan_destroy(cxg_plan* p) {
   if (!p) return CXG_OK;
   if (p->last_stream) cudaStreamSynchronize(p->last_stream);
@@ -487,6 +606,15 @@ int cxg_plan_destroy(cxg_plan* p) {
   for (void* b : {static_cast<void*>(p->refpat.row_ptr), static_cast<void*>(p->refpat.col_idx),
                   static_cast<void*>(p->refpat.src), static_cast<void*>(p->refpat.topo_vals)})
     cudaFree(b);
+  const MpcPlan& mp = p->mpc;
+  for (void* b : {static_cast<void*>(mp.lists.row_ptr), static_cast<void*>(mp.lists.col_idx),
+                  static_cast<void*>(mp.lists.tgt_ptr), static_cast<void*>(mp.lists.src), static_cast<void*>(mp.lists.w),
+                  static_cast<void*>(mp.lists.rhs_ptr), static_cast<void*>(mp.lists.rhs_src),
+                  static_cast<void*>(mp.lists.rhs_w), static_cast<void*>(mp.ext_map), static_cast<void*>(mp.term_ptr),
+                  static_cast<void*>(mp.term_eq), static_cast<void*>(mp.term_coeff), static_cast<void*>(mp.c_x),
+                  static_cast<void*>(mp.vals_x), static_cast<void*>(mp.rhs_x), static_cast<void*>(mp.tmp_x),
+                  static_cast<void*>(mp.kc_x)})
+    cudaFree(b);
   for (void* b : p->stage) cudaFree(b);
   delete p;
   return CXG_OK;
@@ -497,7 +625,7 @@ int cxg_plan_get_info(const cxg_plan* p, cxg_plan_info* info) {
   info->n_nodes = p->n_nodes;
   info->n_elems = p->n_elems;
   info->elem_type = p->type;
-  info->n_free = p->n_free;
+  info->n_free = active_n_free(p);
   info->nnz = active_nnz(p);
   info->n_gauss_points = p->n_gauss;
   info->precision = p->precision;
@@ -516,7 +644,7 @@ int cxg_plan_set_precision(cxg_plan* p, int32_t precision) {
 int cxg_plan_get_pattern(const cxg_plan* p, int64_t* row_ptr, int32_t* col_idx) {
   if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
   if (row_ptr)
-    CHECK_CUDA(cudaMemcpy(row_ptr, active_row_ptr(p), sizeof(int64_t) * (static_cast<size_t>(p->n_free) + 1),
+    CHECK_CUDA(cudaMemcpy(row_ptr, active_row_ptr(p), sizeof(int64_t) * (static_cast<size_t>(active_n_free(p)) + 1),
                           cudaMemcpyDefault), "row_ptr copy");
   if (col_idx)
     CHECK_CUDA(cudaMemcpy(col_idx, active_col_idx(p), sizeof(int32_t) * static_cast<size_t>(active_nnz(p)),
@@ -573,6 +701,7 @@ int cxg_plan_set_ring_bytes(cxg_plan* p, int64_t bytes) {
 int cxg_plan_use_reference_pattern(cxg_plan* p, int32_t enable) {
   if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
   if (p->thermal) return set_err(CXG_ERR_UNSUPPORTED, "the reference pattern covers the structural linear assembly");
+  if (p->mpc.on) return reject_mpc(p);
   if (p->last_stream) CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");
   RefPattern& r = p->refpat;
   if (!enable || r.on) {
@@ -645,12 +774,12 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
                            void* stream) {
   if (!p || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan and vals are required");
   const bool accumulate = (flags & CXG_ACCUMULATE) != 0;
-  if (accumulate && p->refpat.on)
+  if (accumulate && (p->refpat.on || p->mpc.on))
     return set_err(CXG_ERR_UNSUPPORTED, "CXG_ACCUMULATE works on the topological pattern only");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
   const size_t vb = sizeof(double) * static_cast<size_t>(active_nnz(p));
-  const size_t rb = sizeof(double) * static_cast<size_t>(p->n_free);
+  const size_t rb = sizeof(double) * static_cast<size_t>(active_n_free(p));
   const size_t fb = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
   void *dv, *dr, *df = nullptr;
   int rc = staged(p, 0, vals, vb, accumulate, s, &dv);
@@ -661,14 +790,15 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
   ElemArgs a = base_args(p);
   // with the reference's pattern, the assembly runs on the topological pattern and the
   // kept entries are gathered into the caller's values
-  a.vals = p->refpat.on ? p->refpat.topo_vals : static_cast<double*>(dv);
-  a.rhs = static_cast<double*>(dr);
+  a.vals = p->mpc.on ? p->mpc.vals_x : p->refpat.on ? p->refpat.topo_vals : static_cast<double*>(dv);
+  a.rhs = p->mpc.on ? p->mpc.rhs_x : static_cast<double*>(dr);
   V2Args v = v2_args(p, static_cast<const double*>(df), accumulate);
   apply_windows(p, false, v);
   CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, p->precision, a, v, s, p->cfg[p->precision]), "assembly kernels");
   if (p->refpat.on)
     CHECK_CUDA(gather_values(p->refpat.src, p->refpat.topo_vals, p->refpat.nnz, static_cast<double*>(dv), s),
                "reference pattern");
+  if (p->mpc.on) CHECK_CUDA(mpc_reduce(p, static_cast<double*>(dv), static_cast<double*>(dr), s), "constraint reduction");
   if ((rc = copy_out(vals, dv, vb, s))) return rc;
   if ((rc = copy_out(rhs, dr, rb, s))) return rc;
   if (dv != vals || (rhs && dr != rhs)) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
@@ -678,13 +808,13 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
 int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_int, double* rhs,
                          const double* f_ext, void* stream) {
   if (!p || !u || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, u and vals are required");
-  if (int rc0 = reject_refpat(p)) return rc0;
+  if (p->refpat.on) return reject_refpat(p);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
   int rc = ensure_state(p, s);
   if (rc) return rc;
-  const size_t vb = sizeof(double) * static_cast<size_t>(p->pat.nnz);
-  const size_t rb = sizeof(double) * static_cast<size_t>(p->n_free);
+  const size_t vb = sizeof(double) * static_cast<size_t>(active_nnz(p));
+  const size_t rb = sizeof(double) * static_cast<size_t>(active_n_free(p));
   const size_t fb = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
   void *dv, *dr, *df, *du, *dfi;
   rc = staged(p, 0, vals, vb, false, s, &dv);
@@ -695,8 +825,8 @@ int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_i
   if (rc) return rc;
   if ((rc = ensure_v2(p, true))) return rc;
   ElemArgs a = base_args(p);
-  a.vals = static_cast<double*>(dv);
-  a.rhs = static_cast<double*>(dr);
+  a.vals = p->mpc.on ? p->mpc.vals_x : static_cast<double*>(dv);
+  a.rhs = p->mpc.on ? p->mpc.rhs_x : static_cast<double*>(dr);
   a.f_int = static_cast<double*>(dfi);
   a.u = static_cast<const double*>(du);
   a.state_c = p->state[0];
@@ -705,6 +835,7 @@ int cxg_assemble_tangent(cxg_plan* p, const double* u, double* vals, double* f_i
   V2Args v = v2_args(p, static_cast<const double*>(df), false);
   apply_windows(p, true, v);
   CHECK_CUDA(launch_v2(p->type, MODE_TANGENT, p->precision, a, v, s, p->tcfg[p->precision]), "assembly kernels");
+  if (p->mpc.on) CHECK_CUDA(mpc_reduce(p, static_cast<double*>(dv), static_cast<double*>(dr), s), "constraint reduction");
   if ((rc = copy_out(vals, dv, vb, s))) return rc;
   if ((rc = copy_out(rhs, dr, rb, s))) return rc;
   if ((rc = copy_out(f_int, dfi, fb, s))) return rc;
@@ -1125,13 +1256,13 @@ int cxg_spmv(cxg_plan* p, const double* vals, const double* x, double* y, void* 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
   const size_t vb = sizeof(double) * static_cast<size_t>(active_nnz(p));
-  const size_t nb = sizeof(double) * static_cast<size_t>(p->n_free);
+  const size_t nb = sizeof(double) * static_cast<size_t>(active_n_free(p));
   void *dv, *dx, *dy;
   int rc = staged(p, 0, vals, vb, true, s, &dv);
   if (!rc) rc = staged(p, 2, x, nb, true, s, &dx);
   if (!rc) rc = staged(p, 1, y, nb, false, s, &dy);
   if (rc) return rc;
-  CHECK_CUDA(launch_spmv(p->n_free, active_row_ptr(p), active_col_idx(p), static_cast<const double*>(dv),
+  CHECK_CUDA(launch_spmv(active_n_free(p), active_row_ptr(p), active_col_idx(p), static_cast<const double*>(dv),
                          static_cast<const double*>(dx), static_cast<double*>(dy), s), "spmv");
   if ((rc = copy_out(y, dy, nb, s))) return rc;
   if (dy != y) CHECK_CUDA(cudaStreamSynchronize(s), "sync");
@@ -1144,13 +1275,13 @@ int cxg_solve_cg(cxg_plan* p, const double* vals, const double* rhs, double* x, 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->last_stream = s;
   const size_t vb = sizeof(double) * static_cast<size_t>(active_nnz(p));
-  const size_t nb = sizeof(double) * static_cast<size_t>(p->n_free);
+  const size_t nb = sizeof(double) * static_cast<size_t>(active_n_free(p));
   void *dv, *db, *dx;
   int rc = staged(p, 0, vals, vb, true, s, &dv);
   if (!rc) rc = staged(p, 1, rhs, nb, true, s, &db);
   if (!rc) rc = staged(p, 2, x, nb, true, s, &dx);
   if (rc) return rc;
-  const size_t wb = sizeof(double) * (5 * static_cast<size_t>(p->n_free) + 2056);
+  const size_t wb = sizeof(double) * (5 * static_cast<size_t>(active_n_free(p)) + 2056);
   if (p->stage_bytes[5] < wb) {
     cudaFree(p->stage[5]);
     p->stage[5] = nullptr;
@@ -1160,7 +1291,7 @@ int cxg_solve_cg(cxg_plan* p, const double* vals, const double* rhs, double* x, 
   }
   int it = 0;
   double rel = 0.0;
-  CHECK_CUDA(cg_solve(p->n_free, active_row_ptr(p), active_col_idx(p), static_cast<const double*>(dv),
+  CHECK_CUDA(cg_solve(active_n_free(p), active_row_ptr(p), active_col_idx(p), static_cast<const double*>(dv),
                       static_cast<const double*>(db), static_cast<double*>(dx), rtol, max_iter,
                       static_cast<double*>(p->stage[5]), &it, &rel, s), "cg");
   if ((rc = copy_out(x, dx, nb, s))) return rc;

@@ -154,6 +154,31 @@ cudaError_t compact_pattern(const int64_t* row_ptr, const int32_t* col_idx, int3
                             int64_t* nnz_c, cudaStream_t s);
 cudaError_t gather_values(const int64_t* src, const double* topo, int64_t nnz_c, double* out, cudaStream_t s);
 
+// Multi-point constraints (cxg_mpc.cu): the reduced CSR of K_ff = T^T K_x T and, per
+// reduced entry, the list of (extended entry, weight) pairs it sums (tgt_ptr / src / w);
+// per free equation, the list of (extended row, weight) pairs of T^T (rhs_ptr / rhs_src /
+// rhs_w).
+struct MpcLists {
+  int64_t nnz = 0;
+  int64_t* row_ptr = nullptr;
+  int32_t* col_idx = nullptr;
+  int64_t* tgt_ptr = nullptr;
+  int64_t* src = nullptr;
+  double* w = nullptr;
+  int64_t* rhs_ptr = nullptr;
+  int64_t* rhs_src = nullptr;
+  double* rhs_w = nullptr;
+};
+// ext_map[x]: free equation of extended equation x, or -1 - s for slave s whose terms are
+// [term_ptr[s], term_ptr[s+1]) of term_eq / term_coeff.
+cudaError_t build_mpc_reduce(const int64_t* x_row_ptr, const int32_t* x_col, int64_t n_x, int64_t nnz_x,
+                             const int32_t* ext_map, const int64_t* term_ptr, const int32_t* term_eq,
+                             const double* term_coeff, int32_t n_free, MpcLists* out, cudaStream_t s);
+cudaError_t mpc_reduce_values(const MpcLists& m, const double* vals_x, double* vals, cudaStream_t s);
+// rhs = T^T (rhs_x - kc), kc = K_x c (null when every constant is zero); tmp_x[n_x] scratch.
+cudaError_t mpc_reduce_rhs(const MpcLists& m, const double* rhs_x, const double* kc, int64_t n_x, double* tmp_x,
+                           int32_t n_free, double* rhs, cudaStream_t s);
+
 // Launchers (cxg_kernels.cu). `precision` 0 = FP64, 1 = mixed.
 cudaError_t launch_element_kernel(int elem_type, int mode, bool dense, int precision,
                                   const ElemArgs& a, cudaStream_t s);

@@ -37,6 +37,23 @@ struct RefPattern {
   int64_t* src = nullptr;       // [nnz] index of the entry in the topological pattern
   double* topo_vals = nullptr;  // [pat.nnz] one assembly on the topological pattern
 };
+// A model with multi-point constraints (cxg_plan_create_mpc): the plan itself assembles
+// on the extended numbering (slave DOFs kept as equations; n_free and pat are the
+// extended ones) and the linear / tangent entry points reduce to the free system.
+struct MpcPlan {
+  bool on = false;
+  int32_t n_free = 0;            // the reference's free equations
+  MpcLists lists;
+  int32_t* ext_map = nullptr;    // [n_x]
+  int64_t* term_ptr = nullptr;
+  int32_t* term_eq = nullptr;
+  double* term_coeff = nullptr;
+  double* c_x = nullptr;         // [n_x] slave constants, null when all are zero
+  double* vals_x = nullptr;      // [pat.nnz] one extended assembly
+  double* rhs_x = nullptr;       // [n_x]
+  double* tmp_x = nullptr;       // [n_x]
+  double* kc_x = nullptr;        // [n_x] K_x c
+};
 }  // namespace cxg
 
 struct cxg_plan {
@@ -69,6 +86,7 @@ struct cxg_plan {
   int64_t ring_bytes = 0;     // element-buffer budget: 0 default share of L2, < 0 one window
   std::vector<int32_t> node_first, node_last;  // first / last incident element per node
   cxg::RefPattern refpat;
+  cxg::MpcPlan mpc;
   cudaStream_t last_stream = nullptr;
   int64_t device_bytes = 0;
   // staging buffers for host pointers, grown on demand and reused

@@ -103,6 +103,22 @@ typedef struct {
   int32_t n_free;
 } cxg_dofmap_desc;
 
+/* Multi-point constraints (*EQUATION and the constraints expanded into equations) as the
+ * reference's constraint transform holds them (ConstraintTransform::expansion,
+ * include/calculixpp/fem/constraint_transform.hpp:28-47, built by
+ * src/fem/constraint_transform.cpp:25-131): every slave DOF g = 3*node + comp (ascending)
+ * expands onto free equations with coefficients, plus a constant (the full-magnitude
+ * prescribed values of SPC masters). In the cxg_dofmap_desc of such a model, slaves have
+ * dof_eq -1 and prescribed 0; the free numbering is the reference's. */
+typedef struct {
+  int64_t n_slaves;
+  const int64_t* slave_dof;   /* [n_slaves] ascending */
+  const int64_t* term_ptr;    /* [n_slaves + 1] offsets into term_eq / term_coeff */
+  const int32_t* term_eq;     /* free equation of each term */
+  const double* term_coeff;   /* its coefficient */
+  const double* constant;     /* [n_slaves] */
+} cxg_mpc_desc;
+
 typedef struct cxg_plan cxg_plan;
 
 typedef struct {
@@ -128,6 +144,16 @@ CXG_API int cxg_gauss_points_per_element(int32_t elem_type);
  * 76-110, 211-221): the pattern is built once and reused by every assembly. */
 CXG_API int cxg_plan_create(const cxg_mesh_desc* mesh, const cxg_dofmap_desc* dofs,
                     int32_t precision, cxg_plan** out);
+/* A plan for a model with multi-point constraints. The element pass and row gather
+ * assemble the system on an extended numbering in which slave DOFs are equations too;
+ * a reduction then forms K_ff = T^T K_x T and rhs = T^T (rhs_x - K_x c), the congruence
+ * transform of scatter_block (src/fem/assembly.cpp:76-101) and add_external_load
+ * (assembly.cpp:200-208), each CSR value summed in a fixed order. cxg_plan_get_info,
+ * the pattern calls, cxg_assemble_linear, cxg_assemble_tangent, cxg_spmv and
+ * cxg_solve_cg then work on the reduced free system; f_int stays per global DOF. The
+ * other operators return CXG_ERR_UNSUPPORTED on such a plan. */
+CXG_API int cxg_plan_create_mpc(const cxg_mesh_desc* mesh, const cxg_dofmap_desc* dofs, const cxg_mpc_desc* mpc,
+                                int32_t precision, cxg_plan** out);
 CXG_API int cxg_plan_destroy(cxg_plan* plan);
 CXG_API int cxg_plan_get_info(const cxg_plan* plan, cxg_plan_info* info);
 CXG_API int cxg_plan_set_precision(cxg_plan* plan, int32_t precision);
@@ -153,8 +179,8 @@ CXG_API int cxg_plan_set_launch_config(cxg_plan* plan, int32_t mode, int32_t til
  * row gather. The assembly runs in windows of consecutive elements, each followed by
  * the row gather of the nodes it completes, with the buffers holding only as many
  * elements as the budget allows, so that they stay in L2 between the two passes.
- * 0 (default) = five eighths of the GPU's L2; < 0 = one window over the whole mesh
- * (buffers for every element). The windows follow from the element ordering: a node
+ * 0 (default) or < 0 = one window over the whole mesh (buffers for every element);
+ * > 0 = windows whose buffers fit that many bytes. The windows follow from the element ordering: a node
  * waits for its last incident element, so the ring must also hold the largest
  * distance between a node's first and last element; when the budget cannot, the
  * assembly runs as one window. Results do not depend on the budget. */

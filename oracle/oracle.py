@@ -115,6 +115,7 @@ REF_SIGS = dict(_COMMON, **{
     "model_create": (_vp, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _i32t, _vp, _i64t, _vp, _vp, _vp, _i64t,
                            _vp, _vp, _vp]),
     "model_free": (None, [_vp]),
+    "model_add_equation": (_i, [_vp, _i32t, _vp, _vp, _vp]),
     "element_mass": (_i, [_i, _vp, _d, _i, _vp]),
     "model_set_density": (_i, [_vp, _i32t, _vp]),
     "assemble_mass": (_vp, [_vp, _i]),
@@ -475,6 +476,11 @@ class RefModel:
         self.ref._fn("sys_free")(_vp(s))
         return {"n_free": n_free, "rows": rows, "cols": cols, "vals": vals, "rhs": rhs,
                 "dof_eq": dof_eq}
+
+    def add_equation(self, nodes, comps, coeffs):
+        """*EQUATION sum coeff_i u(node_i, comp_i) = 0, the first term dependent."""
+        n, c, k = _i32(nodes), _i32(comps), _f64(coeffs)
+        self.ref._check(self.ref._fn("model_add_equation")(_vp(self.h), n.size, _p(n), _p(c), _p(k)))
 
     def assemble_linear_static(self):
         """Returns the reference LinearSystem (COO in hash-map order) as a dict."""

@@ -309,6 +309,21 @@ void* ref_model_create(int64_t n_nodes, const double* coords, int64_t n_elems,
 
 void ref_model_free(void* model) { delete static_cast<RefModel*>(model); }
 
+// Adds a linear multi-point constraint (*EQUATION) sum coeff_i u(node_i, comp_i) = 0 to the
+// model; the first term is the dependent DOF. Nodes 0-based, comps 0..2.
+int ref_model_add_equation(void* model, int32_t n_terms, const int32_t* nodes, const int32_t* comps,
+                           const double* coeffs) {
+  try {
+    Equation eq;
+    eq.origin = "*EQUATION";
+    for (int32_t i = 0; i < n_terms; ++i) eq.terms.push_back(EquationTerm{nodes[i] + 1, comps[i] + 1, coeffs[i]});
+    static_cast<RefModel*>(model)->model.equations.push_back(eq);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
 // The Model behind a handle, for other harness translation units (ref_cuda_shim.cpp).
 const cxpp::Model* ref_model_get(void* model) { return &static_cast<RefModel*>(model)->model; }
 

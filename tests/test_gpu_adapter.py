@@ -10,6 +10,9 @@ all on the CPU (numerics::solve_linear_static), on the same Model object:
 * the LinearSystem itself: the same triplets (as canonical CSR) within 1e-12, the same rhs;
 * the material-point path (J2, per-element sections): tangent and f_int within 1e-12
   over three increments with commits, against assemble_material_tangent;
+* *EQUATION constraints (slave elimination through the reference's constraint
+  transform, including a slave whose master is a nonzero SPC): the reduced system within
+  1e-12, displacements within 1e-10, the J2 tangent within 1e-12;
 * models the GPU path does not cover (several element types) raise the adapter's
   message instead of returning a wrong system.
 """
@@ -144,3 +147,63 @@ def test_several_element_types_rejected(cuda, ref, adapter):
             adapter.assembler(rm)
     finally:
         ref._fn("model_free")(C.c_void_p(h))
+
+
+def _with_equations(ref, etype, plastic=False):
+    """Cantilever with *EQUATION ties: the tip face's z motion follows its first node,
+    and the y motion of a node near the centre is half that of a node whose y is
+    prescribed to a nonzero value (the expansion's constant goes to the rhs)."""
+    m, (sn, sc, sv), cl, em = _cantilever(etype, (6, 2, 2) if etype == mg.C3D8 else (3, 2, 2), seed=21)
+    tip = mg.face_nodes(m, 0, float(6 if etype == mg.C3D8 else 3))
+    mid = int(np.argmin(np.abs(m.coords - m.coords.mean(axis=0)).sum(axis=1)))
+    pres_node = int(tip[-1])
+    sn = np.concatenate([sn, [pres_node]]).astype(np.int32)
+    sc = np.concatenate([sc, [1]]).astype(np.int32)
+    sv = np.concatenate([sv, [0.02]])
+    mats = ([make_material(210000.0, 0.3, ISO, 0), make_material(150000.0, 0.3, ISO, 0)] if plastic
+            else [make_material(210000.0, 0.3), make_material(70000.0, 0.33)])
+    rm = ref.model(m, mats, em, (sn, sc, sv), cl)
+    for node in tip[1:-1]:
+        rm.add_equation([int(node), int(tip[0])], [2, 2], [1.0, -1.0])
+    rm.add_equation([mid, pres_node], [1, 1], [2.0, -1.0])  # u_y(mid) = u_y(prescribed node) / 2
+    return m, rm
+
+
+@pytest.mark.parametrize("etype", [mg.C3D8, mg.C3D20])
+def test_equations_linear_system_and_solve(cuda, ref, adapter, etype):
+    m, rm = _with_equations(ref, etype)
+    want = rm.assemble_linear_static()
+    nf = want["n_free"]
+    assert nf < 3 * m.n_nodes - 3 * mg.face_nodes(m, 0, 0.0).size - 1  # slaves eliminated
+    rp, ci, v = coo_to_csr(nf, want["rows"], want["cols"], want["vals"])
+    h = adapter.assembler(rm)
+    try:
+        rows, cols, vals, rhs = adapter.assemble_linear(h)
+    finally:
+        adapter.free(h)
+    assert rel_fro(_csr_on(rp, ci, nf, rows, cols, vals), v) <= 1e-12
+    assert rel_fro(rhs, want["rhs"]) <= 1e-12
+    u_cpu, _ = adapter.solve_linear_static(rm, gpu=0)
+    u_gpu, _ = adapter.solve_linear_static(rm, gpu=1)
+    assert rel_fro(u_gpu, u_cpu) <= 1e-10
+
+
+def test_equations_material_tangent(cuda, ref, adapter):
+    m, rm = _with_equations(ref, mg.C3D8, plastic=True)
+    h = adapter.assembler(rm)
+    try:
+        x = m.coords
+        for k in (1, 2):
+            u = np.zeros_like(x)
+            u[:, 0] = 0.004 * k * x[:, 0] * (0.3 + x[:, 2] / x[:, 2].max())
+            u = u.reshape(-1)
+            want = rm.assemble_material_tangent(u)
+            rm.commit()
+            rows, cols, vals, rhs, f_int = adapter.assemble_tangent(h, u, commit=True)
+            nf = want["n_free"]
+            rp, ci, v = coo_to_csr(nf, want["rows"], want["cols"], want["vals"])
+            assert rel_fro(_csr_on(rp, ci, nf, rows, cols, vals), v) <= 1e-12, k
+            assert rel_fro(f_int, want["f_int"]) <= 1e-12, k
+            assert rel_fro(rhs, want["rhs"]) <= 1e-12, k
+    finally:
+        adapter.free(h)

@@ -3,6 +3,7 @@ batch output equals the assembly of that model alone, bit for bit, in FP64 and m
 precision, whatever launch shape the groups run with, directly or as a CUDA graph;
 the autotuner's cache round-trips; J2 models assemble their tangent in the batch with
 the same bits as alone."""
+import ctypes as C
 import json
 
 import numpy as np
@@ -110,9 +111,13 @@ def test_host_buffers_and_rejections(cuda, models):
     dv, dr = b.assemble(torch.as_tensor(f, device=b.device))
     assert torch.equal(hv, dv.cpu()) and torch.equal(hr, dr.cpu())
     b.close()
-    with pytest.raises(CxgError):
-        b2 = Batch(models[:2], "fp64")
-        b2.assemble_tangent(np.zeros(3 * b2.n_nodes))  # host u: device buffers only
+    b2 = Batch(models[:2], "fp64")
+    hu = np.zeros(3 * b2.n_nodes)  # host u: the batched tangent takes device buffers only
+    vals, rhs = b2.buffers()
+    rc = b2.lib.cxg_batch_assemble_tangent(b2.h, C.c_void_p(hu.ctypes.data), C.c_void_p(vals.data_ptr()), None,
+                                           C.c_void_p(rhs.data_ptr()), None, None)
+    assert rc == 1 and b"device buffers" in b2.lib.cxg_last_error()
+    b2.close()
 
 
 J2 = ([0.0, 1.0], [250.0, 1250.0])  # sigma_y 250, linear hardening H = 1000

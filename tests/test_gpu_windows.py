@@ -81,7 +81,7 @@ def test_windowed_tangent_equals_one_window(cuda, precision):
     assert float(one.state()[:, 6].max()) > 0.0
 
 
-def test_default_budget_keeps_small_meshes_in_one_window(cuda):
+def test_default_budget_is_one_window(cuda):
     model = box_model(mg.C3D8, 6, 4, 4)
     plan = Plan(model)
     plan.assemble_linear(model.external_load_vector())
