@@ -202,12 +202,36 @@ cxpp::fem::LinearSystem assemble_linear_static_cuda(const cxpp::Model& model, Pr
   return a.assemble_linear_static();
 }
 
+std::vector<cxpp::Real> CudaBackend::solve_sparse(const std::vector<cxpp::Index>& rows,
+                                                  const std::vector<cxpp::Index>& cols,
+                                                  const std::vector<cxpp::Real>& vals, cxpp::Index n,
+                                                  const std::vector<cxpp::Real>& rhs,
+                                                  cxpp::compute::SolverKind solver) const {
+  if (rows.size() != vals.size() || cols.size() != vals.size() || rhs.size() != static_cast<std::size_t>(n))
+    throw std::invalid_argument("solve_sparse: inconsistent COO / rhs sizes");
+  std::vector<cxpp::Real> x(static_cast<std::size_t>(n), 0.0);
+  const bool cg = solver == cxpp::compute::SolverKind::CG;
+  const int rc = cxg_solve_sparse(n, static_cast<int64_t>(vals.size()), rows.data(), cols.data(), vals.data(),
+                                  rhs.data(), x.data(), cg ? CXG_SOLVER_CG : CXG_SOLVER_DIRECT, 1e-10,
+                                  std::max<int32_t>(1000, 10 * n), nullptr, nullptr);
+  if (rc != CXG_OK) throw std::runtime_error(cxg_last_error());
+  return x;
+}
+
+const cxpp::compute::ComputeBackend& cuda_backend() {
+  static const CudaBackend backend;
+  return backend;
+}
+
 cxpp::StaticFields solve_linear_static_cuda(const cxpp::Model& model,
-                                            std::optional<cxpp::numerics::SolverKind> forced, Precision precision) {
+                                            std::optional<cxpp::numerics::SolverKind> forced, Precision precision,
+                                            bool gpu_solve) {
   const cxpp::fem::LinearSystem sys = assemble_linear_static_cuda(model, precision);
   const cxpp::numerics::SolverKind kind =
       forced ? *forced : cxpp::numerics::resolve_solver_kind(model.solver, sys.n_free);
-  const std::vector<cxpp::Real> uf = cxpp::numerics::solve_reduced(sys, kind);
+  const std::vector<cxpp::Real> uf =
+      gpu_solve ? cuda_backend().solve_sparse(sys.rows, sys.cols, sys.vals, sys.n_free, sys.rhs, kind)
+                : cxpp::numerics::solve_reduced(sys, kind);
   cxpp::StaticFields res;
   const std::size_t n_nodes = model.mesh.num_nodes();
   res.displacement.assign(n_nodes, cxpp::Vec3{0, 0, 0});

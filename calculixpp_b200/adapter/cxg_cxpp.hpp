@@ -20,6 +20,7 @@
 #include <optional>
 #include <vector>
 
+#include "calculixpp/compute/backend.hpp"
 #include "calculixpp/fem/assembly.hpp"
 #include "calculixpp/numerics/linear_static.hpp"
 #include "cxg.h"
@@ -65,15 +66,32 @@ class CudaAssembler {
   std::vector<int64_t> active_;       // mesh element index of every plan element
 };
 
+// ComputeBackend (include/calculixpp/compute/backend.hpp:40-57) on the GPU: solve_sparse
+// through cxg_solve_sparse, the COO triplets of a LinearSystem in, x out. SolverKind::Direct
+// is a sparse Cholesky on the device; SolverKind::CG is the device's Jacobi-preconditioned
+// CG to a relative residual of 1e-10 (the CPU backend uses IC0), throwing
+// std::runtime_error("CG did not converge ...") like the CPU backend
+// (src/compute/cpu_backend.cpp:57-62). select_backend(BackendKind::CUDA) would return it.
+class CudaBackend : public cxpp::compute::ComputeBackend {
+ public:
+  cxpp::compute::BackendKind kind() const override { return cxpp::compute::BackendKind::CUDA; }
+  std::vector<cxpp::Real> solve_sparse(const std::vector<cxpp::Index>& rows, const std::vector<cxpp::Index>& cols,
+                                       const std::vector<cxpp::Real>& vals, cxpp::Index n,
+                                       const std::vector<cxpp::Real>& rhs,
+                                       cxpp::compute::SolverKind solver) const override;
+};
+const cxpp::compute::ComputeBackend& cuda_backend();
+
 // One-shot form of CudaAssembler::assemble_linear_static with the reference's signature.
 cxpp::fem::LinearSystem assemble_linear_static_cuda(const cxpp::Model& model,
                                                     Precision precision = Precision::FP64);
 
 // numerics::solve_linear_static (src/numerics/linear_static.cpp:29-50) with the
-// assembly on the GPU: the same solver choice, solve_reduced through the selected
-// compute backend, expansion through the constraint transform and field recovery.
+// assembly on the GPU: the same solver choice, the solve through the compute backend
+// (the selected one, as solve_reduced does, or cuda_backend() when gpu_solve), expansion
+// through the constraint transform and field recovery.
 cxpp::StaticFields solve_linear_static_cuda(const cxpp::Model& model,
                                             std::optional<cxpp::numerics::SolverKind> forced = std::nullopt,
-                                            Precision precision = Precision::FP64);
+                                            Precision precision = Precision::FP64, bool gpu_solve = false);
 
 }  // namespace cxg_cxpp

@@ -142,7 +142,8 @@ REF_SIGS = dict(_COMMON, **{
 # The reference's drivers with the product's C++ adapter (ref_cuda_shim.cpp).
 ADAPTER_SIGS = {
     "last_error": (C.c_char_p, []),
-    "solve_linear_static": (_i, [_vp, _i, _i, _vp, _vp]),
+    "solve_linear_static": (_i, [_vp, _i, _i, _i, _vp, _vp]),
+    "backend_solve": (_i, [_i32t, _i64t, _vp, _vp, _vp, _vp, _i, _vp]),
     "assembler_create": (_vp, [_vp, _i]),
     "assembler_free": (None, [_vp]),
     "assembler_sizes": (_i, [_vp, _vp, _vp]),
@@ -582,13 +583,23 @@ class RefCuda(_Base):
     def available(path=ADAPTER_SO):
         return os.path.exists(path)
 
-    def solve_linear_static(self, ref_model, gpu, precision=0):
-        """(u (N,3), nodal stress (N,6)) of numerics::solve_linear_static with a direct
-        solve; gpu selects the adapter's assembly."""
+    def solve_linear_static(self, ref_model, gpu, precision=0, solver=0):
+        """(u (N,3), nodal stress (N,6)) of numerics::solve_linear_static; gpu 0 all on
+        the CPU, 1 the adapter's assembly, 2 the adapter's assembly and device solve;
+        solver 0 direct, 1 CG."""
         N = ref_model.mesh.n_nodes
         u, st = np.zeros(3 * N), np.zeros(6 * N)
-        self._check(self._fn("solve_linear_static")(_vp(ref_model.h), int(gpu), int(precision), _p(u), _p(st)))
+        self._check(self._fn("solve_linear_static")(_vp(ref_model.h), int(gpu), int(precision), int(solver), _p(u),
+                                                    _p(st)))
         return u.reshape(N, 3), st.reshape(N, 6)
+
+    def backend_solve(self, n, rows, cols, vals, rhs, solver=0):
+        """CudaBackend::solve_sparse on COO triplets."""
+        rows, cols, vals, rhs = _i32(rows), _i32(cols), _f64(vals), _f64(rhs)
+        x = np.zeros(int(n))
+        self._check(self._fn("backend_solve")(int(n), vals.size, _p(rows), _p(cols), _p(vals), _p(rhs), int(solver),
+                                              _p(x)))
+        return x
 
     def assembler(self, ref_model, precision=0):
         h = self._fn("assembler_create")(_vp(ref_model.h), int(precision))

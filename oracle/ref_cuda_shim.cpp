@@ -32,20 +32,36 @@ extern "C" {
 
 const char* cuda_last_error(void) { return g_err.c_str(); }
 
-// numerics::solve_linear_static with a direct solve (gpu = 0: all on the CPU; 1: the
-// assembly through the adapter). u[3N] displacement, stress[6N] averaged nodal stress.
-int cuda_solve_linear_static(void* model, int gpu, int precision, double* u, double* stress) {
+// numerics::solve_linear_static (gpu = 0: all on the CPU; 1: the assembly through the
+// adapter; 2: the assembly and the solve on the GPU, through CudaBackend). solver 0
+// direct, 1 CG. u[3N] displacement, stress[6N] averaged nodal stress.
+int cuda_solve_linear_static(void* model, int gpu, int precision, int solver, double* u, double* stress) {
   try {
     const cxpp::Model& m = *ref_model_get(model);
-    const auto kind = cxpp::numerics::SolverKind::Direct;
+    const auto kind = solver ? cxpp::numerics::SolverKind::CG : cxpp::numerics::SolverKind::Direct;
     const cxpp::StaticFields r =
-        gpu ? cxg_cxpp::solve_linear_static_cuda(m, kind, static_cast<cxg_cxpp::Precision>(precision))
+        gpu ? cxg_cxpp::solve_linear_static_cuda(m, kind, static_cast<cxg_cxpp::Precision>(precision), gpu == 2)
             : cxpp::numerics::solve_linear_static(m, kind);
     for (std::size_t i = 0; i < r.displacement.size(); ++i)
       for (int d = 0; d < 3; ++d) u[3 * i + d] = r.displacement[i][static_cast<std::size_t>(d)];
     if (stress)
       for (std::size_t i = 0; i < r.stress.size(); ++i)
         for (int d = 0; d < 6; ++d) stress[6 * i + d] = r.stress[i][static_cast<std::size_t>(d)];
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// CudaBackend::solve_sparse on COO triplets (solver 0 direct, 1 CG).
+int cuda_backend_solve(int32_t n, int64_t nnz, const int32_t* rows, const int32_t* cols, const double* vals,
+                       const double* rhs, int solver, double* x) {
+  try {
+    const std::vector<cxpp::Index> r(rows, rows + nnz), c(cols, cols + nnz);
+    const std::vector<cxpp::Real> v(vals, vals + nnz), b(rhs, rhs + n);
+    const std::vector<cxpp::Real> sol = cxg_cxpp::cuda_backend().solve_sparse(
+        r, c, v, n, b, solver ? cxpp::compute::SolverKind::CG : cxpp::compute::SolverKind::Direct);
+    std::memcpy(x, sol.data(), sizeof(double) * static_cast<std::size_t>(n));
     return 0;
   } catch (const std::exception& e) {
     return fail(e);
