@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--j2-n", type=int, default=128, help="cells per axis of the C3D8 J2 block (0: skip)")
     ap.add_argument("--batch-models", type=int, default=256, help="models of the batched workload (0: skip)")
     ap.add_argument("--adj-n", type=int, default=96, help="cells along x and y of the adjoint cantilever (0: skip)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shapes (no tuning sweeps; for profiler runs)")
     return ap.parse_args()
 
 
@@ -199,7 +201,7 @@ def j2_newton(args, world, dev, stream):
     shapes = {}
     for prec in ("fp64", "mixed"):
         plan.set_precision(prec)
-        shapes[prec] = plan.tune(step, tangent=True)
+        shapes[prec] = {"default": True} if args.no_tune else plan.tune(step, tangent=True)
         for _ in range(args.warmup):
             step()
         plan.check()
@@ -317,7 +319,7 @@ def batched(args, world, rank, dev, stream):
     def run(prec):
         b.set_precision(prec)
         t0 = time.perf_counter()
-        cfg = b.tune(f, vals, rhs)
+        cfg = [] if args.no_tune else b.tune(f, vals, rhs)
         t_tune = time.perf_counter() - t0
 
         def step():
@@ -610,7 +612,7 @@ def main():
     shapes = {}
     for prec in ("fp64", "mixed"):
         plan.set_precision(prec)
-        shapes[prec] = plan.tune(step)
+        shapes[prec] = {"default": True} if args.no_tune else plan.tune(step)
         for _ in range(args.warmup):
             step()
         plan.check()

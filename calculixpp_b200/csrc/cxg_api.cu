@@ -351,6 +351,7 @@ V2Args v2_args(cxg_plan* p, const double* f_ext, bool accumulate) {
   v.e_begin = 0;
   v.e_end = p->n_elems;
   v.ring = std::max<int64_t>(p->n_elems, 1);
+  v.ring_base = 0;
   v.node_order = nullptr;
   v.n_begin = 0;
   v.n_end = p->n_nodes;

@@ -108,7 +108,7 @@ struct V2Args {
   // elements [e_begin, e_end), the row gather the nodes node_order[n_begin..n_end)
   // (node_order null: nodes n_begin..n_end in mesh order). The element buffers hold
   // `ring` elements; element e lives in slot e mod ring.
-  int64_t e_begin, e_end, ring;
+  int64_t e_begin, e_end, ring, ring_base;
   const int32_t* node_order;
   int64_t n_begin, n_end;
   // Window schedule read by the launcher (host arrays): n_win windows with element

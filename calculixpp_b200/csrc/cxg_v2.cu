@@ -83,11 +83,13 @@ __host__ __device__ constexpr int blk_index(int n, int a, int b) { return a * n 
 template <typename R>
 __host__ __device__ constexpr int blk_stride() { return sizeof(R) == 8 ? 10 : 12; }
 
-// Slot of element e in the element buffer: a ring of `ring` elements (the whole mesh when
-// the assembly runs as one window). Element indices fit 31 bits (incidence codes are
-// e*n + local index in int32), so the modulo is 32-bit.
-__device__ __forceinline__ int64_t ring_slot(int64_t e, int64_t ring) {
-  return e < ring ? e : static_cast<int64_t>(static_cast<uint32_t>(e) % static_cast<uint32_t>(ring));
+// Slot of element e in the element buffer, a ring of `ring` elements (the whole mesh when
+// the assembly runs as one window; ring_base 0): e mod ring. Every element a window's
+// passes touch lies in [ring_base, ring_base + 2 ring), so one conditional subtraction
+// gives the slot, with no division in the inner loops.
+__device__ __forceinline__ int64_t ring_slot(int64_t e, const V2Args& V) {
+  const int64_t d = e - V.ring_base;
+  return d < V.ring ? d : d - V.ring;
 }
 
 template <typename R>
@@ -174,7 +176,7 @@ __device__ bool j2_point(const J2Mat& M, double lam, double mu_el, double mu, co
     mu_t = mu_el;
     c_t = 0.0;
     mu_hg = mu_el;
-    return false;
+    return 0;
   }
   const double ep0 = cs[6];
   double dgamma = 0.0;
@@ -219,9 +221,13 @@ constexpr float kYieldBandFp32 = 1e-3f;
 // multiplier, the stress and history update and the consistent-tangent parameters in
 // FP32. The consistency scalar f = q_tr - sigma_y(ep0) decides the branch in FP32 only
 // when |f| exceeds kYieldBandFp32 * sigma_y, clear of the FP32 rounding of q_tr; points
-// inside the band, and points whose FP32 Newton does not settle, take the FP64 return.
-// The hardening table is read in FP64 (it is indexed by the FP64 history).
-__device__ bool j2_point_mixed(const J2Mat& M, double lam, double mu_el, double mu, const double* eps,
+// inside the band, and points whose FP32 Newton does not settle, take the FP64 return:
+// the function then returns kJ2Fp64 and writes nothing, and the caller runs j2_point (one
+// call site, so the FP64 return is inlined once). Else it returns 1 for a plastic step and
+// 0 for an elastic one. The hardening table is read in FP64 (it is indexed by the FP64
+// history).
+constexpr int kJ2Fp64 = 2;
+__device__ __forceinline__ int j2_point_mixed(const J2Mat& M, double lam, double mu_el, double mu, const double* eps,
                                const double* cs, double* ts, double* sig, double& lam_t, double& mu_t,
                                double& c_t, double* nv, double& mu_hg) {
   const float l = static_cast<float>(lam), me = static_cast<float>(mu_el), m = static_cast<float>(mu);
@@ -249,8 +255,7 @@ __device__ bool j2_point_mixed(const J2Mat& M, double lam, double mu_el, double 
   double sy0 = 0.0, h0 = 0.0;
   if (M.plastic) hardening2(M, cs[6], sy0, h0);
   const float f = q_tr - static_cast<float>(sy0);
-  if (M.plastic && fabsf(f) <= kYieldBandFp32 * static_cast<float>(sy0))
-    return j2_point(M, lam, mu_el, mu, eps, cs, ts, sig, lam_t, mu_t, c_t, nv, mu_hg);
+  if (M.plastic && fabsf(f) <= kYieldBandFp32 * static_cast<float>(sy0)) return kJ2Fp64;
   if (!M.plastic || f <= 0.0f || xi_norm == 0.0f) {
 #pragma unroll
     for (int i = 0; i < 6; ++i) sig[i] = st[i];
@@ -260,7 +265,7 @@ __device__ bool j2_point_mixed(const J2Mat& M, double lam, double mu_el, double 
     mu_t = mu_el;
     c_t = 0.0;
     mu_hg = mu_el;
-    return false;
+    return 0;
   }
   const double ep0 = cs[6];
   float dgamma = 0.0f;
@@ -278,7 +283,7 @@ __device__ bool j2_point_mixed(const J2Mat& M, double lam, double mu_el, double 
       break;
     }
   }
-  if (!settled) return j2_point(M, lam, mu_el, mu, eps, cs, ts, sig, lam_t, mu_t, c_t, nv, mu_hg);
+  if (!settled) return kJ2Fp64;
   float n32[6];
 #pragma unroll
   for (int i = 0; i < 6; ++i) n32[i] = xi[i] / xi_norm;
@@ -305,7 +310,7 @@ __device__ bool j2_point_mixed(const J2Mat& M, double lam, double mu_el, double 
   mu_t = mt;
   c_t = ct;
   mu_hg = mt - ct * n32[3] * n32[3];
-  return true;
+  return 1;
 }
 
 __constant__ double c_hg2[4][8] = {
@@ -524,18 +529,32 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
         const int mat = A.elem_mat ? A.elem_mat[e] : 0;
         const int64_t gidx = e * nq + q;
         double cs[kStateDoubles], ts[kStateDoubles], sig[6], nv[6] = {0, 0, 0, 0, 0, 0};
-        const int ncomp = A.state_comps;
+        // plastic strain and equivalent plastic strain always; the back stress only when
+        // some material moves it (state_comps 13), else it is zero
+        const bool back = A.state_comps > 7;
 #pragma unroll
-        for (int c = 0; c < kStateDoubles; ++c) cs[c] = c < ncomp ? A.state_c[c * A.n_gauss + gidx] : 0.0;
+        for (int c = 0; c < 7; ++c) cs[c] = A.state_c[c * A.n_gauss + gidx];
+        if (back) {
+#pragma unroll
+          for (int c = 7; c < kStateDoubles; ++c) cs[c] = A.state_c[c * A.n_gauss + gidx];
+        } else {
+#pragma unroll
+          for (int c = 7; c < kStateDoubles; ++c) cs[c] = 0.0;
+        }
         double lt, mt, ct, mhg;
         // FP64 return in the FP64 path; FP32 (with the FP64 band near yield) in mixed precision
-        const bool pl = sizeof(R) == 8
+        const int r = sizeof(R) == 8 ? kJ2Fp64
+                                     : j2_point_mixed(A.mats[mat], W.lam[ei], W.mu[ei], W.mu_j2[ei], eps, cs, ts, sig,
+                                                      lt, mt, ct, nv, mhg);
+        const bool pl = r == kJ2Fp64
                             ? j2_point(A.mats[mat], W.lam[ei], W.mu[ei], W.mu_j2[ei], eps, cs, ts, sig, lt, mt, ct, nv, mhg)
-                            : j2_point_mixed(A.mats[mat], W.lam[ei], W.mu[ei], W.mu_j2[ei], eps, cs, ts, sig, lt, mt,
-                                             ct, nv, mhg);
+                            : r != 0;
 #pragma unroll
-        for (int c = 0; c < kStateDoubles; ++c)
-          if (c < ncomp) A.state_t[c * A.n_gauss + gidx] = ts[c];
+        for (int c = 0; c < 7; ++c) A.state_t[c * A.n_gauss + gidx] = ts[c];
+        if (back) {
+#pragma unroll
+          for (int c = 7; c < kStateDoubles; ++c) A.state_t[c * A.n_gauss + gidx] = ts[c];
+        }
         for (int c = 0; c < 6; ++c) W.sig[ei][q][c] = sq * sig[c];
         W.dp[ei][q][0] = static_cast<R>(sq * lt);
         W.dp[ei][q][1] = static_cast<R>(sq * mt);
@@ -680,7 +699,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
           }
         }
         if constexpr (!STAGE) {
-          R* out = reinterpret_cast<R*>(V.edata) + ring_slot(e, V.ring) * (NB * blk_stride<R>());
+          R* out = reinterpret_cast<R*>(V.edata) + ring_slot(e, V) * (NB * blk_stride<R>());
 #pragma unroll
           for (int i = 0; i < TR; ++i)
 #pragma unroll
@@ -726,7 +745,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
       }
       __syncwarp();
       for (int ei = 0; ei < EPW && e0 + ei < e_end; ++ei) {
-        R* out = reinterpret_cast<R*>(V.edata) + ring_slot(e0 + ei, V.ring) * (NB * BS);
+        R* out = reinterpret_cast<R*>(V.edata) + ring_slot(e0 + ei, V) * (NB * BS);
         const R* sb = stg + ei * NB * 9;
         for (int pc = lane; pc < NB * CPB; pc += 32) {
           const int k = pc / CPB, part = pc % CPB;
@@ -770,7 +789,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
             for (int d = 0; d < 3; ++d) f[d] += ka * gu[d];
           }
         }
-        for (int d = 0; d < 3; ++d) V.fdata[ring_slot(e, V.ring) * (3 * n) + 3 * a + d] = f[d];
+        for (int d = 0; d < 3; ++d) V.fdata[ring_slot(e, V) * (3 * n) + 3 * a + d] = f[d];
       }
     }
     __syncwarp();
@@ -812,9 +831,9 @@ struct P2Pass {
   bool active;
 };
 
-template <int ET, typename R>
-__device__ __forceinline__ void p2_fetch(const ElemArgs& A, const R* ed, int64_t ring, int code, bool active, int lb,
-                                         P2Pass<R>& p) {
+template <int ET, typename R, bool WIN>
+__device__ __forceinline__ void p2_fetch(const ElemArgs& A, const V2Args& V, const R* ed, int code, bool active,
+                                         int lb, P2Pass<R>& p) {
   constexpr int n = nodes_of(ET), NB = n * (n + 1) / 2;
   p.active = active;
   p.e = code / n;
@@ -824,7 +843,7 @@ __device__ __forceinline__ void p2_fetch(const ElemArgs& A, const R* ed, int64_t
     p.slotv = __ldg(A.slot + (p.e * n + p.la) * n + lb);
     const bool tr = lb < p.la;
     double raw[9];
-    load_block<R>(ed + ring_slot(p.e, ring) * (NB * blk_stride<R>()) +
+    load_block<R>(ed + (WIN ? ring_slot(p.e, V) : p.e) * (NB * blk_stride<R>()) +
                       (tr ? blk_index(n, lb, p.la) : blk_index(n, p.la, lb)) * blk_stride<R>(),
                   raw);
 #pragma unroll
@@ -837,7 +856,7 @@ __device__ __forceinline__ void p2_fetch(const ElemArgs& A, const R* ed, int64_t
   }
 }
 
-template <int ET, bool TAN, typename R, bool DIAGFIX>
+template <int ET, bool TAN, typename R, bool DIAGFIX, bool WIN>
 __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   constexpr int n = nodes_of(ET);
   constexpr int GS = P2Geo<ET, DIAGFIX>::GS, EG = P2Geo<ET, DIAGFIX>::EG;
@@ -851,9 +870,10 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   const int sub = lane / GS, lb = lane % GS;
   const bool lane_ok = lb < n;
   double* mine = buf + sub * stride;
-  // nodes [V.n_begin, V.n_end) of this window's node list (node_order), or of the mesh
-  for (int64_t idx = V.n_begin + gwarp; idx < V.n_end; idx += nwarps) {
-    const int64_t a = V.node_order ? static_cast<int64_t>(V.node_order[idx]) : idx;
+  // nodes [V.n_begin, V.n_end) of this window's node list (node_order, WIN), or of the mesh
+  const int64_t n_begin = WIN ? V.n_begin : 0, n_end = WIN ? V.n_end : A.n_nodes;
+  for (int64_t idx = n_begin + gwarp; idx < n_end; idx += nwarps) {
+    const int64_t a = WIN ? static_cast<int64_t>(V.node_order[idx]) : idx;
     const int ma = A.node_mask[a];
     const int nf = __popc(ma);
     const int L = static_cast<int>(A.node_rowlen[a]);
@@ -878,7 +898,7 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
       const int code_l = lane < cnt ? __ldg(V.inc_code + c0 + lane) : 0;
       for (int k = 0; k < cnt; k += EG) {
         P2Pass<R> cur;
-        p2_fetch<ET, R>(A, ed, V.ring, __shfl_sync(0xffffffffu, code_l, (k + sub) & 31), lane_ok && k + sub < cnt, lb,
+        p2_fetch<ET, R, WIN>(A, V, ed, __shfl_sync(0xffffffffu, code_l, (k + sub) & 31), lane_ok && k + sub < cnt, lb,
                         cur);
         if (cur.active && (!DIAGFIX || lb != cur.la)) {
           double* col = mine + cur.slotv;
@@ -912,7 +932,7 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
         }
         if (TAN && cur.active && lb == cur.la) {
 #pragma unroll
-          for (int d = 0; d < 3; ++d) fs[d] += __ldg(V.fdata + ring_slot(cur.e, V.ring) * (3 * n) + 3 * cur.la + d);
+          for (int d = 0; d < 3; ++d) fs[d] += __ldg(V.fdata + (WIN ? ring_slot(cur.e, V) : cur.e) * (3 * n) + 3 * cur.la + d);
         }
         if (DIAGFIX && cur.active) {
           if (lb != cur.la) {
@@ -985,17 +1005,20 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   }
 }
 
-// Blocks of at most 8 warps. The mixed-precision gather of the <= 8-node families is
-// compiled for 3 resident blocks per SM (<= 85 registers), which its short rows leave
-// room for in shared memory; the other gathers are compiled without a register budget.
-template <int ET, bool TAN, typename R, bool DIAGFIX>
+// Blocks of at most 8 warps. The mixed-precision gathers (all but the tangent gather of
+// the > 8-node families, which needs more registers) are compiled for 3 resident blocks
+// per SM (<= 85 registers), which their rows leave room for in shared memory; the other
+// gathers are compiled without a register budget.
+// WIN: the windowed schedule (node list and element ring); the one-window gather is
+// compiled without either, so it keeps the registers of a plain node loop.
+template <int ET, bool TAN, typename R, bool DIAGFIX, bool WIN>
 __global__ void p2_kernel(ElemArgs A, V2Args V) {
-  p2_body<ET, TAN, R, DIAGFIX>(A, V);
+  p2_body<ET, TAN, R, DIAGFIX, WIN>(A, V);
 }
 
-template <int ET, bool TAN, typename R, bool DIAGFIX>
+template <int ET, bool TAN, typename R, bool DIAGFIX, bool WIN>
 __global__ void __launch_bounds__(256, 3) p2_kernel_short(ElemArgs A, V2Args V) {
-  p2_body<ET, TAN, R, DIAGFIX>(A, V);
+  p2_body<ET, TAN, R, DIAGFIX, WIN>(A, V);
 }
 
 int sm_count() {
@@ -1045,7 +1068,9 @@ cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg
 
 template <int ET, bool TAN, typename R, bool DF>
 cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaStream_t s) {
-  auto kern = (DF && nodes_of(ET) <= 8) ? p2_kernel_short<ET, TAN, R, DF> : p2_kernel<ET, TAN, R, DF>;
+  constexpr bool kShort = DF && (nodes_of(ET) <= 8 || !TAN);
+  auto kern = v.node_order ? (kShort ? p2_kernel_short<ET, TAN, R, DF, true> : p2_kernel<ET, TAN, R, DF, true>)
+                           : (kShort ? p2_kernel_short<ET, TAN, R, DF, false> : p2_kernel<ET, TAN, R, DF, false>);
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
   // configured count when it fits)
   const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
@@ -1083,6 +1108,9 @@ cudaError_t launch_v2_type(int mode, int precision, const ElemArgs& a, const V2A
   for (int32_t k = 0; k < v.n_win; ++k) {
     w.e_begin = v.win_e[k];
     w.e_end = v.win_e[k + 1];
+    // both passes of window k touch elements in [e_end - ring, e_end) only
+    const int64_t lo = std::max<int64_t>(0, w.e_end - v.ring);
+    w.ring_base = lo / v.ring * v.ring;
     w.n_begin = v.win_n[k];
     w.n_end = v.win_n[k + 1];
     const cudaError_t err = launch_v2_pair<ET>(mode, precision, a, w, c, s);
