@@ -12,7 +12,8 @@ from .assembly import (LinearSystem, Material, MaterialPoints, Model, Plan, Ther
                        assemble_material_tangent, element_stiffness, element_tangent_force,
                        make_material_points)
 from .batch import Batch
+from .solve import solve_sparse
 
 __all__ = ["meshgen", "Batch", "ThermalPlan", "CxgError", "load_library", "LinearSystem", "Material", "MaterialPoints", "Model",
            "Plan", "assemble_linear_static", "assemble_material_tangent", "element_stiffness",
-           "element_tangent_force", "make_material_points"]
+           "element_tangent_force", "make_material_points", "solve_sparse"]

@@ -22,6 +22,7 @@ CXG_ERR_NO_GPU = 7
 CXG_ERR_NOT_CONVERGED = 8
 
 FP64, MIXED = 0, 1
+SOLVER_DIRECT, SOLVER_CG, SOLVER_IC0_CG = 0, 1, 2
 COMMITTED, TRIAL = 0, 1
 ACCUMULATE = 1
 

@@ -212,7 +212,7 @@ std::vector<cxpp::Real> CudaBackend::solve_sparse(const std::vector<cxpp::Index>
   std::vector<cxpp::Real> x(static_cast<std::size_t>(n), 0.0);
   const bool cg = solver == cxpp::compute::SolverKind::CG;
   const int rc = cxg_solve_sparse(n, static_cast<int64_t>(vals.size()), rows.data(), cols.data(), vals.data(),
-                                  rhs.data(), x.data(), cg ? CXG_SOLVER_CG : CXG_SOLVER_DIRECT, 1e-10,
+                                  rhs.data(), x.data(), cg ? CXG_SOLVER_IC0_CG : CXG_SOLVER_DIRECT, 1e-10,
                                   std::max<int32_t>(1000, 10 * n), nullptr, nullptr);
   if (rc != CXG_OK) throw std::runtime_error(cxg_last_error());
   return x;

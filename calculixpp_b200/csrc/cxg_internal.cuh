@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
+
 #include <cstdint>
 
 #include "cxg_elements.hpp"
@@ -199,6 +201,12 @@ cudaError_t launch_spmv(int32_t nrows, const int64_t* rp, const int32_t* ci, con
 // Jacobi-preconditioned CG on CSR; work holds 5*n + 2056 doubles.
 cudaError_t cg_solve(int32_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* b, double* x,
                      double rtol, int max_iter, double* work, int* iters_out, double* rel_out, cudaStream_t s);
+// The same CG loop with z = M^-1 r given by `precond` (launched on the loop's stream);
+// work holds 5*n + 2056 doubles, the fifth n-vector unused by the loop.
+using Preconditioner = std::function<cudaError_t(const double* r, double* z)>;
+cudaError_t pcg_solve(int32_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* b, double* x,
+                      double rtol, int max_iter, double* work, int* iters_out, double* rel_out, cudaStream_t s,
+                      const Preconditioner& precond);
 // Element tables (constant memory) are uploaded once per device.
 cudaError_t ensure_tables();
 

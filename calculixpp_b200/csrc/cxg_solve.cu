@@ -227,23 +227,35 @@ cudaError_t launch_spmv(int32_t nrows, const int64_t* rp, const int32_t* ci, con
   return cudaGetLastError();
 }
 
-// Jacobi-PCG. work: 5*n + 2048 + 8 doubles. Host reads the residual every `check`
+// Jacobi-PCG. work: 5*n + 2048 + 8 doubles. Host reads the residual every 20
 // iterations; returns iterations and the final relative residual.
 cudaError_t cg_solve(int32_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* b, double* x,
                      double rtol, int max_iter, double* work, int* iters_out, double* rel_out, cudaStream_t s) {
+  double* dinv = work + 4 * static_cast<int64_t>(n);
+  diag_inv_kernel<<<g1(n), 256, 0, s>>>(n, rp, ci, v, dinv);
+  const Preconditioner jacobi = [&](const double* r, double* z) {
+    cg_precond<<<g1(n), 256, 0, s>>>(n, dinv, r, z);
+    return cudaGetLastError();
+  };
+  return pcg_solve(n, rp, ci, v, b, x, rtol, max_iter, work, iters_out, rel_out, s, jacobi);
+}
+
+// Preconditioned CG with z = M^-1 r from `precond`. work: 5*n + 2048 + 8 doubles (the
+// fifth n-vector is left to the preconditioner's owner).
+cudaError_t pcg_solve(int32_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* b, double* x,
+                      double rtol, int max_iter, double* work, int* iters_out, double* rel_out, cudaStream_t s,
+                      const Preconditioner& precond) {
   double* r = work;
   double* z = r + n;
   double* p = z + n;
   double* Ap = p + n;
-  double* dinv = Ap + n;
-  double* partial = dinv + n;
+  double* partial = Ap + 2 * static_cast<int64_t>(n);
   double* sc = partial + 2048;  // rz, rz_new, pAp, bb, rr
   const unsigned gd = g1(n);
   cudaError_t e;
-  diag_inv_kernel<<<gd, 256, 0, s>>>(n, rp, ci, v, dinv);
   if ((e = launch_spmv(n, rp, ci, v, x, Ap, s)) != cudaSuccess) return e;
   residual_kernel<<<gd, 256, 0, s>>>(n, b, Ap, r);
-  cg_precond<<<gd, 256, 0, s>>>(n, dinv, r, z);
+  if ((e = precond(r, z)) != cudaSuccess) return e;
   cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
   auto dot = [&](const double* a, const double* c, double* out) {
     dot_kernel<<<gd, 256, 0, s>>>(n, a, c, partial);
@@ -261,7 +273,7 @@ cudaError_t cg_solve(int32_t n, const int64_t* rp, const int32_t* ci, const doub
     if ((e = launch_spmv(n, rp, ci, v, p, Ap, s)) != cudaSuccess) return e;
     dot(p, Ap, sc + 2);
     cg_update_xr<<<gd, 256, 0, s>>>(n, sc + 0, sc + 2, x, r, p, Ap);
-    cg_precond<<<gd, 256, 0, s>>>(n, dinv, r, z);
+    if ((e = precond(r, z)) != cudaSuccess) return e;
     dot(r, z, sc + 1);
     cg_update_p<<<gd, 256, 0, s>>>(n, sc + 1, sc + 0, z, p);
     cudaMemcpyAsync(sc + 0, sc + 1, sizeof(double), cudaMemcpyDeviceToDevice, s);

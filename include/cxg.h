@@ -296,12 +296,17 @@ CXG_API int cxg_spmv(cxg_plan* plan, const double* vals, const double* x, double
 /* ComputeBackend::solve_sparse (include/calculixpp/compute/backend.hpp:51-56) on the
  * device: A x = rhs for A given as COO triplets (rows[k], cols[k], vals[k]) of an n x n
  * SPD matrix, duplicate entries summed; host or device arrays. solver CXG_SOLVER_DIRECT:
- * sparse Cholesky on the device (the reference's spsolve); CXG_SOLVER_CG:
- * Jacobi-preconditioned CG to rtol (the reference's CG kind uses IC0; the answer agrees
- * to the tolerance), CXG_ERR_NOT_CONVERGED past max_iter as the reference throws
- * (cpu_backend.cpp:57-62). iterations / rel_residual may be NULL. */
+ * sparse Cholesky on the device (the reference's spsolve); CXG_SOLVER_IC0_CG: CG
+ * preconditioned with a zero-fill incomplete Cholesky factor of A, the reference's CG
+ * kind (cpu_backend.cpp:52-63; on a non-positive pivot the factor is retried on
+ * A + alpha diag(A), alpha = 1e-4 .. 1e-1, CXG_ERR_NOT_CONVERGED past that);
+ * CXG_SOLVER_CG: Jacobi-preconditioned CG (more iterations, no factorisation, no
+ * triangular solves). The CG kinds stop at ||r|| <= rtol ||rhs|| and return
+ * CXG_ERR_NOT_CONVERGED past max_iter, as the reference throws (cpu_backend.cpp:57-62).
+ * iterations / rel_residual may be NULL. */
 #define CXG_SOLVER_DIRECT 0
 #define CXG_SOLVER_CG 1
+#define CXG_SOLVER_IC0_CG 2
 CXG_API int cxg_solve_sparse(int32_t n, int64_t nnz, const int32_t* rows, const int32_t* cols, const double* vals,
                              const double* rhs, double* x, int32_t solver, double rtol, int32_t max_iter,
                              int32_t* iterations, double* rel_residual);

@@ -178,3 +178,52 @@ def test_negative_jacobian_in_plan(cuda):
         plan.assemble_linear()
     assert exc.value.code == 4
     assert "non-positive element Jacobian" in str(exc.value)
+
+
+def _translation_residual(plan, n_nodes, vals):
+    """max over rows of |K t| / max|K| for the three unit translations t (every DOF free)."""
+    rp, ci = (to_np(t) for t in plan.pattern())
+    K = sp.csr_matrix((to_np(vals), ci, rp), shape=(3 * n_nodes, 3 * n_nodes))
+    worst = 0.0
+    for d in range(3):
+        t = np.zeros(3 * n_nodes)
+        t[d::3] = 1.0
+        worst = max(worst, np.abs(K @ t).max() / np.abs(K.data).max())
+    return worst
+
+
+@pytest.mark.parametrize("etype", ALL_TYPES)
+def test_mixed_rigid_translations_in_null_space(cuda, etype):
+    """Mixed precision keeps the rigid translations in the null space of K to FP64
+    rounding: the element pass forms each diagonal block in FP64 as minus the sum of the
+    element row's FP32 off-diagonal blocks, so every assembled row sums to ~1e-16 of the
+    largest entry, where FP32 diagonal blocks would leave ~1e-7. No constraint, so K is
+    the full singular matrix."""
+    quad = etype in (mg.C3D20, mg.C3D20R, mg.C3D15, mg.C3D10)
+    dims = (3, 2, 2) if quad else (5, 3, 2)
+    m = mg.box_mesh(etype, *dims, float(dims[0]), float(dims[1]), float(dims[2]), jitter=0.1, seed=etype)
+    m.young = mg.lognormal_young(m.n_elems, seed=etype)
+    m.poisson = np.full(m.n_elems, 0.3)
+    none = (np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    model = Model(m, [Material(200000.0, 0.3)], None, none, None)
+    plan = Plan(model, "mixed")
+    vals, _ = plan.assemble_linear(np.zeros(3 * m.n_nodes))
+    assert _translation_residual(plan, m.n_nodes, vals) <= 1e-13
+
+
+@pytest.mark.parametrize("etype", [mg.C3D8, mg.C3D8R, mg.C3D20])
+def test_mixed_tangent_rigid_translations_in_null_space(cuda, etype):
+    """The same for the consistent tangent of a J2 state with yielded points."""
+    quad = etype == mg.C3D20
+    n = 3 if quad else 5
+    m = mg.box_mesh(etype, n, n, n, 1.0, 1.0, 1.0, jitter=0.05, seed=etype)
+    m.young = np.full(m.n_elems, mg.J2_E)
+    m.poisson = np.full(m.n_elems, mg.J2_NU)
+    none = (np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    model = Model(m, [Material(mg.J2_E, mg.J2_NU, mg.j2_table())], None, none, None)
+    u = mg.graded_uniaxial_field(m.coords, 0.01)
+    plan = Plan(model, "mixed")
+    vals, _, _ = plan.assemble_tangent(u)
+    ep = to_np(plan.state(committed=False))[:, 6]
+    assert (ep > 0).mean() > 0.2  # yielded points take the plastic tangent
+    assert _translation_residual(plan, m.n_nodes, vals) <= 1e-13
