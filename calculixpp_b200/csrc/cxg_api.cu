@@ -346,7 +346,7 @@ V2Args v2_args(cxg_plan* p, const double* f_ext, bool accumulate) {
   v.inc_ptr = p->pat.inc_ptr;
   v.inc_code = p->pat.inc_code;
   v.f_ext = f_ext;
-  v.max_row = p->pat.max_row;
+  v.max_adj = p->pat.max_adj;
   v.accumulate = accumulate ? 1 : 0;
   v.e_begin = 0;
   v.e_end = p->n_elems;
@@ -375,7 +375,8 @@ ElemArgs base_args(cxg_plan* p) {
   a.node_eq0 = p->pat.node_eq0;
   a.prescribed = p->prescribed;
   a.slot = p->pat.slot;
-  a.conn_mask = p->pat.conn_mask;
+  a.adj_ptr = p->pat.adj_ptr;
+  a.adj_node = p->pat.adj_node;
   a.n_gauss = p->n_gauss;
   a.status = p->status;
   return a;
@@ -599,7 +600,7 @@ int cxg_plan_destroy(cxg_plan* p) {
   if (p->last_stream) cudaStreamSynchronize(p->last_stream);
   void* bufs[] = {p->coords, p->conn, p->young, p->poisson, p->elem_mat, p->mats, p->dof_eq, p->prescribed,
                   p->pat.row_ptr, p->pat.col_idx, p->pat.node_base, p->pat.node_rowlen, p->pat.node_mask,
-                  p->pat.node_eq0, p->pat.slot, p->pat.conn_mask, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
+                  p->pat.node_eq0, p->pat.slot, p->pat.adj_ptr, p->pat.adj_node, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
                   p->status, p->edata, p->fdata};
   for (void* b : bufs) cudaFree(b);
   for (auto& row : p->sched)

@@ -74,8 +74,9 @@ struct ElemArgs {
   const uint8_t* node_mask;   // [N] bit i: component i free
   const int32_t* node_eq0;    // [N] first free equation of the node (or -1)
   const double* prescribed;   // [3N]
-  const uint16_t* slot;       // [E*n*n] column offset of node b inside node a's rows
-  const uint8_t* conn_mask;   // [E*n] node_mask of every element node
+  const uint16_t* slot;       // [E*n*n] position of node b in node a's adjacency list
+  const int64_t* adj_ptr;     // [N+1] node adjacency (row gather)
+  const int32_t* adj_node;    // [M]
   // state (tangent mode), SoA [13][G]
   const double* state_c;
   double* state_t;
@@ -103,8 +104,8 @@ struct V2Args {
   const int64_t* inc_ptr;   // node -> incident elements
   const int32_t* inc_code;
   const double* f_ext;      // [3N] load vector for the rhs, or null
-  int64_t max_row;          // largest (free rows x row length) of any node
-  int64_t row_stride;       // set by the launcher
+  int64_t max_adj;          // longest adjacency list of any node
+  int64_t row_stride;       // set by the launcher: doubles per row-buffer copy
   int accumulate;           // add into vals / rhs / f_int instead of overwriting
   // The window of one element-pass + row-gather pair: the element pass integrates
   // elements [e_begin, e_end), the row gather the nodes node_order[n_begin..n_end)
@@ -219,12 +220,16 @@ struct PatternOut {
   int32_t* node_rowlen = nullptr;
   uint8_t* node_mask = nullptr;
   int32_t* node_eq0 = nullptr;
-  uint16_t* slot = nullptr;     // [E*n*n]
-  uint8_t* conn_mask = nullptr; // [E*n] free-component mask of each element node
+  uint16_t* slot = nullptr;     // [E*n*n] position of node b in node a's adjacency list
+  // node adjacency: neighbours of node a (itself included, ascending) are
+  // adj_node[adj_ptr[a] .. adj_ptr[a+1])
+  int64_t* adj_ptr = nullptr;   // [N+1]
+  int32_t* adj_node = nullptr;  // [M]
   // node -> incident elements, ascending element order: codes e*n + local node index
   int64_t* inc_ptr = nullptr;   // [N+1]
   int32_t* inc_code = nullptr;  // [E*n]
   int64_t max_row = 0;          // max over nodes of (free rows) x (row length)
+  int64_t max_adj = 0;          // max over nodes of the adjacency list length
   int64_t device_bytes = 0;
 };
 // Returns a cxg_status code; on error *msg is set.

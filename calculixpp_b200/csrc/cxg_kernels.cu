@@ -12,8 +12,8 @@
 //            plastic counterparts) in registers, form K_ab in closed form
 //              K_ab = lam* G + mu* (G^T + tr(G) I) - c M
 //            (the isotropic B^T D B without the 6x6 B products of
-//            src/fem/element.cpp:440-462), and scatter K_ab and K_ab^T into the CSR
-//            values with FP64 atomic adds (or store them in dense element matrices);
+//            src/fem/element.cpp:440-462), and store K_ab and K_ab^T in the dense
+//            element matrices of the per-element API;
 //   phase D  lanes stride over nodes for the internal force f_a = sum_q s_q S_q g_a.
 // Precision: FP64, or "mixed" where the Gram blocks and K_ab are formed in FP32 from
 // FP32 gradients while Jacobians, their inverses, the J2 update and every global
@@ -177,13 +177,7 @@ struct WarpSmem {
   double gc[3 * n];  // FP64 gradients at the last Gauss point (C3D8R: the centroid)
   double vol;        // w det J there (C3D8R: 8 det J = element volume)
   double u[T ? 3 * n : 1];
-  double presc[3 * n];
   double sig[T ? nq * 6 : 1];  // s_q * sigma_q (Voigt)
-  long long base[n];
-  int node[n];
-  int rowlen[n];
-  int eq0[n];
-  int mask[n];
   int flags;                   // bit0: some Gauss point plastic
   R g[nq * GS];                // [q][d][k] physical gradients
   R s[nq];                     // w_q det J_q
@@ -280,9 +274,9 @@ __device__ __forceinline__ void add_hourglass(const WS& W, int a, int b, double 
   K[2][2] += h;
 }
 
-// Dense element-matrix store, or CSR scatter with FP64 atomic adds: rows of node a /
-// columns of node b, and (a != b) the transposed block into rows of b. Prescribed
-// columns move -K_fc u_c into the rhs (src/fem/assembly.cpp:95-96).
+// Dense element-matrix store: rows of node a / columns of node b, and (a != b) the
+// transposed block into rows of b. (The assembled CSR systems are formed by the
+// two-pass element pass and row gather of cxg_v2.cu.)
 template <int n, bool DENSE, typename WS>
 __device__ __forceinline__ void write_pair(const ElemArgs& A, const WS& W, int64_t e, int a, int b,
                                            const double (&K)[3][3]) {
@@ -295,40 +289,6 @@ __device__ __forceinline__ void write_pair(const ElemArgs& A, const WS& W, int64
         Ke[(3 * b + j) * nd + 3 * a + i] = K[i][j];
       }
     return;
-  }
-  const unsigned short* sl = A.slot + e * n * n;
-  const int ma = W.mask[a], mb = W.mask[b];
-  {
-    const int64_t col0 = sl[a * n + b];
-    for (int i = 0; i < 3; ++i) {
-      if (!((ma >> i) & 1)) continue;
-      const int ri = __popc(ma & ((1 << i) - 1));
-      double* row = A.vals + W.base[a] + static_cast<int64_t>(ri) * W.rowlen[a] + col0;
-      double rr = 0.0;
-      for (int j = 0; j < 3; ++j) {
-        if ((mb >> j) & 1)
-          atomicAdd(row + __popc(mb & ((1 << j) - 1)), K[i][j]);
-        else
-          rr -= K[i][j] * W.presc[3 * b + j];
-      }
-      if (A.rhs && rr != 0.0) atomicAdd(A.rhs + W.eq0[a] + ri, rr);
-    }
-  }
-  if (a != b) {
-    const int64_t col0 = sl[b * n + a];
-    for (int j = 0; j < 3; ++j) {
-      if (!((mb >> j) & 1)) continue;
-      const int rj = __popc(mb & ((1 << j) - 1));
-      double* row = A.vals + W.base[b] + static_cast<int64_t>(rj) * W.rowlen[b] + col0;
-      double rr = 0.0;
-      for (int i = 0; i < 3; ++i) {
-        if ((ma >> i) & 1)
-          atomicAdd(row + __popc(ma & ((1 << i) - 1)), K[i][j]);
-        else
-          rr -= K[i][j] * W.presc[3 * a + i];
-      }
-      if (A.rhs && rr != 0.0) atomicAdd(A.rhs + W.eq0[b] + rj, rr);
-    }
   }
 }
 
@@ -370,27 +330,9 @@ __global__ void __launch_bounds__(kThreads) element_kernel(ElemArgs A) {
 
   for (int64_t e = gwarp; e < A.n_elems; e += nwarps) {
     // ---- phase A: gather ------------------------------------------------------
-    if (DENSE) {
-      for (int t = lane; t < nd; t += 32) {
-        W.x[t] = A.elem_coords[e * nd + t];
-        if (TAN) W.u[t] = A.u[e * nd + t];
-        W.presc[t] = 0.0;
-      }
-    } else {
-      for (int t = lane; t < n; t += 32) {
-        const int node = A.conn[e * n + t];
-        W.node[t] = node;
-        const int msk = A.node_mask[node];
-        W.mask[t] = msk;
-        W.base[t] = A.node_base[node];
-        W.rowlen[t] = A.node_rowlen[node];
-        W.eq0[t] = A.node_eq0[node];
-        for (int d = 0; d < 3; ++d) {
-          W.x[3 * t + d] = A.coords[3 * static_cast<int64_t>(node) + d];
-          W.presc[3 * t + d] = (msk >> d) & 1 ? 0.0 : A.prescribed[3 * static_cast<int64_t>(node) + d];
-          if (TAN) W.u[3 * t + d] = A.u[3 * static_cast<int64_t>(node) + d];
-        }
-      }
+    for (int t = lane; t < nd; t += 32) {
+      W.x[t] = A.elem_coords[e * nd + t];
+      if (TAN) W.u[t] = A.u[e * nd + t];
     }
     const double E = A.young[e];
     const double nu = A.poisson[e];
@@ -581,11 +523,7 @@ __global__ void __launch_bounds__(kThreads) element_kernel(ElemArgs A) {
             for (int d = 0; d < 3; ++d) f[d] += ka * gu[d];
           }
         }
-        if (DENSE) {
-          for (int d = 0; d < 3; ++d) A.fe[e * nd + 3 * a + d] = f[d];
-        } else if (A.f_int) {
-          for (int d = 0; d < 3; ++d) atomicAdd(A.f_int + 3 * static_cast<int64_t>(W.node[a]) + d, f[d]);
-        }
+        for (int d = 0; d < 3; ++d) A.fe[e * nd + 3 * a + d] = f[d];
       }
     }
     __syncwarp();
@@ -621,12 +559,10 @@ cudaError_t launch_t(const ElemArgs& a, cudaStream_t s) {
 
 template <int ET>
 cudaError_t launch_type(int mode, bool dense, int precision, const ElemArgs& a, cudaStream_t s) {
-  if (mode == MODE_LINEAR) {
-    if (dense) return precision ? launch_t<ET, MODE_LINEAR, true, float>(a, s) : launch_t<ET, MODE_LINEAR, true, double>(a, s);
-    return precision ? launch_t<ET, MODE_LINEAR, false, float>(a, s) : launch_t<ET, MODE_LINEAR, false, double>(a, s);
-  }
-  if (dense) return precision ? launch_t<ET, MODE_TANGENT, true, float>(a, s) : launch_t<ET, MODE_TANGENT, true, double>(a, s);
-  return precision ? launch_t<ET, MODE_TANGENT, false, float>(a, s) : launch_t<ET, MODE_TANGENT, false, double>(a, s);
+  if (!dense) return cudaErrorNotSupported;  // CSR assembly is the two-pass path
+  if (mode == MODE_LINEAR)
+    return precision ? launch_t<ET, MODE_LINEAR, true, float>(a, s) : launch_t<ET, MODE_LINEAR, true, double>(a, s);
+  return precision ? launch_t<ET, MODE_TANGENT, true, float>(a, s) : launch_t<ET, MODE_TANGENT, true, double>(a, s);
 }
 
 __global__ void rhs_init_kernel(const int32_t* dof_eq, const double* f_ext, int64_t ndof, double* rhs) {

@@ -12,9 +12,10 @@
 //   3. node_base(a) = exclusive scan of (free rows of a) * rowlen(a); row_ptr and
 //      col_idx follow. This relies on the reference's free numbering being ascending
 //      in g = 3*node + comp (constraint_transform.cpp:78-82), which is validated;
-//   4. the slot map stores, per element and ordered node pair (a, b), the column
-//      offset of b inside a's rows (uint16), so the element kernel addresses
-//      vals[node_base(a) + r*rowlen(a) + slot + rank_b(j)] with no search.
+//   4. the adjacency (adj_ptr, adj_node: the neighbours of each node, ascending) is
+//      kept for the row gather, and the slot map stores, per element and ordered node
+//      pair (a, b), the position of b in a's adjacency list (uint16), so the gather
+//      adds block (a, b) into a's rows with no search.
 // The pattern is topological: an entry whose every element contribution is exactly
 // zero is kept (the reference skips exact-zero contributions, assembly.cpp:90).
 #include <cub/cub.cuh>
@@ -58,12 +59,6 @@ __global__ void check_numbering_kernel(const int32_t* dof_eq, const int32_t* sca
 
 // Free-component mask of every element node, so the row gather needs no connectivity
 // lookup before it knows which columns of a block exist.
-__global__ void conn_mask_kernel(const int32_t* conn, int64_t count, const uint8_t* node_mask, uint8_t* out) {
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    out[i] = node_mask[conn[i]];
-}
-
 __global__ void node_info_kernel(const int32_t* dof_eq, int64_t n_nodes, uint8_t* mask,
                                  int32_t* eq0) {
   for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a < n_nodes;
@@ -152,8 +147,7 @@ __global__ void col_idx_kernel(const uint64_t* uniq, int64_t M, uint64_t N, cons
 }
 
 __global__ void slot_kernel(const int32_t* conn, int64_t n_elems, int npe, uint64_t N,
-                            const uint64_t* uniq, const int64_t* node_ptr, const int32_t* adj_off,
-                            uint16_t* slot, int* overflow) {
+                            const uint64_t* uniq, const int64_t* node_ptr, uint16_t* slot, int* overflow) {
   const int64_t total = n_elems * npe * npe;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -169,10 +163,21 @@ __global__ void slot_kernel(const int32_t* conn, int64_t n_elems, int npe, uint6
       else
         hi = mid;
     }
-    const int32_t off = adj_off[lo];
-    if (off > 65535) atomicExch(overflow, 1);
-    slot[i] = static_cast<uint16_t>(off);
+    const int64_t pos = lo - node_ptr[na];
+    if (pos > 65535) atomicExch(overflow, 1);
+    slot[i] = static_cast<uint16_t>(pos);
   }
+}
+
+// adjacency list entries: column node of each (a, b) key, and the list length per node
+__global__ void adj_kernel(const uint64_t* uniq, int64_t M, uint64_t N, const int64_t* node_ptr, int64_t n_nodes,
+                           int32_t* adj_node, int64_t* adj_len) {
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < M;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    adj_node[t] = static_cast<int32_t>(uniq[t] % N);
+  for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a < n_nodes;
+       a += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    adj_len[a] = node_ptr[a + 1] - node_ptr[a];
 }
 
 __global__ void iota_kernel(int32_t* v, int64_t n) {
@@ -236,7 +241,6 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
   void* d_temp = nullptr;
   size_t temp_bytes = 0;
   int64_t* d_M = nullptr;
-  int64_t* d_node_ptr = nullptr;
   int32_t* d_adj_off = nullptr;
   int64_t* d_node_nnz = nullptr;
   int h_flag = 0;
@@ -340,12 +344,13 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
     uniq = other;
   }
 
-  CXG_TRY(dalloc(&d_node_ptr, n_nodes + 1, &scratch));
+  CXG_TRY(dalloc(&out->adj_ptr, n_nodes + 1, &out->device_bytes));
+  CXG_TRY(dalloc(&out->adj_node, M, &out->device_bytes));
   CXG_TRY(dalloc(&d_adj_off, M, &scratch));
   CXG_TRY(dalloc(&d_node_nnz, n_nodes, &scratch));
-  node_ptr_kernel<<<grid_for(n_nodes + 1), 256, 0, s>>>(uniq, M, n_nodes, N, d_node_ptr);
+  node_ptr_kernel<<<grid_for(n_nodes + 1), 256, 0, s>>>(uniq, M, n_nodes, N, out->adj_ptr);
   CXG_TRY(cudaGetLastError());
-  rowlen_kernel<<<grid_for(n_nodes), 256, 0, s>>>(uniq, d_node_ptr, n_nodes, N, out->node_mask,
+  rowlen_kernel<<<grid_for(n_nodes), 256, 0, s>>>(uniq, out->adj_ptr, n_nodes, N, out->node_mask,
                                                   out->node_rowlen, d_adj_off, d_node_nnz);
   CXG_TRY(cudaGetLastError());
   temp_bytes = 0;
@@ -365,10 +370,6 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
   CXG_TRY(dalloc(&out->row_ptr, static_cast<size_t>(n_free) + 1, &out->device_bytes));
   CXG_TRY(dalloc(&out->col_idx, static_cast<size_t>(out->nnz), &out->device_bytes));
   CXG_TRY(dalloc(&out->slot, static_cast<size_t>(P), &out->device_bytes));
-  CXG_TRY(dalloc(&out->conn_mask, static_cast<size_t>(n_elems) * npe, &out->device_bytes));
-  if (n_elems > 0)
-    conn_mask_kernel<<<grid_for(n_elems * npe), 256, 0, s>>>(d_conn, n_elems * npe, out->node_mask, out->conn_mask);
-  CXG_TRY(cudaGetLastError());
   row_ptr_kernel<<<grid_for(n_nodes), 256, 0, s>>>(n_nodes, out->node_mask, out->node_eq0, out->node_base,
                                                    out->node_rowlen, out->row_ptr);
   CXG_TRY(cudaGetLastError());
@@ -377,26 +378,34 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
                                              out->node_rowlen, d_adj_off, out->col_idx);
   CXG_TRY(cudaGetLastError());
   CXG_TRY(cudaMemsetAsync(d_flag, 0, sizeof(int), s));
-  slot_kernel<<<grid_for(P), 256, 0, s>>>(d_conn, n_elems, npe, N, uniq, d_node_ptr, d_adj_off, out->slot, d_flag);
+  slot_kernel<<<grid_for(P), 256, 0, s>>>(d_conn, n_elems, npe, N, uniq, out->adj_ptr, out->slot, d_flag);
   CXG_TRY(cudaGetLastError());
   CXG_TRY(cudaMemcpyAsync(&h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
   CXG_TRY(cudaStreamSynchronize(s));
   if (h_flag) {
-    *msg = "a CSR row holds more than 65535 columns; not supported";
+    *msg = "a node has more than 65535 neighbours; not supported";
     rc = 5;
     goto done;
   }
 
-  // largest per-node row block (free rows x row length): sizes the gather's buffers
+  // largest per-node row block (free rows x row length) and adjacency list: size the
+  // gather's buffers
   {
     int64_t* d_max = nullptr;
-    CXG_TRY(cudaMalloc(&d_max, sizeof(int64_t)));
+    CXG_TRY(cudaMalloc(&d_max, 2 * sizeof(int64_t)));
     temp_bytes = 0;
     CXG_TRY(cub::DeviceReduce::Max(nullptr, temp_bytes, d_node_nnz, d_max, static_cast<int>(n_nodes), s));
     CXG_TRY(cudaMalloc(&d_temp, temp_bytes));
     CXG_TRY(cub::DeviceReduce::Max(d_temp, temp_bytes, d_node_nnz, d_max, static_cast<int>(n_nodes), s));
-    CXG_TRY(cudaMemcpyAsync(&out->max_row, d_max, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    adj_kernel<<<grid_for(std::max<int64_t>(M, n_nodes)), 256, 0, s>>>(uniq, M, N, out->adj_ptr, n_nodes,
+                                                                       out->adj_node, d_node_nnz);
+    CXG_TRY(cudaGetLastError());
+    CXG_TRY(cub::DeviceReduce::Max(d_temp, temp_bytes, d_node_nnz, d_max + 1, static_cast<int>(n_nodes), s));
+    int64_t hm[2] = {0, 0};
+    CXG_TRY(cudaMemcpyAsync(hm, d_max, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     CXG_TRY(cudaStreamSynchronize(s));
+    out->max_row = n_nodes > 0 ? hm[0] : 0;
+    out->max_adj = n_nodes > 0 ? hm[1] : 0;
     cudaFree(d_max);
     cudaFree(d_temp);
     d_temp = nullptr;
@@ -436,7 +445,6 @@ done:
   cudaFree(d_keys);
   cudaFree(d_keys2);
   cudaFree(d_M);
-  cudaFree(d_node_ptr);
   cudaFree(d_adj_off);
   cudaFree(d_node_nnz);
   return rc;

@@ -110,7 +110,7 @@ __device__ __forceinline__ void store_block(R* dst, const R (&v)[9]) {
 }
 
 template <typename R>
-__device__ __forceinline__ void load_block(const R* src, double (&v)[9]) {
+__device__ __forceinline__ void load_block(const R* src, R (&v)[9]) {
   if constexpr (sizeof(R) == 8) {
     const double2* d = reinterpret_cast<const double2*>(src);
     const double2 a = __ldg(d), b = __ldg(d + 1), c = __ldg(d + 2), e = __ldg(d + 3), f = __ldg(d + 4);
@@ -797,24 +797,27 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 }
 
 // ---- P2: row gather ------------------------------------------------------------------
-// One warp per node a. Lanes form EG groups of GS lanes (GS = 16 for elements of at
-// most 16 nodes, else 32; 8 for the <= 8-node families in mixed precision); lane lb of
-// group s handles column node lb of incident element k + s, so EG elements are applied
-// per pass. Every group copy of the rows is zeroed and read once per node, which for the
-// short rows of the <= 8-node families in FP64 costs more shared-memory traffic than
-// the idle lanes of two 16-lane groups (measured: the FP64 C3D8 tangent gather is 10 %
-// faster with two groups than with four, the mixed one 3 % slower, so it keeps four).
-// Each group adds into its own copy of the node's rows
-// in shared memory (within one element every target is distinct, so plain adds, no
-// atomics); the copies are summed in a fixed order when the rows are stored. The
-// node's incident-element codes come in with one coalesced load per 32 elements and
-// are handed out by shuffles; the free-component mask of each column node comes from
-// the per-element-node mask array, so a pass waits for one round of independent loads.
-// The connectivity is read only for constrained columns. In mixed precision the
-// diagonal 3x3 block of node a is minus the FP64 sum of all off-diagonal FP32 blocks of
-// its element rows: every lane keeps a running sum of the blocks it adds, and one
-// butterfly over the warp per node forms the block, so rigid translations stay in the
-// null space of the assembled rows to FP64 accuracy.
+// One warp per node a. The node's three rows are staged in shared memory at full width:
+// row i holds 3 entries for each node of a's adjacency list (position s, from the
+// element slot map), every component, free or not. Lanes form EG groups of GS lanes
+// (GS = 16 for elements of at most 16 nodes, else 32; 8 for the <= 8-node families in
+// mixed precision); lane lb of group s handles column node lb of incident element
+// k + s, so EG elements are applied per pass, each group into its own copy of the rows
+// (within one element every target is distinct: plain adds, no atomics). The inner
+// loop is one block fetch and 9 adds per lane. Every group copy is zeroed and read once
+// per node, which for the short rows of the <= 8-node families in FP64 costs more
+// shared-memory traffic than the idle lanes of two 16-lane groups (measured: the FP64
+// C3D8 tangent gather is 10 % faster with two groups than with four). The epilogue
+// reads every staged entry as the sum of the group copies in group order, and
+//  - in mixed precision forms the diagonal block of node a as minus the FP64 sum of
+//    all off-diagonal FP32 blocks in its rows (27 lanes: 9 entries x 3 phases, added in
+//    a fixed order), so rigid translations stay in the null space of K to FP64 accuracy;
+//  - stores the free rows: interior nodes (every neighbour fully free) as staged, with
+//    coalesced writes; the others lane by neighbour, at the compressed columns a warp
+//    scan of the neighbours' free-component counts gives, moving the prescribed
+//    columns into the rhs (-K_fc u_c, src/fem/assembly.cpp:95-96).
+// The node's incident-element codes come in with one coalesced load per 32 elements and
+// are handed out by shuffles.
 template <int ET, bool DIAGFIX>
 struct P2Geo {
   static constexpr int n = nodes_of(ET);
@@ -822,12 +825,11 @@ struct P2Geo {
   static constexpr int EG = 32 / GS;
 };
 
-
 template <typename R>
 struct P2Pass {
   double v[9];
   int64_t e;
-  int la, mb, slotv;
+  int la, slotv;
   bool active;
 };
 
@@ -839,17 +841,15 @@ __device__ __forceinline__ void p2_fetch(const ElemArgs& A, const V2Args& V, con
   p.e = code / n;
   p.la = code % n;
   if (active) {
-    p.mb = __ldg(A.conn_mask + p.e * n + lb);
     p.slotv = __ldg(A.slot + (p.e * n + p.la) * n + lb);
     const bool tr = lb < p.la;
-    double raw[9];
+    R raw[9];
     load_block<R>(ed + (WIN ? ring_slot(p.e, V) : p.e) * (NB * blk_stride<R>()) +
                       (tr ? blk_index(n, lb, p.la) : blk_index(n, p.la, lb)) * blk_stride<R>(),
                   raw);
 #pragma unroll
-    for (int q = 0; q < 9; ++q) p.v[q] = tr ? raw[3 * (q % 3) + q / 3] : raw[q];
+    for (int q = 0; q < 9; ++q) p.v[q] = static_cast<double>(tr ? raw[3 * (q % 3) + q / 3] : raw[q]);
   } else {
-    p.mb = 0;
     p.slotv = 0;
 #pragma unroll
     for (int q = 0; q < 9; ++q) p.v[q] = 0.0;
@@ -860,9 +860,10 @@ template <int ET, bool TAN, typename R, bool DIAGFIX, bool WIN>
 __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   constexpr int n = nodes_of(ET);
   constexpr int GS = P2Geo<ET, DIAGFIX>::GS, EG = P2Geo<ET, DIAGFIX>::EG;
+  constexpr unsigned kAll = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int stride = static_cast<int>(V.row_stride);  // shared-memory offsets are 32-bit
+  const int stride = static_cast<int>(V.row_stride);  // doubles of one row-buffer copy
   double* buf = reinterpret_cast<double*>(smem) + warp * (EG * stride);
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
@@ -872,114 +873,157 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   double* mine = buf + sub * stride;
   // nodes [V.n_begin, V.n_end) of this window's node list (node_order, WIN), or of the mesh
   const int64_t n_begin = WIN ? V.n_begin : 0, n_end = WIN ? V.n_end : A.n_nodes;
+  // per-node scalars, all loaded at the node's start
+  struct NodeInfo {
+    int64_t a, j0, j1, i0, i1, base;
+    int ma, L;
+  };
+  auto node_info = [&](int64_t idx) {
+    NodeInfo t;
+    t.a = WIN ? static_cast<int64_t>(V.node_order[idx]) : idx;
+    t.ma = A.node_mask[t.a];
+    t.j0 = A.adj_ptr[t.a];
+    t.j1 = A.adj_ptr[t.a + 1];
+    t.i0 = V.inc_ptr[t.a];
+    t.i1 = V.inc_ptr[t.a + 1];
+    t.base = A.node_base[t.a];
+    t.L = static_cast<int>(A.node_rowlen[t.a]);
+    return t;
+  };
   for (int64_t idx = n_begin + gwarp; idx < n_end; idx += nwarps) {
-    const int64_t a = WIN ? static_cast<int64_t>(V.node_order[idx]) : idx;
-    const int ma = A.node_mask[a];
-    const int nf = __popc(ma);
-    const int L = static_cast<int>(A.node_rowlen[a]);
-    const int total = nf * L;
-    double* vout = A.vals + A.node_base[a];
-    const int64_t i0 = V.inc_ptr[a], i1 = V.inc_ptr[a + 1];
-    // offset of row i (free component i of node a) in the row buffer
-    int row_off[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) row_off[i] = __popc(ma & ((1 << i) - 1)) * L;
+    const NodeInfo cur_node = node_info(idx);
+    const int64_t a = cur_node.a;
+    const int ma = cur_node.ma;
+    const int64_t j0 = cur_node.j0;
+    const int K = static_cast<int>(cur_node.j1 - j0);  // neighbours, a itself included
+    const int W = 3 * K;                               // full-width row length
+    const int total = 3 * W;
+    const int64_t i0 = cur_node.i0, i1 = cur_node.i1;
+    const int L = cur_node.L;
     for (int g = 0; g < EG; ++g)
-      for (int t = lane; t < total; t += 32) buf[g * stride + t] = (g == 0 && V.accumulate) ? vout[t] : 0.0;
+      for (int t = lane; t < total; t += 32) buf[g * stride + t] = 0.0;
     __syncwarp();
-    double rr[3] = {0.0, 0.0, 0.0};
     double fs[3] = {0.0, 0.0, 0.0};
-    double dsum[9];  // this lane's FP64 sum of the off-diagonal blocks it added (DIAGFIX)
-#pragma unroll
-    for (int q = 0; q < 9; ++q) dsum[q] = 0.0;
-    int slot_aa = 0;  // column offset of node a in its own rows
+    int slot_aa = 0;  // position of node a in its own adjacency list (DIAGFIX)
     for (int64_t c0 = i0; c0 < i1; c0 += 32) {
       const int cnt = static_cast<int>(i1 - c0 < 32 ? i1 - c0 : 32);
       const int code_l = lane < cnt ? __ldg(V.inc_code + c0 + lane) : 0;
       for (int k = 0; k < cnt; k += EG) {
         P2Pass<R> cur;
-        p2_fetch<ET, R, WIN>(A, V, ed, __shfl_sync(0xffffffffu, code_l, (k + sub) & 31), lane_ok && k + sub < cnt, lb,
-                        cur);
+        p2_fetch<ET, R, WIN>(A, V, ed, __shfl_sync(kAll, code_l, (k + sub) & 31), lane_ok && k + sub < cnt, lb, cur);
         if (cur.active && (!DIAGFIX || lb != cur.la)) {
-          double* col = mine + cur.slotv;
-          if (cur.mb == 7) {  // every component of the column node is free
+          double* c = mine + 3 * cur.slotv;
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              if ((ma >> i) & 1) {
-                double* r = col + row_off[i];
-                r[0] += cur.v[3 * i];
-                r[1] += cur.v[3 * i + 1];
-                r[2] += cur.v[3 * i + 2];
-              }
-            }
-          } else {
-            int64_t nb = -1;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              if (!((ma >> i) & 1)) continue;
-#pragma unroll
-              for (int j = 0; j < 3; ++j) {
-                if ((cur.mb >> j) & 1) {
-                  col[row_off[i] + __popc(cur.mb & ((1 << j) - 1))] += cur.v[3 * i + j];
-                } else {
-                  if (nb < 0) nb = A.conn[cur.e * n + lb];
-                  const double pv = A.prescribed[3 * nb + j];
-                  if (pv != 0.0) rr[i] -= cur.v[3 * i + j] * pv;
-                }
-              }
-            }
+          for (int i = 0; i < 3; ++i) {
+            c[i * W] += cur.v[3 * i];
+            c[i * W + 1] += cur.v[3 * i + 1];
+            c[i * W + 2] += cur.v[3 * i + 2];
           }
         }
         if (TAN && cur.active && lb == cur.la) {
 #pragma unroll
           for (int d = 0; d < 3; ++d) fs[d] += __ldg(V.fdata + (WIN ? ring_slot(cur.e, V) : cur.e) * (3 * n) + 3 * cur.la + d);
         }
-        if (DIAGFIX && cur.active) {
-          if (lb != cur.la) {
-#pragma unroll
-            for (int q = 0; q < 9; ++q) dsum[q] += cur.v[q];
-          } else {
-            slot_aa = cur.slotv;  // slot(la, la)
-          }
-        }
+        if (DIAGFIX && cur.active && lb == cur.la) slot_aa = cur.slotv;
         __syncwarp();
       }
     }
+    // staged entry t: the group copies summed in group order
+    auto staged = [&](int t) {
+      double v = buf[t];
+#pragma unroll
+      for (int g = 1; g < EG; ++g) v += buf[g * stride + t];
+      return v;
+    };
     if (DIAGFIX) {
-      // diagonal block of node a: minus the FP64 sum of every off-diagonal FP32 block
-      // added to its rows, reduced over the warp in a fixed order
-      double d9[9];
+      // diagonal block of node a: minus the FP64 sum of every off-diagonal block in its
+      // rows; lane l sums the blocks of neighbours l, l + 32, ..., then a butterfly
+      // (the same bits on every lane)
+      slot_aa = static_cast<int>(__reduce_max_sync(kAll, static_cast<unsigned>(slot_aa)));
+      double d[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int s = lane; s < K; s += 32) {
+        if (s == slot_aa) continue;
 #pragma unroll
-      for (int q = 0; q < 9; ++q) {
-        double x = dsum[q];
+        for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
-        d9[q] = -x;
+          for (int j = 0; j < 3; ++j) d[3 * i + j] += staged(i * W + 3 * s + j);
       }
-      slot_aa = static_cast<int>(__reduce_max_sync(0xffffffffu, static_cast<unsigned>(slot_aa)));
+#pragma unroll
+      for (int q = 0; q < 9; ++q)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) d[q] += __shfl_xor_sync(kAll, d[q], off);
       if (lane < 9 && i1 > i0) {
-        const int i = lane / 3, j = lane % 3;
-        double d = d9[0];
+        double dq = d[0];
 #pragma unroll
         for (int q = 1; q < 9; ++q)
-          if (q == lane) d = d9[q];
-        if ((ma >> i) & 1) {
-          if ((ma >> j) & 1) {
-            const int ro = i == 0 ? row_off[0] : (i == 1 ? row_off[1] : row_off[2]);
-            buf[ro + slot_aa + __popc(ma & ((1 << j) - 1))] += d;
-          } else {
-            const double pv = A.prescribed[3 * a + j];
-            if (pv != 0.0) rr[i] -= d * pv;
+          if (q == lane) dq = d[q];
+        buf[(lane / 3) * W + 3 * slot_aa + lane % 3] = -dq;
+      }
+      __syncwarp();
+    }
+    // Interior nodes (every neighbour fully free, L == W) store the staged rows as they
+    // are, coalesced. At the others each lane takes a neighbour: a warp scan of the
+    // neighbours' free-component counts gives its first compressed column, its free
+    // columns are stored there and its prescribed columns go to the rhs.
+    double rr[3] = {0.0, 0.0, 0.0};
+    double* orow0 = A.vals + cur_node.base;
+    if (L == W) {
+      double* orow = orow0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        if (!((ma >> i) & 1)) continue;
+        for (int c = lane; c < L; c += 32) {
+          const double v = staged(i * W + c);
+          orow[c] = V.accumulate ? orow[c] + v : v;
+        }
+        orow += L;
+      }
+    } else {
+      int carry = 0;
+      for (int s0 = 0; s0 < K; s0 += 32) {
+        const int s = s0 + lane;
+        const bool ok = s < K;
+        const int b = ok ? __ldg(A.adj_node + j0 + s) : 0;
+        const int mb = ok ? static_cast<int>(A.node_mask[b]) : 0;
+        const int pc = __popc(mb);
+        int incl = pc;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const int y = __shfl_up_sync(kAll, incl, off);
+          if (lane >= off) incl += y;
+        }
+        const int c = carry + incl - pc;
+        carry += __shfl_sync(kAll, incl, 31);
+        if (ok) {
+#pragma unroll
+          for (int jj = 0; jj < 3; ++jj) {
+            if ((mb >> jj) & 1) {
+              const int col = c + __popc(mb & ((1 << jj) - 1));
+              int ri = 0;
+#pragma unroll
+              for (int i = 0; i < 3; ++i) {
+                if (!((ma >> i) & 1)) continue;
+                double* o = orow0 + static_cast<int64_t>(ri) * L + col;
+                const double v = staged(i * W + 3 * s + jj);
+                *o = V.accumulate ? *o + v : v;
+                ++ri;
+              }
+            } else {
+              const double pv = A.prescribed[3 * static_cast<int64_t>(b) + jj];
+              if (pv != 0.0) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) rr[i] -= staged(i * W + 3 * s + jj) * pv;
+              }
+            }
           }
         }
       }
-      __syncwarp();
     }
     if (A.rhs) {
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         double v = rr[r];
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kAll, v, off);
         if (lane == 0 && ((ma >> r) & 1)) {
           const int64_t eq = A.node_eq0[a] + __popc(ma & ((1 << r) - 1));
           const double prev = V.accumulate ? A.rhs[eq] : (V.f_ext ? V.f_ext[3 * a + r] : 0.0);
@@ -991,33 +1035,19 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         double v = fs[d];
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kAll, v, off);
         if (lane == 0) A.f_int[3 * a + d] = (V.accumulate ? A.f_int[3 * a + d] : 0.0) + v;
       }
-    }
-    for (int t = lane; t < total; t += 32) {
-      double v = buf[t];
-#pragma unroll
-      for (int g = 1; g < EG; ++g) v += buf[g * stride + t];
-      vout[t] = v;
     }
     __syncwarp();
   }
 }
 
-// Blocks of at most 8 warps. The mixed-precision gathers (all but the tangent gather of
-// the > 8-node families, which needs more registers) are compiled for 3 resident blocks
-// per SM (<= 85 registers), which their rows leave room for in shared memory; the other
-// gathers are compiled without a register budget.
+// Blocks of at most 8 warps, compiled without a register budget (48-72 registers).
 // WIN: the windowed schedule (node list and element ring); the one-window gather is
 // compiled without either, so it keeps the registers of a plain node loop.
 template <int ET, bool TAN, typename R, bool DIAGFIX, bool WIN>
 __global__ void p2_kernel(ElemArgs A, V2Args V) {
-  p2_body<ET, TAN, R, DIAGFIX, WIN>(A, V);
-}
-
-template <int ET, bool TAN, typename R, bool DIAGFIX, bool WIN>
-__global__ void __launch_bounds__(256, 3) p2_kernel_short(ElemArgs A, V2Args V) {
   p2_body<ET, TAN, R, DIAGFIX, WIN>(A, V);
 }
 
@@ -1068,12 +1098,12 @@ cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg
 
 template <int ET, bool TAN, typename R, bool DF>
 cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaStream_t s) {
-  constexpr bool kShort = DF && (nodes_of(ET) <= 8 || !TAN);
-  auto kern = v.node_order ? (kShort ? p2_kernel_short<ET, TAN, R, DF, true> : p2_kernel<ET, TAN, R, DF, true>)
-                           : (kShort ? p2_kernel_short<ET, TAN, R, DF, false> : p2_kernel<ET, TAN, R, DF, false>);
+  auto kern = v.node_order ? p2_kernel<ET, TAN, R, DF, true> : p2_kernel<ET, TAN, R, DF, false>;
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
-  // configured count when it fits)
-  const int64_t stride = std::max<int64_t>(2, (v.max_row + 1) / 2 * 2);
+  // configured count when it fits). Per warp: EG full-width copies of three rows of
+  // 3 x max_adj doubles. (Shared memory beyond that comes out of the L1 cache the
+  // scattered block loads reuse.)
+  const int64_t stride = std::max<int64_t>(2, (9 * v.max_adj + 1) / 2 * 2);
   const int64_t wbytes = P2Geo<ET, DF>::EG * stride * 8;
   int warps = cfg.p2_warps > 0 ? std::min(cfg.p2_warps, 8) : 8;
   while (warps > 1 && warps * wbytes > 160 * 1024) warps /= 2;
