@@ -192,6 +192,11 @@ class Plan:
         1 = 2x2, 2 = 4x4. Results do not depend on it."""
         _lib.check(self.lib.cxg_plan_set_launch_config(self.h, int(tangent), tile, p1_blocks_per_sm, p2_warps))
 
+    def set_j2_fp32_return(self, enable=True):
+        """Mixed precision, material-point assembly: the J2 return in FP32 (FP64 near the
+        yield surface) instead of FP64 (cxg_plan_set_j2_fp32_return)."""
+        _lib.check(self.lib.cxg_plan_set_j2_fp32_return(self.h, int(bool(enable))))
+
     def set_ring_bytes(self, nbytes: int):
         """Element-buffer budget of the windowed assembly (cxg_plan_set_ring_bytes):
         0 or < 0 = one window over the whole mesh, > 0 = windows whose buffers fit."""

@@ -691,6 +691,12 @@ int cxg_plan_set_launch_config(cxg_plan* p, int32_t mode, int32_t tile, int32_t 
   return CXG_OK;
 }
 
+int cxg_plan_set_j2_fp32_return(cxg_plan* p, int32_t enable) {
+  if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
+  p->tcfg[CXG_MIXED].j2_fp32 = enable ? 1 : 0;
+  return CXG_OK;
+}
+
 int cxg_plan_set_ring_bytes(cxg_plan* p, int64_t bytes) {
   if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
   if (p->last_stream) CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");

@@ -132,6 +132,9 @@ struct LaunchCfg {
   int p2_warps = 0;
   int p2_blocks_per_sm = 0;
   int passes = 3;
+  // mixed-precision material-point pass: the J2 return in FP32 (j2_point_mixed) instead
+  // of FP64
+  int j2_fp32 = 0;
 };
 size_t v2_edata_bytes(int elem_type, int64_t n_elems, int precision);
 // Bytes of element buffer per element (blocks, plus the internal force in tangent mode).

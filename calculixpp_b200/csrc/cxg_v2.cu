@@ -422,7 +422,9 @@ constexpr int p1_min_blocks() {
   return by_smem < 1 ? 1 : (by_smem > cap ? cap : by_smem);
 }
 
-template <int ET, int MODE, typename R, int TILE>
+// J2F32 (mixed-precision material-point pass only): the J2 return in FP32
+// (j2_point_mixed) instead of FP64.
+template <int ET, int MODE, typename R, int TILE, bool J2F32>
 __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_kernel(ElemArgs A, V2Args V) {
   using G = Geo<ET, TILE>;
   constexpr int n = G::n, nq = G::nq, npad = G::npad, EPW = G::EPW, NT = G::NT, NB = G::NB;
@@ -542,8 +544,8 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
           for (int c = 7; c < kStateDoubles; ++c) cs[c] = 0.0;
         }
         double lt, mt, ct, mhg;
-        // FP64 return in the FP64 path; FP32 (with the FP64 band near yield) in mixed precision
-        const int r = sizeof(R) == 8 ? kJ2Fp64
+        // FP64 return, or with J2F32 the FP32 return (with the FP64 band near yield)
+        const int r = (sizeof(R) == 8 || !J2F32) ? kJ2Fp64
                                      : j2_point_mixed(A.mats[mat], W.lam[ei], W.mu[ei], W.mu_j2[ei], eps, cs, ts, sig,
                                                       lt, mt, ct, nv, mhg);
         const bool pl = r == kJ2Fp64
@@ -800,14 +802,13 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 // One warp per node a. The node's three rows are staged in shared memory at full width:
 // row i holds 3 entries for each node of a's adjacency list (position s, from the
 // element slot map), every component, free or not. Lanes form EG groups of GS lanes
-// (GS = 16 for elements of at most 16 nodes, else 32; 8 for the <= 8-node families in
-// mixed precision); lane lb of group s handles column node lb of incident element
+// (GS = 16 for elements of at most 16 nodes, else 32); lane lb of group s handles column node lb of incident element
 // k + s, so EG elements are applied per pass, each group into its own copy of the rows
 // (within one element every target is distinct: plain adds, no atomics). The inner
 // loop is one block fetch and 9 adds per lane. Every group copy is zeroed and read once
-// per node, which for the short rows of the <= 8-node families in FP64 costs more
-// shared-memory traffic than the idle lanes of two 16-lane groups (measured: the FP64
-// C3D8 tangent gather is 10 % faster with two groups than with four). The epilogue
+// per node, which for the short rows of the <= 8-node families costs more shared-memory
+// traffic than the idle lanes of two 16-lane groups (measured on the C3D8 tangent
+// gather, two groups against four: FP64 10 %, mixed 12 % faster). The epilogue
 // reads every staged entry as the sum of the group copies in group order, and
 //  - in mixed precision forms the diagonal block of node a as minus the FP64 sum of
 //    all off-diagonal FP32 blocks in its rows (27 lanes: 9 entries x 3 phases, added in
@@ -821,7 +822,7 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
 template <int ET, bool DIAGFIX>
 struct P2Geo {
   static constexpr int n = nodes_of(ET);
-  static constexpr int GS = (DIAGFIX && n <= 8) ? 8 : (n <= 16 ? 16 : 32);
+  static constexpr int GS = n <= 16 ? 16 : 32;
   static constexpr int EG = 32 / GS;
 };
 
@@ -1069,7 +1070,10 @@ template <int ET, int MODE, typename R, int TILE>
 cudaError_t launch_p1_tile(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg, cudaStream_t s) {
   constexpr size_t smem = p1_smem_bytes<ET, MODE, R, TILE>();
   static_assert(smem <= 227 * 1024, "element pass shared memory");
-  auto kern = p1_kernel<ET, MODE, R, TILE>;
+  auto kern = p1_kernel<ET, MODE, R, TILE, false>;
+  if constexpr (MODE == MODE_TANGENT && sizeof(R) == 4) {
+    if (cfg.j2_fp32) kern = p1_kernel<ET, MODE, R, TILE, true>;
+  }
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (err != cudaSuccess) return err;
   int per_sm = 0;

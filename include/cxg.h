@@ -174,6 +174,14 @@ CXG_API int cxg_plan_update_young(cxg_plan* plan, const double* young);
  * do not depend on the shape. */
 CXG_API int cxg_plan_set_launch_config(cxg_plan* plan, int32_t mode, int32_t tile, int32_t p1_blocks_per_sm,
                                        int32_t p2_warps);
+/* No counterpart in the reference. Mixed-precision material-point assembly: enable != 0
+ * runs the J2 return (src/fem/plasticity.cpp:90-236: trial stress, local Newton on the
+ * plastic multiplier, stress and history update, tangent parameters) in FP32, with the
+ * FP64 return for points whose consistency scalar lies within 1e-3 sigma_y of the yield
+ * surface and for points whose FP32 Newton does not settle; 0 (default) keeps the FP64
+ * return with FP32 tangent blocks, which measured faster on the B200 (the element pass
+ * is not bound by its arithmetic) and keeps the history bit-for-bit FP64. */
+CXG_API int cxg_plan_set_j2_fp32_return(cxg_plan* plan, int32_t enable);
 /* No counterpart in the reference (a tuning knob of this library). Device-memory
  * budget of the element buffers that carry K_e blocks from the element pass to the
  * row gather. The assembly runs in windows of consecutive elements, each followed by

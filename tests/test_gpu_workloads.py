@@ -4,7 +4,9 @@ at sizes the oracle finishes in seconds:
 * the J2 Newton workload (C3D8 block, graded uniaxial ramp, `c3d8_j2_block` +
   `j2_increment`) through all 10 increments with a commit after each: FP64 tangent and
   f_int within 1e-12 relative, J2 history within 1e-10 per Gauss point; the mixed path's
-  K and f_int against the same oracle within 1e-6;
+  K and f_int against the same oracle within 1e-6, its history (FP64 return) equal to
+  the FP64 path's bit for bit, and with the FP32 return K and f_int within 1e-6 and the
+  history within 1e-5 of its magnitude;
 * the C3D20 block (`c3d20_block`, lognormal E): CSR pattern bit-exact, FP64 values within
   1e-12, displacements within 1e-10 after the same direct solve; mixed displacements
   within 1e-6 of the oracle's;
@@ -62,6 +64,8 @@ def test_j2_workload_ramp(cuda, port):
     model = Model(m, mats_dev, None, spc1, None)
     plan64 = Plan(model, "fp64")
     planmx = Plan(model, "mixed")
+    planf32 = Plan(model, "mixed")
+    planf32.set_j2_fp32_return(True)
     mats, em = per_element_materials(model)
     dof_eq, pre, nf = model.dof_map()
     committed = np.zeros(plan64.n_gauss * 13)
@@ -76,8 +80,16 @@ def test_j2_workload_ramp(cuda, port):
         vmx, fmx, _ = planmx.assemble_tangent(u)
         assert rel_fro(_on_oracle_pattern(planmx, vmx, rp, ci), vo) <= 1e-6, k
         assert rel_fro(to_np(fmx), fo) <= 1e-6, k
+        assert np.array_equal(to_np(planmx.state(committed=False)).reshape(-1), s64), k
+        vf, ff, _ = planf32.assemble_tangent(u)
+        assert rel_fro(_on_oracle_pattern(planf32, vf, rp, ci), vo) <= 1e-6, k
+        assert rel_fro(to_np(ff), fo) <= 1e-6, k
+        sf = to_np(planf32.state(committed=False)).reshape(-1)
+        # FP32 Newton increments: ~1e-6 relative error of the increment
+        assert np.abs(sf - so).max() <= 1e-5 * max(np.abs(so).max(), 1e-12), k
         plan64.commit()
         planmx.commit()
+        planf32.commit()
         committed = so
     yielded = np.mean(committed.reshape(-1, 13)[:, 6] > 0)
     assert 0.2 < yielded < 0.6, yielded  # the ramp yields part of the block (~40 % at full size)
