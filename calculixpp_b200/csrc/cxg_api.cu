@@ -375,8 +375,9 @@ ElemArgs base_args(cxg_plan* p) {
   a.node_eq0 = p->pat.node_eq0;
   a.prescribed = p->prescribed;
   a.slot = p->pat.slot;
-  a.adj_ptr = p->pat.adj_ptr;
-  a.adj_node = p->pat.adj_node;
+  a.adj_len = p->pat.adj_len;
+  a.bnd_ptr = p->pat.bnd_ptr;
+  a.bnd_node = p->pat.bnd_node;
   a.n_gauss = p->n_gauss;
   a.status = p->status;
   return a;
@@ -600,7 +601,7 @@ int cxg_plan_destroy(cxg_plan* p) {
   if (p->last_stream) cudaStreamSynchronize(p->last_stream);
   void* bufs[] = {p->coords, p->conn, p->young, p->poisson, p->elem_mat, p->mats, p->dof_eq, p->prescribed,
                   p->pat.row_ptr, p->pat.col_idx, p->pat.node_base, p->pat.node_rowlen, p->pat.node_mask,
-                  p->pat.node_eq0, p->pat.slot, p->pat.adj_ptr, p->pat.adj_node, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
+                  p->pat.node_eq0, p->pat.slot, p->pat.adj_len, p->pat.bnd_ptr, p->pat.bnd_node, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
                   p->status, p->edata, p->fdata};
   for (void* b : bufs) cudaFree(b);
   for (auto& row : p->sched)

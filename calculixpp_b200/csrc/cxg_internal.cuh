@@ -75,8 +75,9 @@ struct ElemArgs {
   const int32_t* node_eq0;    // [N] first free equation of the node (or -1)
   const double* prescribed;   // [3N]
   const uint16_t* slot;       // [E*n*n] position of node b in node a's adjacency list
-  const int64_t* adj_ptr;     // [N+1] node adjacency (row gather)
-  const int32_t* adj_node;    // [M]
+  const uint16_t* adj_len;    // [N] adjacency list length (row gather)
+  const int64_t* bnd_ptr;     // [N+1] adjacency of the compressed-row nodes
+  const int32_t* bnd_node;
   // state (tangent mode), SoA [13][G]
   const double* state_c;
   double* state_t;
@@ -224,10 +225,12 @@ struct PatternOut {
   uint8_t* node_mask = nullptr;
   int32_t* node_eq0 = nullptr;
   uint16_t* slot = nullptr;     // [E*n*n] position of node b in node a's adjacency list
-  // node adjacency: neighbours of node a (itself included, ascending) are
-  // adj_node[adj_ptr[a] .. adj_ptr[a+1])
-  int64_t* adj_ptr = nullptr;   // [N+1]
-  int32_t* adj_node = nullptr;  // [M]
+  // node adjacency (neighbours of a node, itself included, ascending): the list length
+  // of every node, and the list itself for the nodes with a neighbour that is not fully
+  // free (bnd_node[bnd_ptr[a] .. bnd_ptr[a+1]); empty for the others)
+  uint16_t* adj_len = nullptr;  // [N]
+  int64_t* bnd_ptr = nullptr;   // [N+1]
+  int32_t* bnd_node = nullptr;
   // node -> incident elements, ascending element order: codes e*n + local node index
   int64_t* inc_ptr = nullptr;   // [N+1]
   int32_t* inc_code = nullptr;  // [E*n]

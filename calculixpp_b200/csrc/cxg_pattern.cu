@@ -12,10 +12,11 @@
 //   3. node_base(a) = exclusive scan of (free rows of a) * rowlen(a); row_ptr and
 //      col_idx follow. This relies on the reference's free numbering being ascending
 //      in g = 3*node + comp (constraint_transform.cpp:78-82), which is validated;
-//   4. the adjacency (adj_ptr, adj_node: the neighbours of each node, ascending) is
-//      kept for the row gather, and the slot map stores, per element and ordered node
-//      pair (a, b), the position of b in a's adjacency list (uint16), so the gather
-//      adds block (a, b) into a's rows with no search.
+//   4. the slot map stores, per element and ordered node pair (a, b), the position of b
+//      in a's adjacency list (uint16), so the row gather adds block (a, b) into a's
+//      rows with no search; the gather keeps the list length of every node (adj_len)
+//      and, for the nodes with a neighbour that is not fully free (their rows are
+//      compressed), the neighbours themselves (bnd_ptr, bnd_node).
 // The pattern is topological: an entry whose every element contribution is exactly
 // zero is kept (the reference skips exact-zero contributions, assembly.cpp:90).
 #include <cub/cub.cuh>
@@ -164,20 +165,33 @@ __global__ void slot_kernel(const int32_t* conn, int64_t n_elems, int npe, uint6
         hi = mid;
     }
     const int64_t pos = lo - node_ptr[na];
-    if (pos > 65535) atomicExch(overflow, 1);
+    if (pos > 65534) atomicExch(overflow, 1);  // list lengths are uint16
     slot[i] = static_cast<uint16_t>(pos);
   }
 }
 
-// adjacency list entries: column node of each (a, b) key, and the list length per node
-__global__ void adj_kernel(const uint64_t* uniq, int64_t M, uint64_t N, const int64_t* node_ptr, int64_t n_nodes,
-                           int32_t* adj_node, int64_t* adj_len) {
-  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < M;
-       t += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    adj_node[t] = static_cast<int32_t>(uniq[t] % N);
+// adjacency list length per node (uint16, and int64 for the max reduction), and the
+// list length again for the nodes whose rows are compressed (row length != 3 x list
+// length), 0 for the others
+__global__ void adj_len_kernel(const int64_t* node_ptr, const int32_t* rowlen, int64_t n_nodes, uint16_t* adj_len,
+                               int64_t* len64, int64_t* bnd_len) {
   for (int64_t a = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; a < n_nodes;
-       a += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    adj_len[a] = node_ptr[a + 1] - node_ptr[a];
+       a += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t k = node_ptr[a + 1] - node_ptr[a];
+    adj_len[a] = static_cast<uint16_t>(k);
+    len64[a] = k;
+    bnd_len[a] = rowlen[a] == 3 * k ? 0 : k;
+  }
+}
+
+// neighbours of the compressed-row nodes, in list order
+__global__ void bnd_node_kernel(const uint64_t* uniq, int64_t M, uint64_t N, const int64_t* node_ptr,
+                                const int64_t* bnd_ptr, int32_t* bnd_node) {
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < M;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t a = static_cast<int64_t>(uniq[t] / N);
+    if (bnd_ptr[a + 1] > bnd_ptr[a]) bnd_node[bnd_ptr[a] + (t - node_ptr[a])] = static_cast<int32_t>(uniq[t] % N);
+  }
 }
 
 __global__ void iota_kernel(int32_t* v, int64_t n) {
@@ -241,6 +255,7 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
   void* d_temp = nullptr;
   size_t temp_bytes = 0;
   int64_t* d_M = nullptr;
+  int64_t* d_node_ptr = nullptr;
   int32_t* d_adj_off = nullptr;
   int64_t* d_node_nnz = nullptr;
   int h_flag = 0;
@@ -344,13 +359,12 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
     uniq = other;
   }
 
-  CXG_TRY(dalloc(&out->adj_ptr, n_nodes + 1, &out->device_bytes));
-  CXG_TRY(dalloc(&out->adj_node, M, &out->device_bytes));
+  CXG_TRY(dalloc(&d_node_ptr, n_nodes + 1, &scratch));
   CXG_TRY(dalloc(&d_adj_off, M, &scratch));
   CXG_TRY(dalloc(&d_node_nnz, n_nodes, &scratch));
-  node_ptr_kernel<<<grid_for(n_nodes + 1), 256, 0, s>>>(uniq, M, n_nodes, N, out->adj_ptr);
+  node_ptr_kernel<<<grid_for(n_nodes + 1), 256, 0, s>>>(uniq, M, n_nodes, N, d_node_ptr);
   CXG_TRY(cudaGetLastError());
-  rowlen_kernel<<<grid_for(n_nodes), 256, 0, s>>>(uniq, out->adj_ptr, n_nodes, N, out->node_mask,
+  rowlen_kernel<<<grid_for(n_nodes), 256, 0, s>>>(uniq, d_node_ptr, n_nodes, N, out->node_mask,
                                                   out->node_rowlen, d_adj_off, d_node_nnz);
   CXG_TRY(cudaGetLastError());
   temp_bytes = 0;
@@ -378,7 +392,7 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
                                              out->node_rowlen, d_adj_off, out->col_idx);
   CXG_TRY(cudaGetLastError());
   CXG_TRY(cudaMemsetAsync(d_flag, 0, sizeof(int), s));
-  slot_kernel<<<grid_for(P), 256, 0, s>>>(d_conn, n_elems, npe, N, uniq, out->adj_ptr, out->slot, d_flag);
+  slot_kernel<<<grid_for(P), 256, 0, s>>>(d_conn, n_elems, npe, N, uniq, d_node_ptr, out->slot, d_flag);
   CXG_TRY(cudaGetLastError());
   CXG_TRY(cudaMemcpyAsync(&h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
   CXG_TRY(cudaStreamSynchronize(s));
@@ -388,25 +402,45 @@ int build_pattern(int elem_type, int64_t n_nodes, int64_t n_elems, const int32_t
     goto done;
   }
 
-  // largest per-node row block (free rows x row length) and adjacency list: size the
-  // gather's buffers
+  // largest per-node row block (free rows x row length) and adjacency list (they size
+  // the gather's buffers); list lengths, and the neighbours of the compressed-row nodes
   {
     int64_t* d_max = nullptr;
+    int64_t* d_bnd_len = nullptr;
     CXG_TRY(cudaMalloc(&d_max, 2 * sizeof(int64_t)));
+    CXG_TRY(cudaMalloc(&d_bnd_len, sizeof(int64_t) * static_cast<size_t>(std::max<int64_t>(n_nodes, 1))));
     temp_bytes = 0;
     CXG_TRY(cub::DeviceReduce::Max(nullptr, temp_bytes, d_node_nnz, d_max, static_cast<int>(n_nodes), s));
+    size_t scan_bytes = 0;
+    CXG_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, d_bnd_len, d_bnd_len, static_cast<int>(n_nodes) + 1, s));
+    temp_bytes = std::max(temp_bytes, scan_bytes);
     CXG_TRY(cudaMalloc(&d_temp, temp_bytes));
     CXG_TRY(cub::DeviceReduce::Max(d_temp, temp_bytes, d_node_nnz, d_max, static_cast<int>(n_nodes), s));
-    adj_kernel<<<grid_for(std::max<int64_t>(M, n_nodes)), 256, 0, s>>>(uniq, M, N, out->adj_ptr, n_nodes,
-                                                                       out->adj_node, d_node_nnz);
+    CXG_TRY(dalloc(&out->adj_len, n_nodes, &out->device_bytes));
+    CXG_TRY(dalloc(&out->bnd_ptr, n_nodes + 1, &out->device_bytes));
+    adj_len_kernel<<<grid_for(n_nodes), 256, 0, s>>>(d_node_ptr, out->node_rowlen, n_nodes, out->adj_len, d_node_nnz,
+                                                     d_bnd_len);
     CXG_TRY(cudaGetLastError());
     CXG_TRY(cub::DeviceReduce::Max(d_temp, temp_bytes, d_node_nnz, d_max + 1, static_cast<int>(n_nodes), s));
-    int64_t hm[2] = {0, 0};
+    CXG_TRY(cudaMemsetAsync(out->bnd_ptr + n_nodes, 0, sizeof(int64_t), s));
+    CXG_TRY(cub::DeviceScan::ExclusiveSum(d_temp, temp_bytes, d_bnd_len, out->bnd_ptr, static_cast<int>(n_nodes), s));
+    int64_t hm[2] = {0, 0}, last[2] = {0, 0};
     CXG_TRY(cudaMemcpyAsync(hm, d_max, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    if (n_nodes > 0) {
+      CXG_TRY(cudaMemcpyAsync(&last[0], out->bnd_ptr + n_nodes - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      CXG_TRY(cudaMemcpyAsync(&last[1], d_bnd_len + n_nodes - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    }
+    CXG_TRY(cudaStreamSynchronize(s));
+    const int64_t n_bnd = last[0] + last[1];
+    CXG_TRY(cudaMemcpyAsync(out->bnd_ptr + n_nodes, &n_bnd, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    CXG_TRY(dalloc(&out->bnd_node, n_bnd, &out->device_bytes));
+    bnd_node_kernel<<<grid_for(M), 256, 0, s>>>(uniq, M, N, d_node_ptr, out->bnd_ptr, out->bnd_node);
+    CXG_TRY(cudaGetLastError());
     CXG_TRY(cudaStreamSynchronize(s));
     out->max_row = n_nodes > 0 ? hm[0] : 0;
     out->max_adj = n_nodes > 0 ? hm[1] : 0;
     cudaFree(d_max);
+    cudaFree(d_bnd_len);
     cudaFree(d_temp);
     d_temp = nullptr;
   }
@@ -445,6 +479,7 @@ done:
   cudaFree(d_keys);
   cudaFree(d_keys2);
   cudaFree(d_M);
+  cudaFree(d_node_ptr);
   cudaFree(d_adj_off);
   cudaFree(d_node_nnz);
   return rc;

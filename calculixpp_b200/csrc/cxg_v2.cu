@@ -876,15 +876,14 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   const int64_t n_begin = WIN ? V.n_begin : 0, n_end = WIN ? V.n_end : A.n_nodes;
   // per-node scalars, all loaded at the node's start
   struct NodeInfo {
-    int64_t a, j0, j1, i0, i1, base;
-    int ma, L;
+    int64_t a, i0, i1, base;
+    int ma, L, K;
   };
   auto node_info = [&](int64_t idx) {
     NodeInfo t;
     t.a = WIN ? static_cast<int64_t>(V.node_order[idx]) : idx;
     t.ma = A.node_mask[t.a];
-    t.j0 = A.adj_ptr[t.a];
-    t.j1 = A.adj_ptr[t.a + 1];
+    t.K = A.adj_len[t.a];
     t.i0 = V.inc_ptr[t.a];
     t.i1 = V.inc_ptr[t.a + 1];
     t.base = A.node_base[t.a];
@@ -895,8 +894,7 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
     const NodeInfo cur_node = node_info(idx);
     const int64_t a = cur_node.a;
     const int ma = cur_node.ma;
-    const int64_t j0 = cur_node.j0;
-    const int K = static_cast<int>(cur_node.j1 - j0);  // neighbours, a itself included
+    const int K = cur_node.K;  // neighbours, a itself included
     const int W = 3 * K;                               // full-width row length
     const int total = 3 * W;
     const int64_t i0 = cur_node.i0, i1 = cur_node.i1;
@@ -980,11 +978,12 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
         orow += L;
       }
     } else {
+      const int32_t* nbr = A.bnd_node + A.bnd_ptr[a];
       int carry = 0;
       for (int s0 = 0; s0 < K; s0 += 32) {
         const int s = s0 + lane;
         const bool ok = s < K;
-        const int b = ok ? __ldg(A.adj_node + j0 + s) : 0;
+        const int b = ok ? __ldg(nbr + s) : 0;
         const int mb = ok ? static_cast<int>(A.node_mask[b]) : 0;
         const int pc = __popc(mb);
         int incl = pc;
