@@ -1123,11 +1123,12 @@ error:
   return NULL;
 }
 
-/* ---- field recovery: src/fem/stress.cpp (elastic, no thermal strain) ------------- */
-/* strain_stress_at, stress.cpp:19-42 (eps_th = 0): du[i][j] = sum_k g_k[j] u_k[i],
- * engineering strain, sigma = D eps. */
-static void strain_stress_at(const double* g, int n, const double* ue, const double* D, double* strain,
+/* ---- field recovery and thermal strain: src/fem/stress.cpp, src/fem/loads.cpp ---- */
+/* strain_stress_at, stress.cpp:19-42: du[i][j] = sum_k g_k[j] u_k[i], engineering strain,
+ * sigma = D (eps - eps_th) with eps_th = {eth, eth, eth, 0, 0, 0}. */
+static void strain_stress_at(const double* g, int n, const double* ue, const double* D, double eth, double* strain,
                              double* stress) {
+  const double eps_th[6] = {eth, eth, eth, 0.0, 0.0, 0.0};
   double du[3][3];
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) {
@@ -1143,7 +1144,7 @@ static void strain_stress_at(const double* g, int n, const double* ue, const dou
   strain[5] = du[1][2] + du[2][1];
   for (int i = 0; i < 6; ++i) {
     double v = 0.0;
-    for (int j = 0; j < 6; ++j) v += D[6 * i + j] * (strain[j] - 0.0);
+    for (int j = 0; j < 6; ++j) v += D[6 * i + j] * (strain[j] - eps_th[j]);
     stress[i] = v;
   }
 }
@@ -1160,37 +1161,118 @@ static int gather_element(int64_t n_nodes, const double* coords, const int32_t* 
   return 0;
 }
 
+/* Thermal-strain inputs of one element (NULL node_temp: none). te_k = T_k - t_ref where
+ * node k has an applied temperature, 0 elsewhere (element_temp_change, stress.cpp:76-91;
+ * thermal_strain_load_vector takes T = t_ref at such nodes, loads.cpp:537-541, the same
+ * te). alpha is the element's expansion coefficient as the caller evaluated its table at
+ * the element's mean temperature (element_alpha, stress.cpp:97-105; loads.cpp:548-550),
+ * 0 without *EXPANSION. Returns 1 when some te_k is nonzero and alpha is nonzero. */
+static int element_te(const double* node_temp, const uint8_t* node_applied, const double* elem_alpha,
+                      const double* elem_tref, int64_t e, const int32_t* c, int n, double* te, double* alpha) {
+  int any = 0;
+  *alpha = node_temp && elem_alpha ? elem_alpha[e] : 0.0;
+  for (int k = 0; k < n; ++k) {
+    te[k] = 0.0;
+    if (node_temp && (!node_applied || node_applied[c[k]])) te[k] = node_temp[c[k]] - elem_tref[e];
+    if (te[k] != 0.0) any = 1;
+  }
+  return any && *alpha != 0.0;
+}
+
+/* element_thermal_load, element.cpp:636-665: fe = sum_q det w B^T D eps_th,
+ * eps_th = alpha sum_k N_k te_k on the normal components. */
+static int element_thermal_load(int type, const double* x, const double* D, double alpha, const double* te,
+                                double* fe) {
+  double gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det;
+  const int n = cxo_nodes_per_element(type), ndof = 3 * n;
+  memset(fe, 0, sizeof(double) * (size_t)ndof);
+  const int ng = cxo_gauss_rule(type, gp);
+  for (int q = 0; q < ng; ++q) {
+    cxo_shape(type, gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
+    if (gradients_from_shape(n, dN, x, g, &det)) return -1;
+    double dT = 0.0;
+    for (int k = 0; k < n; ++k) dT += N[k] * te[k];
+    const double eth = alpha * dT;
+    const double eps_th[6] = {eth, eth, eth, 0.0, 0.0, 0.0};
+    double sig_th[6];
+    for (int i = 0; i < 6; ++i) {
+      double v = 0.0;
+      for (int j = 0; j < 6; ++j) v += D[6 * i + j] * eps_th[j];
+      sig_th[i] = v;
+    }
+    accumulate_fint(g, ndof, sig_th, det * gp[4 * q + 3], fe);
+  }
+  return 0;
+}
+
+/* thermal_strain_load_vector, loads.cpp:515-560: f[3 * n_nodes] = sum over the elements
+ * with an expansion coefficient and a temperature change of element_thermal_load. */
+int cxo_thermal_strain_load(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                            const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
+                            const double* node_temp, const uint8_t* node_applied, const double* elem_alpha,
+                            const double* elem_tref, double* f) {
+  double x[3 * MAXN], D[36], te[MAXN], fe[3 * MAXN], alpha;
+  memset(f, 0, sizeof(double) * 3 * (size_t)n_nodes);
+  for (int64_t e = 0; e < n_elems; ++e) {
+    const int n = cxo_nodes_per_element(types[e]);
+    const int32_t* c = conn + conn_ptr[e];
+    if (n == 0 || conn_ptr[e + 1] - conn_ptr[e] != n) return fail("unsupported element type or bad connectivity");
+    for (int k = 0; k < n; ++k) {
+      if (c[k] < 0 || c[k] >= n_nodes) return fail("element references unknown node");
+      for (int d = 0; d < 3; ++d) x[3 * k + d] = coords[3 * (int64_t)c[k] + d];
+    }
+    if (!element_te(node_temp, node_applied, elem_alpha, elem_tref, e, c, n, te, &alpha)) continue;
+    elastic_D(young[e], poisson[e], D);
+    if (element_thermal_load(types[e], x, D, alpha, te, fe)) return -1;
+    for (int a = 0; a < 3 * n; ++a) f[3 * (int64_t)c[a / 3] + a % 3] += fe[a];
+  }
+  return 0;
+}
+
 /* recover_gauss_stress, stress.cpp:147-187: out[6 * G] (element order, Gauss-rule order);
  * young/poisson per element. */
-int cxo_recover_gauss_stress(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
-                             const int64_t* conn_ptr, const int32_t* conn, const double* young,
-                             const double* poisson, const double* u, double* out) {
+int cxo_recover_gauss_stress_th(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                                const int64_t* conn_ptr, const int32_t* conn, const double* young,
+                                const double* poisson, const double* node_temp, const uint8_t* node_applied,
+                                const double* elem_alpha, const double* elem_tref, const double* u, double* out) {
   double x[3 * MAXN], ue[3 * MAXN], D[36], gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det, strain[6];
+  double te[MAXN], alpha;
   int64_t off = 0;
   for (int64_t e = 0; e < n_elems; ++e) {
     const int n = cxo_nodes_per_element(types[e]);
     if (n == 0 || conn_ptr[e + 1] - conn_ptr[e] != n) return fail("unsupported element type or bad connectivity");
     if (gather_element(n_nodes, coords, conn + conn_ptr[e], n, u, x, ue)) return -1;
     elastic_D(young[e], poisson[e], D);
+    const int th = element_te(node_temp, node_applied, elem_alpha, elem_tref, e, conn + conn_ptr[e], n, te, &alpha);
     const int ng = cxo_gauss_rule(types[e], gp);
     for (int q = 0; q < ng; ++q, ++off) {
       cxo_shape(types[e], gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
       if (gradients_from_shape(n, dN, x, g, &det)) return -1;
-      strain_stress_at(g, n, ue, D, strain, out + 6 * off);
+      double dT = 0.0;
+      for (int k = 0; k < n; ++k) dT += N[k] * (th ? te[k] : 0.0);
+      strain_stress_at(g, n, ue, D, th ? alpha * dT : 0.0, strain, out + 6 * off);
     }
   }
   return 0;
 }
 
-/* recover_fields, stress.cpp:189-271 (elastic, no thermal strain): nodal strain/stress
- * averaged over the incident elements, reaction = f_int - f_ext with
- * f_int = sum_e K_e u_e (accumulate_internal_force, stress.cpp:56-75). */
-int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
-                       const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
-                       const double* u, const double* f_ext, double* strain_out, double* stress_out,
-                       double* reaction) {
+int cxo_recover_gauss_stress(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                             const int64_t* conn_ptr, const int32_t* conn, const double* young,
+                             const double* poisson, const double* u, double* out) {
+  return cxo_recover_gauss_stress_th(n_nodes, coords, n_elems, types, conn_ptr, conn, young, poisson, NULL, NULL,
+                                     NULL, NULL, u, out);
+}
+
+/* recover_fields, stress.cpp:189-271 (elastic): nodal strain/stress averaged over the
+ * incident elements, reaction = f_int - f_ext with f_int = sum_e (K_e u_e - f_th_e)
+ * (accumulate_internal_force, stress.cpp:56-75); thermal inputs as element_te. */
+int cxo_recover_fields_th(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                          const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
+                          const double* node_temp, const uint8_t* node_applied, const double* elem_alpha,
+                          const double* elem_tref, const double* u, const double* f_ext, double* strain_out,
+                          double* stress_out, double* reaction) {
   double x[3 * MAXN], ue[3 * MAXN], D[36], gp[4 * 27], N[MAXN], dN[3 * MAXN], g[3 * MAXN], det;
-  double Ke[60 * 60], gs[27][6], ge[27][6];
+  double Ke[60 * 60], gs[27][6], ge[27][6], te[MAXN], fth[3 * MAXN], alpha;
   int* count = calloc((size_t)n_nodes, sizeof(int));
   double* f_int = calloc((size_t)(3 * n_nodes), sizeof(double));
   if (!count || !f_int) {
@@ -1210,18 +1292,25 @@ int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, c
     }
     if ((rc = gather_element(n_nodes, coords, c, n, u, x, ue))) break;
     elastic_D(young[e], poisson[e], D);
+    /* thermal strain and its equivalent load (stress.cpp:207-213) */
+    const int th = element_te(node_temp, node_applied, elem_alpha, elem_tref, e, c, n, te, &alpha);
+    if (th && (rc = element_thermal_load(types[e], x, D, alpha, te, fth))) break;
     if ((rc = cxo_element_stiffness(types[e], x, young[e], poisson[e], Ke))) break;
     const int ndof = 3 * n;
+    /* f_int_e = K_e u_e - f_th_e (accumulate_internal_force, stress.cpp:56-75) */
     for (int a = 0; a < ndof; ++a) {
       double v = 0.0;
       for (int b = 0; b < ndof; ++b) v += Ke[a * ndof + b] * ue[b];
+      if (th) v -= fth[a];
       f_int[3 * (int64_t)c[a / 3] + a % 3] += v;
     }
     const int ng = cxo_gauss_rule(types[e], gp);
     for (int q = 0; q < ng; ++q) {
       cxo_shape(types[e], gp[4 * q], gp[4 * q + 1], gp[4 * q + 2], N, dN);
       if ((rc = gradients_from_shape(n, dN, x, g, &det))) break;
-      strain_stress_at(g, n, ue, D, ge[q], gs[q]);
+      double dT = 0.0;
+      for (int k = 0; k < n; ++k) dT += N[k] * (th ? te[k] : 0.0);
+      strain_stress_at(g, n, ue, D, th ? alpha * dT : 0.0, ge[q], gs[q]);
     }
     if (rc) break;
     /* extrapolate_gp_to_nodes (extrapolation.hpp:26-55): C3D10 corners by the a4 matrix
@@ -1284,6 +1373,14 @@ int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, c
   free(count);
   free(f_int);
   return rc;
+}
+
+int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                       const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
+                       const double* u, const double* f_ext, double* strain_out, double* stress_out,
+                       double* reaction) {
+  return cxo_recover_fields_th(n_nodes, coords, n_elems, types, conn_ptr, conn, young, poisson, NULL, NULL, NULL, NULL,
+                               u, f_ext, strain_out, stress_out, reaction);
 }
 
 int cxo_system_info(const cxo_system* s, int32_t* n_free, int64_t* nnz) {

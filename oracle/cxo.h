@@ -104,6 +104,23 @@ int cxo_recover_gauss_stress(int64_t n_nodes, const double* coords, int64_t n_el
 int cxo_recover_fields(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
                        const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
                        const double* u, const double* f_ext, double* strain, double* stress, double* reaction);
+/* Thermal strain (loads.cpp:515-560, stress.cpp:76-271): node_temp[n_nodes] applied
+ * temperatures, node_applied[n_nodes] 0/1 (NULL: every node), elem_alpha[n_elems] the
+ * expansion coefficient at the element's mean temperature (0: none), elem_tref[n_elems];
+ * NULL node_temp: no thermal strain. */
+int cxo_thermal_strain_load(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                            const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
+                            const double* node_temp, const uint8_t* node_applied, const double* elem_alpha,
+                            const double* elem_tref, double* f);
+int cxo_recover_gauss_stress_th(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                                const int64_t* conn_ptr, const int32_t* conn, const double* young,
+                                const double* poisson, const double* node_temp, const uint8_t* node_applied,
+                                const double* elem_alpha, const double* elem_tref, const double* u, double* out);
+int cxo_recover_fields_th(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                          const int64_t* conn_ptr, const int32_t* conn, const double* young, const double* poisson,
+                          const double* node_temp, const uint8_t* node_applied, const double* elem_alpha,
+                          const double* elem_tref, const double* u, const double* f_ext, double* strain_out,
+                          double* stress_out, double* reaction);
 
 /* element_conduction (n x n) and assemble_conduction without films (src/fem/thermal.cpp:
  * 92-141): t_dof_eq[N] / t_prescribed[N] scalar temperature DOF map, flux[N] may be NULL. */

@@ -104,6 +104,11 @@ PORT_SIGS = dict(_COMMON, **{
     "assemble_scalar": (_vp, [_i, _i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32t]),
     "recover_gauss_stress": (_i, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "recover_fields": (_i, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "thermal_strain_load": (_i, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "recover_gauss_stress_th": (_i, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                     _vp]),
+    "recover_fields_th": (_i, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                               _vp, _vp, _vp]),
     "assemble_conduction": (_vp, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _i32t, _vp]),
     "system_info": (_i, [_vp, _vp, _vp]),
     "system_copy": (_i, [_vp, _vp, _vp, _vp, _vp]),
@@ -122,6 +127,9 @@ REF_SIGS = dict(_COMMON, **{
     "assemble_geometric": (_vp, [_vp, _vp]),
     "recover_gauss_stress": (_i, [_vp, _vp, _vp]),
     "recover_fields": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "model_set_expansion": (_i, [_vp, _i32t, _vp, _vp, _vp, _vp]),
+    "model_set_temperature": (_i, [_vp, _i64t, _vp, _vp]),
+    "thermal_strain_load_vector": (_i, [_vp, _vp]),
     "assemble_conduction": (_vp, [_vp, _i32t, _vp, _i64t, _vp, _vp]),
     "assemble_linear_static": (_vp, [_vp]),
     "sys_info": (_i, [_vp, _vp, _vp]),
@@ -365,6 +373,42 @@ class Port(_Base):
                       _p(None if f_ext is None else _f64(f_ext)), _p(st), _p(ss), _p(rf)))
         return st.reshape(N, 6), ss.reshape(N, 6), rf.reshape(N, 3)
 
+    @staticmethod
+    def _thermal_args(thermal):
+        """(node_temp, node_applied, elem_alpha, elem_tref) pointers; thermal None: none."""
+        if thermal is None:
+            return (None, None, None, None), ()
+        t, applied, alpha, tref = thermal
+        keep = (_f64(t), None if applied is None else np.ascontiguousarray(applied, dtype=np.uint8), _f64(alpha),
+                _f64(tref))
+        return tuple(_p(k) for k in keep), keep
+
+    def thermal_strain_load(self, mesh, young, poisson, thermal):
+        """thermal_strain_load_vector (src/fem/loads.cpp:515-560): f[3N]. thermal = (node_temp,
+        node_applied or None, elem_alpha, elem_tref)."""
+        out = np.zeros(3 * mesh.n_nodes)
+        ptrs, _keep = self._thermal_args(thermal)
+        self._check(self._fn("thermal_strain_load")(*self._recover_args(mesh, young, poisson), *ptrs, _p(out)))
+        return out
+
+    def recover_gauss_stress_th(self, mesh, young, poisson, thermal, u):
+        """recover_gauss_stress with the thermal-strain correction (stress.cpp:147-187): (G, 6)."""
+        out = np.zeros(6 * mesh.n_elems * NGP[mesh.etype])
+        ptrs, _keep = self._thermal_args(thermal)
+        self._check(self._fn("recover_gauss_stress_th")(*self._recover_args(mesh, young, poisson), *ptrs,
+                                                         _p(_f64(u)), _p(out)))
+        return out.reshape(-1, 6)
+
+    def recover_fields_th(self, mesh, young, poisson, thermal, u, f_ext=None):
+        """recover_fields with thermal strain (stress.cpp:189-271): strain, stress, reaction."""
+        N = mesh.n_nodes
+        st, ss, rf = np.zeros(6 * N), np.zeros(6 * N), np.zeros(3 * N)
+        ptrs, _keep = self._thermal_args(thermal)
+        self._check(self._fn("recover_fields_th")(*self._recover_args(mesh, young, poisson), *ptrs, _p(_f64(u)),
+                                                   _p(None if f_ext is None else _f64(f_ext)), _p(st), _p(ss),
+                                                   _p(rf)))
+        return st.reshape(N, 6), ss.reshape(N, 6), rf.reshape(N, 3)
+
     def assemble_conduction(self, mesh, conductivity, t_dof_eq, t_prescribed, n_free, flux=None):
         """assemble_conduction without films (src/fem/thermal.cpp:92-141): (rp, ci, vals, rhs)."""
         E = mesh.n_elems
@@ -516,6 +560,25 @@ class RefModel:
         st, ss, rf = np.zeros(6 * N), np.zeros(6 * N), np.zeros(3 * N)
         self.ref._check(self.ref._fn("recover_fields")(_vp(self.h), _p(_f64(u)), _p(st), _p(ss), _p(rf)))
         return st.reshape(N, 6), ss.reshape(N, 6), rf.reshape(N, 3)
+
+    def set_expansion(self, tables, trefs):
+        """*EXPANSION per material: tables[k] = (alpha values, temperatures) or None."""
+        npts = np.array([0 if t is None else len(t[0]) for t in tables], dtype=np.int32)
+        vals = _f64(np.concatenate([np.asarray(t[0], float) for t in tables if t is not None] or [np.zeros(0)]))
+        temps = _f64(np.concatenate([np.asarray(t[1], float) for t in tables if t is not None] or [np.zeros(0)]))
+        tr = _f64(trefs)
+        self.ref._check(self.ref._fn("model_set_expansion")(_vp(self.h), C.c_int32(npts.size), _p(npts), _p(vals),
+                                                             _p(temps), _p(tr)))
+
+    def set_temperature(self, nodes, temps):
+        """Applied temperatures (Model::applied_temperature), nodes 0-based."""
+        nd, tv = _i32(nodes), _f64(temps)
+        self.ref._check(self.ref._fn("model_set_temperature")(_vp(self.h), nd.size, _p(nd), _p(tv)))
+
+    def thermal_strain_load_vector(self):
+        out = np.zeros(3 * self.mesh.n_nodes)
+        self.ref._check(self.ref._fn("thermal_strain_load_vector")(_vp(self.h), _p(out)))
+        return out
 
     def set_density(self, rho_per_material):
         rho = _f64(rho_per_material)

@@ -30,6 +30,7 @@
 
 #include "calculixpp/core/model.hpp"
 #include "calculixpp/fem/assembly.hpp"
+#include "calculixpp/fem/loads.hpp"
 #include "calculixpp/fem/stress.hpp"
 #include "calculixpp/fem/thermal.hpp"
 #include "calculixpp/fem/element.hpp"
@@ -318,6 +319,58 @@ int ref_model_add_equation(void* model, int32_t n_terms, const int32_t* nodes, c
     eq.origin = "*EQUATION";
     for (int32_t i = 0; i < n_terms; ++i) eq.terms.push_back(EquationTerm{nodes[i] + 1, comps[i] + 1, coeffs[i]});
     static_cast<RefModel*>(model)->model.equations.push_back(eq);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// *EXPANSION of material k (Material::expansion): an alpha(T) table of n_points[k] rows
+// (alpha_vals / alpha_temps, rows of all materials concatenated) and the reference
+// temperature tref[k]; n_points[k] == 0 leaves material k without expansion.
+int ref_model_set_expansion(void* model, int32_t n_mats, const int32_t* n_points, const double* alpha_vals,
+                            const double* alpha_temps, const double* tref) {
+  try {
+    Model& m = static_cast<RefModel*>(model)->model;
+    int64_t off = 0;
+    for (int32_t k = 0; k < n_mats; ++k) {
+      const auto it = m.materials.find("M" + std::to_string(k));
+      const int32_t np = n_points[k];
+      if (it != m.materials.end() && np > 0) {
+        Expansion ex;
+        for (int32_t r = 0; r < np; ++r) {
+          ex.alpha.value.push_back(alpha_vals[off + r]);
+          ex.alpha.temp.push_back(alpha_temps[off + r]);
+        }
+        ex.t_ref = tref[k];
+        it->second.expansion = ex;
+      }
+      off += np;
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// Applied temperatures (Model::applied_temperature): nodes 0-based.
+int ref_model_set_temperature(void* model, int64_t n, const int32_t* nodes, const double* temps) {
+  try {
+    Model& m = static_cast<RefModel*>(model)->model;
+    m.applied_temperature.clear();
+    for (int64_t i = 0; i < n; ++i) m.applied_temperature[static_cast<Index>(nodes[i] + 1)] = temps[i];
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// thermal_strain_load_vector (loads.cpp:515-560): out[3N].
+int ref_thermal_strain_load_vector(void* model, double* out) {
+  try {
+    const Model& m = static_cast<RefModel*>(model)->model;
+    const std::vector<Real> f = thermal_strain_load_vector(m);
+    std::copy(f.begin(), f.end(), out);
     return 0;
   } catch (const std::exception& e) {
     return fail(e);
