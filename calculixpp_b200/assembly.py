@@ -197,6 +197,32 @@ class Plan:
         yield surface) instead of FP64 (cxg_plan_set_j2_fp32_return)."""
         _lib.check(self.lib.cxg_plan_set_j2_fp32_return(self.h, int(bool(enable))))
 
+    def set_thermal_strain(self, node_temp=None, node_applied=None, elem_alpha=None, elem_tref=None):
+        """Thermal-strain inputs (cxg_plan_set_thermal_strain; see `thermal_strain_inputs`):
+        applied temperature per node, applied flags (None: all), expansion coefficient and
+        reference temperature per element. node_temp None clears. The linear assembly then
+        adds the thermal-strain load to the rhs and the recovery uses sigma = D (eps - eps_th)."""
+        if node_temp is None:
+            _lib.check(self.lib.cxg_plan_set_thermal_strain(self.h, None, None, None, None))
+            return
+        t = np.ascontiguousarray(node_temp, dtype=np.float64)
+        ap = None if node_applied is None else np.ascontiguousarray(node_applied, dtype=np.uint8)
+        al = np.ascontiguousarray(elem_alpha, dtype=np.float64)
+        tr = np.ascontiguousarray(elem_tref, dtype=np.float64)
+        if t.size != self.model.mesh.n_nodes or al.size != self.model.mesh.n_elems or tr.size != al.size:
+            raise ValueError("node_temp[n_nodes], elem_alpha[n_elems] and elem_tref[n_elems] are required")
+        ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_plan_set_thermal_strain(self.h, ptr(t), ptr(ap), ptr(al), ptr(tr)))
+
+    def thermal_strain_load(self):
+        """thermal_strain_load_vector (src/fem/loads.cpp:515-560): f_th[3N] on the device."""
+        out = torch.empty(3 * self.model.mesh.n_nodes, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_thermal_strain_load(self.h, _ptr(out), _stream()))
+            self.check()
+        return out
+
     def set_ring_bytes(self, nbytes: int):
         """Element-buffer budget of the windowed assembly (cxg_plan_set_ring_bytes):
         0 or < 0 = one window over the whole mesh, > 0 = windows whose buffers fit."""

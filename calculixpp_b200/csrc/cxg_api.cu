@@ -380,6 +380,10 @@ ElemArgs base_args(cxg_plan* p) {
   a.bnd_node = p->pat.bnd_node;
   a.n_gauss = p->n_gauss;
   a.status = p->status;
+  a.th_temp = p->th_temp;
+  a.th_applied = p->th_applied;
+  a.th_alpha = p->th_alpha;
+  a.th_tref = p->th_tref;
   return a;
 }
 
@@ -596,9 +600,14 @@ int cxg_plan_create_mpc(const cxg_mesh_desc* m, const cxg_dofmap_desc* d, const 
   return CXG_OK;
 }
 
+namespace thermal {
+void release(cxg_plan* p);
+}
+
 int cxg_plan_destroy(cxg_plan* p) {
   if (!p) return CXG_OK;
   if (p->last_stream) cudaStreamSynchronize(p->last_stream);
+  thermal::release(p);
   void* bufs[] = {p->coords, p->conn, p->young, p->poisson, p->elem_mat, p->mats, p->dof_eq, p->prescribed,
                   p->pat.row_ptr, p->pat.col_idx, p->pat.node_base, p->pat.node_rowlen, p->pat.node_mask,
                   p->pat.node_eq0, p->pat.slot, p->pat.adj_len, p->pat.bnd_ptr, p->pat.bnd_node, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
@@ -775,6 +784,86 @@ int cxg_plan_check(cxg_plan* p, int64_t* bad) {
   return plan_status(p, bad);
 }
 
+namespace thermal {
+
+__global__ void add_into_kernel(int64_t n, double* a, const double* b) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    a[i] += b[i];
+}
+
+// thermal_strain_load_vector of the plan into out[3N] (device)
+int load_device(cxg_plan* p, double* out, cudaStream_t s) {
+  const int n = nodes_of(p->type);
+  double* felem = nullptr;
+  CHECK_CUDA(cudaMallocAsync(&felem, sizeof(double) * std::max<size_t>(static_cast<size_t>(p->n_elems) * 3 * n, 1), s),
+             "thermal load scratch");
+  ElemArgs a = base_args(p);
+  a.u = nullptr;
+  const cudaError_t err = launch_recover(p->type, a, p->pat.inc_ptr, p->pat.inc_code, nullptr, nullptr, felem, nullptr,
+                                         nullptr, nullptr, out, true, s);
+  cudaFreeAsync(felem, s);
+  CHECK_CUDA(err, "thermal load kernels");
+  return CXG_OK;
+}
+
+void release(cxg_plan* p) {
+  for (void* b : {static_cast<void*>(p->th_temp), static_cast<void*>(p->th_applied), static_cast<void*>(p->th_alpha),
+                  static_cast<void*>(p->th_tref), static_cast<void*>(p->th_load)})
+    cudaFree(b);
+  p->th_temp = nullptr;
+  p->th_applied = nullptr;
+  p->th_alpha = nullptr;
+  p->th_tref = nullptr;
+  p->th_load = nullptr;
+}
+
+}  // namespace thermal
+
+int cxg_plan_set_thermal_strain(cxg_plan* p, const double* node_temp, const uint8_t* node_applied,
+                                const double* elem_alpha, const double* elem_tref) {
+  if (!p) return set_err(CXG_ERR_INVALID_ARGUMENT, "null plan");
+  if (p->last_stream) CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");
+  thermal::release(p);
+  if (!node_temp) return CXG_OK;
+  if (!elem_alpha || !elem_tref) return set_err(CXG_ERR_INVALID_ARGUMENT, "elem_alpha and elem_tref are required");
+  if (p->thermal) return set_err(CXG_ERR_UNSUPPORTED, "thermal strain applies to displacement plans");
+  const size_t N = static_cast<size_t>(std::max<int64_t>(p->n_nodes, 1)), E = static_cast<size_t>(std::max<int64_t>(p->n_elems, 1));
+  cudaError_t e = cudaMalloc(&p->th_temp, sizeof(double) * N);
+  if (e == cudaSuccess && node_applied) e = cudaMalloc(&p->th_applied, N);
+  if (e == cudaSuccess) e = cudaMalloc(&p->th_alpha, sizeof(double) * E);
+  if (e == cudaSuccess) e = cudaMalloc(&p->th_tref, sizeof(double) * E);
+  if (e == cudaSuccess) e = cudaMalloc(&p->th_load, sizeof(double) * 3 * N);
+  const size_t nn = static_cast<size_t>(p->n_nodes), ne = static_cast<size_t>(p->n_elems);
+  if (e == cudaSuccess && nn) e = cudaMemcpy(p->th_temp, node_temp, sizeof(double) * nn, cudaMemcpyDefault);
+  if (e == cudaSuccess && nn && node_applied) e = cudaMemcpy(p->th_applied, node_applied, nn, cudaMemcpyDefault);
+  if (e == cudaSuccess && ne) e = cudaMemcpy(p->th_alpha, elem_alpha, sizeof(double) * ne, cudaMemcpyDefault);
+  if (e == cudaSuccess && ne) e = cudaMemcpy(p->th_tref, elem_tref, sizeof(double) * ne, cudaMemcpyDefault);
+  if (e != cudaSuccess) {
+    thermal::release(p);
+    return cuda_err(e, "thermal strain inputs");
+  }
+  return CXG_OK;
+}
+
+int cxg_thermal_strain_load(cxg_plan* p, double* f_th, void* stream) {
+  if (!p || !f_th) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan and f_th are required");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->last_stream = s;
+  const size_t fb = sizeof(double) * 3 * static_cast<size_t>(p->n_nodes);
+  if (!p->th_temp) {
+    CHECK_CUDA(cudaMemsetAsync(f_th, 0, fb, s), "zero load");  // no thermal strain set
+    return CXG_OK;
+  }
+  void* df = nullptr;
+  int rc = staged(p, 2, f_th, fb, false, s, &df);
+  if (!rc) rc = thermal::load_device(p, static_cast<double*>(df), s);
+  if (!rc) rc = copy_out(f_th, df, fb, s);
+  if (rc) return rc;
+  if (df != f_th) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
+  return CXG_OK;
+}
+
 int cxg_assemble_linear(cxg_plan* p, double* vals, double* rhs, const double* f_ext, void* stream) {
   return cxg_assemble_linear_ex(p, vals, rhs, f_ext, 0, stream);
 }
@@ -796,6 +885,17 @@ int cxg_assemble_linear_ex(cxg_plan* p, double* vals, double* rhs, const double*
   if (!rc && !accumulate) rc = staged(p, 2, f_ext, fb, true, s, &df);
   if (rc) return rc;
   if ((rc = ensure_v2(p, false))) return rc;
+  // thermal-strain equivalent load added to the external load (assembly.cpp:251-253)
+  if (p->th_temp && !accumulate) {
+    if ((rc = thermal::load_device(p, p->th_load, s))) return rc;
+    if (df) {
+      const int64_t n3 = 3 * p->n_nodes;
+      thermal::add_into_kernel<<<static_cast<unsigned>(std::min<int64_t>((n3 + 255) / 256, 148 * 16) + 1), 256, 0, s>>>(
+          n3, p->th_load, static_cast<const double*>(df));
+      CHECK_CUDA(cudaGetLastError(), "thermal load");
+    }
+    df = p->th_load;
+  }
   ElemArgs a = base_args(p);
   // with the reference's pattern, the assembly runs on the topological pattern and the
   // kept entries are gathered into the caller's values
@@ -991,7 +1091,7 @@ int cxg_recover_gauss_stress(cxg_plan* p, const double* u, double* gp_stress, vo
   ElemArgs a = base_args(p);
   a.u = static_cast<const double*>(du);
   CHECK_CUDA(launch_recover(p->type, a, nullptr, nullptr, static_cast<double*>(dg), nullptr, nullptr, nullptr, nullptr,
-                            nullptr, nullptr, s),
+                            nullptr, nullptr, false, s),
              "recovery kernel");
   if ((rc = copy_out(gp_stress, dg, gb, s))) return rc;
   if (dg != gp_stress) CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
@@ -1025,7 +1125,7 @@ int cxg_recover_fields(cxg_plan* p, const double* u, const double* f_ext, double
   const cudaError_t err = launch_recover(p->type, a, p->pat.inc_ptr, p->pat.inc_code, nullptr, scratch,
                                          scratch + 12 * static_cast<size_t>(sets) * static_cast<size_t>(p->n_elems),
                                          static_cast<const double*>(df), static_cast<double*>(dst),
-                                         static_cast<double*>(dss), static_cast<double*>(drf), s);
+                                         static_cast<double*>(dss), static_cast<double*>(drf), false, s);
   cudaFreeAsync(scratch, s);
   CHECK_CUDA(err, "recovery kernels");
   if ((rc = copy_out(strain, dst, sb, s))) return rc;

@@ -87,6 +87,13 @@ struct ElemArgs {
   // material moves it (every kinematic modulus is 0); components 7..12 are then zero
   // and left untouched
   int state_comps;
+  // thermal strain (null th_temp: none): applied temperature per node, whether it is
+  // applied (null: every node), expansion coefficient and reference temperature per
+  // element (alpha 0: no expansion)
+  const double* th_temp;      // [N]
+  const uint8_t* th_applied;  // [N]
+  const double* th_alpha;     // [E]
+  const double* th_tref;      // [E]
   // displacement (tangent mode)
   const double* u;           // [3N] (mesh) or [E*n*3] (dense)
   // outputs
@@ -198,7 +205,7 @@ cudaError_t launch_state_transpose(const double* src, double* dst, int64_t G, bo
 // stress only); strain/stress[6N], reaction[3N] outputs.
 cudaError_t launch_recover(int elem_type, const ElemArgs& a, const int64_t* inc_ptr, const int32_t* inc_code,
                            double* gp_stress, double* emean, double* felem, const double* f_ext, double* strain,
-                           double* stress, double* reaction, cudaStream_t s);
+                           double* stress, double* reaction, bool thermal_load, cudaStream_t s);
 cudaError_t launch_adjoint(int elem_type, const ElemArgs& a, double* dc_dE, double* dc_dX,
                            cudaStream_t s);
 cudaError_t launch_spmv(int32_t nrows, const int64_t* rp, const int32_t* ci, const double* v, const double* x,

@@ -103,6 +103,12 @@ struct cxg_plan {
   // (the J2 tangent tiles carry three accumulator terms; 2x4 measured 1.6x slower)
   cxg::LaunchCfg tcfg[2] = {tangent_default(), tangent_default()};
   bool thermal = false;    // temperature plan: DOF 0 of every node, components 1 and 2 fixed
+  // thermal strain (cxg_plan_set_thermal_strain): device copies, null when not set
+  double* th_temp = nullptr;
+  uint8_t* th_applied = nullptr;
+  double* th_alpha = nullptr;
+  double* th_tref = nullptr;
+  double* th_load = nullptr;  // [3N] scratch: thermal-strain load (+ f_ext) of the linear assembly
 };
 
 

@@ -1,5 +1,13 @@
 // Field recovery from a displacement field (recover_gauss_stress / recover_fields,
-// src/fem/stress.cpp:147-271; linear elasticity, no thermal strain).
+// src/fem/stress.cpp:147-271; linear elasticity), and the thermal-strain load vector
+// (thermal_strain_load_vector, src/fem/loads.cpp:515-560; element_thermal_load,
+// element.cpp:636-665).
+//
+// Thermal strain, when the plan has it: te_k = T_k - t_ref at the element's nodes with an
+// applied temperature (0 elsewhere), eps_th = alpha sum_k N_k te_k on the normal
+// components at every Gauss point; the stress is D (eps - eps_th) and the element force
+// sum_q detJ w sigma_q g_a is then K_e u_e - f_th_e. In thermal-load mode the element pass
+// forms D eps_th instead (no displacement), and the node pass sums f_th.
 //
 // Element pass: one warp per element. Lanes take Gauss points: physical gradients,
 // displacement gradient, engineering strain and sigma = D eps (written out per point
@@ -32,10 +40,11 @@ constexpr int rec_sets() {
 template <int ET>
 constexpr int rec_warp_doubles() {
   constexpr int n = nodes_of(ET), nq = gauss_of(ET);
-  return 6 * n + nq + nq * n * 3 + nq * 12;  // x, u, detJ w, gradients, strain + stress
+  return 7 * n + nq + nq * n * 3 + nq * 12;  // x, u, te, detJ w, gradients, strain + stress
 }
 
-template <int ET>
+// THLOAD: thermal-load mode (felem = f_th_e; no displacement, no means)
+template <int ET, bool THLOAD>
 __global__ void __launch_bounds__(kRecWarps * 32) rec_elem_kernel(ElemArgs A, double* gp_stress, double* emean,
                                                                   double* felem) {
   constexpr int n = nodes_of(ET), nq = gauss_of(ET);
@@ -43,16 +52,20 @@ __global__ void __launch_bounds__(kRecWarps * 32) rec_elem_kernel(ElemArgs A, do
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* x = reinterpret_cast<double*>(smem) + warp * rec_warp_doubles<ET>();
   double* uu = x + 3 * n;
-  double* sq = uu + 3 * n;
+  double* te = uu + 3 * n;  // [n] temperature change of the element's nodes
+  double* sq = te + n;
   double* g = sq + nq;         // [nq][n][3]
   double* es = g + nq * n * 3; // [nq][12]: strain[6], stress[6]
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * kRecWarps + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kRecWarps;
   for (int64_t e = gwarp; e < A.n_elems; e += nwarps) {
+    const double alpha = A.th_temp ? A.th_alpha[e] : 0.0;
     for (int t = lane; t < 3 * n; t += 32) {
       const int64_t node = A.conn[e * n + t / 3];
       x[t] = A.coords[3 * node + t % 3];
-      uu[t] = A.u[3 * node + t % 3];
+      uu[t] = THLOAD ? 0.0 : A.u[3 * node + t % 3];
+      if (t % 3 == 0)
+        te[t / 3] = alpha != 0.0 && (!A.th_applied || A.th_applied[node]) ? A.th_temp[node] - A.th_tref[e] : 0.0;
     }
     __syncwarp();
     const double E = A.young[e], nu = A.poisson[e];
@@ -91,6 +104,12 @@ __global__ void __launch_bounds__(kRecWarps * 32) rec_elem_kernel(ElemArgs A, do
         for (int i = 0; i < 3; ++i)
           for (int j = 0; j < 3; ++j) du[i][j] += gk[j] * uu[3 * k + i];
       }
+      double eth = 0.0;  // alpha sum_k N_k te_k
+      if (alpha != 0.0) {
+        double dT = 0.0;
+        for (int k = 0; k < n; ++k) dT += c_N[nn_offset(ET) + k * nq + q] * te[k];
+        eth = alpha * dT;
+      }
       double* st = es + 12 * q;
       st[0] = du[0][0];
       st[1] = du[1][1];
@@ -98,13 +117,15 @@ __global__ void __launch_bounds__(kRecWarps * 32) rec_elem_kernel(ElemArgs A, do
       st[3] = du[0][1] + du[1][0];
       st[4] = du[0][2] + du[2][0];
       st[5] = du[1][2] + du[2][1];
-      const double tr = st[0] + st[1] + st[2];
-      st[6] = lam * tr + 2.0 * mu * st[0];
-      st[7] = lam * tr + 2.0 * mu * st[1];
-      st[8] = lam * tr + 2.0 * mu * st[2];
-      st[9] = mu * st[3];
-      st[10] = mu * st[4];
-      st[11] = mu * st[5];
+      // elastic strain: eps - eps_th, or eps_th itself in thermal-load mode (D eps_th)
+      const double e0 = THLOAD ? eth : st[0] - eth, e1 = THLOAD ? eth : st[1] - eth, e2 = THLOAD ? eth : st[2] - eth;
+      const double tr = e0 + e1 + e2;
+      st[6] = lam * tr + 2.0 * mu * e0;
+      st[7] = lam * tr + 2.0 * mu * e1;
+      st[8] = lam * tr + 2.0 * mu * e2;
+      st[9] = THLOAD ? 0.0 : mu * st[3];
+      st[10] = THLOAD ? 0.0 : mu * st[4];
+      st[11] = THLOAD ? 0.0 : mu * st[5];
       if (gp_stress)
         for (int c = 0; c < 6; ++c) gp_stress[(e * nq + q) * 6 + c] = st[6 + c];
     }
@@ -167,7 +188,8 @@ __global__ void rec_node_kernel(ElemArgs A, const int64_t* inc_ptr, const int32_
       const int64_t e = code / n;
       const int la = code % n;
       const int64_t set = rec_sets<ET>() == 1 ? e : e * n + la;
-      for (int c = 0; c < 12; ++c) m[c] += emean[set * 12 + c];
+      if (emean)
+        for (int c = 0; c < 12; ++c) m[c] += emean[set * 12 + c];
       for (int d = 0; d < 3; ++d) f[d] += felem[e * (3 * n) + 3 * la + d];
     }
     const int64_t cnt = i1 - i0;
@@ -187,9 +209,9 @@ unsigned rec_grid(int64_t n) {
 template <int ET>
 cudaError_t launch_recover_t(const ElemArgs& a, const int64_t* inc_ptr, const int32_t* inc_code, double* gp_stress,
                              double* emean, double* felem, const double* f_ext, double* strain, double* stress,
-                             double* reaction, cudaStream_t s) {
+                             double* reaction, bool thermal_load, cudaStream_t s) {
   if (a.n_elems > 0) {
-    auto kern = rec_elem_kernel<ET>;
+    auto kern = thermal_load ? rec_elem_kernel<ET, true> : rec_elem_kernel<ET, false>;
     const size_t smem = sizeof(double) * kRecWarps * rec_warp_doubles<ET>();
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (err != cudaSuccess) return err;
@@ -198,7 +220,7 @@ cudaError_t launch_recover_t(const ElemArgs& a, const int64_t* inc_ptr, const in
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
   }
-  if (emean && felem) {
+  if (felem && inc_ptr) {
     rec_node_kernel<ET><<<rec_grid(a.n_nodes), 256, 0, s>>>(a, inc_ptr, inc_code, emean, felem, f_ext, strain, stress,
                                                             reaction);
     return cudaGetLastError();
@@ -210,10 +232,12 @@ cudaError_t launch_recover_t(const ElemArgs& a, const int64_t* inc_ptr, const in
 
 cudaError_t launch_recover(int t, const ElemArgs& a, const int64_t* inc_ptr, const int32_t* inc_code,
                            double* gp_stress, double* emean, double* felem, const double* f_ext, double* strain,
-                           double* stress, double* reaction, cudaStream_t s) {
+                           double* stress, double* reaction, bool thermal_load, cudaStream_t s) {
   switch (t) {
-#define CXG_REC(T) \
-  case T: return launch_recover_t<T>(a, inc_ptr, inc_code, gp_stress, emean, felem, f_ext, strain, stress, reaction, s);
+#define CXG_REC(T)                                                                                             \
+  case T:                                                                                                      \
+    return launch_recover_t<T>(a, inc_ptr, inc_code, gp_stress, emean, felem, f_ext, strain, stress, reaction, \
+                               thermal_load, s);
     CXG_REC(C3D4)
     CXG_REC(C3D10)
     CXG_REC(C3D8)

@@ -262,14 +262,36 @@ CXG_API int cxg_thermal_plan_create(const cxg_mesh_desc* mesh, const int32_t* t_
 CXG_API int cxg_assemble_conduction(cxg_plan* plan, const double* conductivity, const double* flux, double* vals,
                                     double* rhs, void* stream);
 
+/* ---- thermal strain (*EXPANSION with an applied temperature field) ---------------------
+ * Inputs of the reference's thermal-strain path (Material::expansion,
+ * Model::applied_temperature; element_temp_change / element_alpha, src/fem/stress.cpp:
+ * 76-105): node_temp[n_nodes] the applied temperature of every node, node_applied[n_nodes]
+ * 1 where a temperature is applied (NULL: every node), elem_alpha[n_elems] the expansion
+ * coefficient of the element's material at the element's mean temperature (nodes without
+ * an applied temperature counting as t_ref; 0 for elements without *EXPANSION),
+ * elem_tref[n_elems] the material's reference temperature. Host or device arrays, copied.
+ * node_temp = NULL clears. Once set, cxg_assemble_linear(_ex) adds the thermal-strain load
+ * to the rhs as assemble_linear_static does (src/fem/assembly.cpp:251-253; not with
+ * CXG_ACCUMULATE), and the field recovery uses sigma = D (eps - eps_th) and
+ * f_int = K u - f_th (stress.cpp:147-271). The material-point assembly ignores it, as the
+ * reference's does. */
+CXG_API int cxg_plan_set_thermal_strain(cxg_plan* plan, const double* node_temp, const uint8_t* node_applied,
+                                        const double* elem_alpha, const double* elem_tref);
+/* thermal_strain_load_vector (src/fem/loads.cpp:515-560): f_th[3*n_nodes] = sum_e
+ * int B^T D eps_th dV, eps_th = alpha sum_k N_k te_k on the normal components (zeros when
+ * no thermal strain is set). */
+CXG_API int cxg_thermal_strain_load(cxg_plan* plan, double* f_th, void* stream);
+
 /* ---- field recovery from a displacement field u[3*n_nodes] (linear elasticity) -------
  * recover_gauss_stress (src/fem/stress.cpp:147-187): gp_stress[6 * n_gauss_points],
- * sigma = D B u_e per Gauss point (Voigt, engineering shear), element order. */
+ * sigma = D (B u_e - eps_th) per Gauss point (Voigt, engineering shear; eps_th = 0 unless
+ * cxg_plan_set_thermal_strain), element order. */
 CXG_API int cxg_recover_gauss_stress(cxg_plan* plan, const double* u, double* gp_stress, void* stream);
-/* recover_fields (stress.cpp:189-271) without thermal strain: nodal strain and stress
+/* recover_fields (stress.cpp:189-271): nodal strain (mechanical, B u) and stress
  * [6 * n_nodes]: each incident element's Gauss-point values extrapolated to the node
  * (the mean for hexahedra, wedges and C3D4; the corner matrix and midside averages for
- * C3D10, include/calculixpp/fem/extrapolation.hpp:26-55), averaged over the elements; reaction[3 * n_nodes] = f_int - f_ext with f_int = sum_e K_e u_e. Any output
+ * C3D10, include/calculixpp/fem/extrapolation.hpp:26-55), averaged over the elements;
+ * reaction[3 * n_nodes] = f_int - f_ext with f_int = sum_e (K_e u_e - f_th_e). Any output
  * and f_ext may be NULL. C3D8R (hourglass forces) is rejected with CXG_ERR_UNSUPPORTED. */
 CXG_API int cxg_recover_fields(cxg_plan* plan, const double* u, const double* f_ext, double* strain,
                                double* stress, double* reaction, void* stream);
