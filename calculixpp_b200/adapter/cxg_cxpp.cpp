@@ -70,8 +70,6 @@ CudaAssembler::CudaAssembler(const cxpp::Model& model, Precision precision) : mo
     constant.push_back(ex.constant);
   }
   if (!model.springs.empty()) unsupported("*SPRING connectors");
-  for (cxpp::Real v : cxpp::fem::thermal_strain_load_vector(model))
-    if (v != 0.0) unsupported("a thermal-strain load");
 
   const std::vector<bool> active = model.element_active_mask();
   const std::vector<cxpp::ElasticIso> elastic = model.element_elastic();
@@ -146,6 +144,34 @@ CudaAssembler::CudaAssembler(const cxpp::Model& model, Precision precision) : mo
   col_idx_.resize(static_cast<std::size_t>(info.nnz));
   check(cxg_plan_get_pattern(plan_, row_ptr_.data(), col_idx_.data()));
   f_ext_ = cxpp::fem::external_load_vector(model);
+
+  // thermal strain (*EXPANSION with applied temperatures): the reference's own inputs,
+  // alpha evaluated at each element's mean temperature (the nodes without an applied
+  // temperature counting as t_ref, element_alpha, src/fem/stress.cpp:97-105)
+  if (model.has_thermal_strain()) {
+    const std::size_t N = mesh.num_nodes();
+    std::vector<double> node_temp(N, 0.0), alpha(E, 0.0), tref(E, 0.0);
+    std::vector<uint8_t> applied(N, 0);
+    for (const auto& [id, t] : model.applied_temperature) {
+      const cxpp::Index ni = mesh.node_index(id);
+      if (ni < 0) continue;
+      node_temp[static_cast<std::size_t>(ni)] = t;
+      applied[static_cast<std::size_t>(ni)] = 1;
+    }
+    const std::vector<std::optional<cxpp::Expansion>> expansion = model.element_expansion();
+    for (std::size_t k = 0; k < E; ++k) {
+      const std::optional<cxpp::Expansion>& ex = expansion[static_cast<std::size_t>(active_[k])];
+      if (!ex || ex->empty()) continue;
+      double tsum = 0.0;
+      for (int i = 0; i < npe; ++i) {
+        const std::size_t ni = static_cast<std::size_t>(conn[k * npe + i]);
+        tsum += applied[ni] ? node_temp[ni] : ex->t_ref;
+      }
+      alpha[k] = ex->alpha.at(tsum / static_cast<double>(npe));
+      tref[k] = ex->t_ref;
+    }
+    check(cxg_plan_set_thermal_strain(plan_, node_temp.data(), applied.data(), alpha.data(), tref.data()));
+  }
 }
 
 CudaAssembler::~CudaAssembler() { cxg_plan_destroy(plan_); }

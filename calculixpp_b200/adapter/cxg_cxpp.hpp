@@ -12,8 +12,9 @@
 // per-element sections and materials (elastic, J2 plasticity), *BOUNDARY single-point
 // constraints, *EQUATION and the other constraints the reference expands into linear
 // equations (through its own constraint transform), *CLOAD/*DLOAD/*GRAV loads through
-// external_load_vector, deactivated elements (*MODEL CHANGE). Anything else (several
-// element types, springs, thermal-strain loads, hyperelastic or user materials) throws
+// external_load_vector, thermal strain (*EXPANSION with applied temperatures),
+// deactivated elements (*MODEL CHANGE). Anything else (several element types, springs,
+// hyperelastic or user materials) throws
 // std::runtime_error naming the feature, before any GPU work.
 #pragma once
 

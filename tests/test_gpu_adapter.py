@@ -81,6 +81,34 @@ def test_solve_linear_static_on_gpu_assembly(cuda, ref, adapter, etype):
     assert rel_fro(u_mx, u_cpu) <= 1e-6
 
 
+@pytest.mark.parametrize("etype", [mg.C3D8, mg.C3D20])
+def test_thermal_strain_model(cuda, ref, adapter, etype):
+    """A model with *EXPANSION (a constant alpha on one section, an alpha(T) table on the
+    other) and temperatures applied on part of the nodes: the adapter passes the reference
+    model's own thermal inputs to the plan, so the linear system's rhs carries the
+    thermal-strain load (assemble_linear_static, src/fem/assembly.cpp:251-253) and the
+    solve agrees with the reference pipeline on the CPU."""
+    quad = etype == mg.C3D20
+    m, spc, cl, em = _cantilever(etype, (4, 2, 2) if quad else (8, 3, 3), seed=30 + etype)
+    mats = [make_material(210000.0, 0.3), make_material(70000.0, 0.33)]
+    rm = ref.model(m, mats, em, spc, cl)
+    rm.set_expansion([([1.2e-5], [0.0]), ([1.0e-5, 2.0e-5], [0.0, 300.0])], [20.0, 0.0])
+    rng = np.random.default_rng(etype)
+    nodes = np.flatnonzero(rng.uniform(size=m.n_nodes) < 0.8)
+    rm.set_temperature(nodes, rng.uniform(50.0, 250.0, nodes.size))
+    want = rm.assemble_linear_static()
+    h = adapter.assembler(rm)
+    try:
+        _, _, _, rhs = adapter.assemble_linear(h)
+    finally:
+        adapter.free(h)
+    assert rel_fro(rhs, want["rhs"]) <= 1e-12
+    u_cpu, s_cpu = adapter.solve_linear_static(rm, gpu=0)
+    u_gpu, s_gpu = adapter.solve_linear_static(rm, gpu=1)
+    assert rel_fro(u_gpu, u_cpu) <= 1e-10
+    assert rel_fro(s_gpu, s_cpu) <= 1e-9
+
+
 @pytest.mark.parametrize("etype", [mg.C3D8, mg.C3D8R, mg.C3D20R, mg.C3D15])
 def test_linear_system_matches_reference(cuda, ref, adapter, etype):
     quad = etype in (mg.C3D20R, mg.C3D15)
