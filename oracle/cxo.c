@@ -1082,10 +1082,151 @@ int cxo_element_conduction(int type, const double* x, double k, double* Kt) {
   return 0;
 }
 
-cxo_system* cxo_assemble_conduction(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
-                                    const int64_t* conn_ptr, const int32_t* conn, const double* conductivity,
-                                    const int32_t* t_dof_eq, const double* t_prescribed, int32_t n_free,
-                                    const double* flux) {
+/* ---- element faces: src/fem/loads.cpp:13-190, 313-389 --------------------------- */
+/* face node tables (0-based), loads.cpp:16-46: tet (T3/T6), hex (Q4/Q8), wedge */
+static const int kFaceTet[4][6] = {{0, 2, 1, 6, 5, 4}, {0, 1, 3, 4, 8, 7}, {1, 2, 3, 5, 9, 8}, {0, 3, 2, 7, 9, 6}};
+static const int kFaceHex[6][8] = {{0, 1, 2, 3, 8, 9, 10, 11},   {4, 7, 6, 5, 15, 14, 13, 12},
+                                   {0, 4, 5, 1, 16, 12, 17, 8},  {1, 5, 6, 2, 17, 13, 18, 9},
+                                   {2, 6, 7, 3, 18, 14, 19, 10}, {3, 7, 4, 0, 19, 15, 16, 11}};
+static const int kFaceWedge[5][8] = {{0, 2, 1, 8, 7, 6, -1, -1},
+                                     {3, 4, 5, 12, 13, 14, -1, -1},
+                                     {0, 1, 4, 3, 6, 10, 12, 9},
+                                     {1, 2, 5, 4, 7, 11, 13, 10},
+                                     {2, 0, 3, 5, 8, 9, 14, 11}};
+
+/* face_kind_of, loads.cpp:317-350: local face nodes fn, count *nf, *quad; -1 on error */
+static int face_kind(int type, int face, int* fn, int* nf, int* quad) {
+  const int* row = NULL;
+  switch (type) {
+    case T_C3D4:
+    case T_C3D10:
+      if (face < 1 || face > 4) return fail("tet face must be 1..4");
+      *nf = type == T_C3D4 ? 3 : 6;
+      *quad = 0;
+      row = kFaceTet[face - 1];
+      break;
+    case T_C3D8:
+    case T_C3D8R:
+    case T_C3D20:
+    case T_C3D20R:
+      if (face < 1 || face > 6) return fail("hex face must be 1..6");
+      *nf = (type == T_C3D8 || type == T_C3D8R) ? 4 : 8;
+      *quad = 1;
+      row = kFaceHex[face - 1];
+      break;
+    case T_C3D6:
+    case T_C3D15:
+      if (face < 1 || face > 5) return fail("wedge face must be 1..5");
+      *quad = face > 2;
+      *nf = face <= 2 ? (type == T_C3D6 ? 3 : 6) : (type == T_C3D6 ? 4 : 8);
+      row = kFaceWedge[face - 1];
+      break;
+    default:
+      return fail("unsupported element type for surface load");
+  }
+  for (int i = 0; i < *nf; ++i) fn[i] = row[i];
+  return 0;
+}
+
+/* face_shape, loads.cpp:83-138: T3/T6 in barycentric (a, b), Q4/Q8 on [-1,1]^2 */
+static void face_shape(int quad, int nf, double a, double b, double* N, double* dxi, double* deta) {
+  for (int i = 0; i < 8; ++i) N[i] = dxi[i] = deta[i] = 0.0;
+  if (!quad) {
+    const double l1 = 1.0 - a - b, l2 = a, l3 = b;
+    if (nf == 3) {
+      N[0] = l1; N[1] = l2; N[2] = l3;
+      dxi[0] = -1; dxi[1] = 1; dxi[2] = 0;
+      deta[0] = -1; deta[1] = 0; deta[2] = 1;
+      return;
+    }
+    N[0] = l1 * (2 * l1 - 1); N[1] = l2 * (2 * l2 - 1); N[2] = l3 * (2 * l3 - 1);
+    N[3] = 4 * l1 * l2; N[4] = 4 * l2 * l3; N[5] = 4 * l3 * l1;
+    dxi[0] = -(4 * l1 - 1); dxi[1] = 4 * l2 - 1; dxi[2] = 0; dxi[3] = 4 * (l1 - l2); dxi[4] = 4 * l3; dxi[5] = -4 * l3;
+    deta[0] = -(4 * l1 - 1); deta[1] = 0; deta[2] = 4 * l3 - 1; deta[3] = -4 * l2; deta[4] = 4 * l2;
+    deta[5] = 4 * (l1 - l3);
+    return;
+  }
+  static const int sgn[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+  if (nf == 4) {
+    for (int k = 0; k < 4; ++k) {
+      const double g = 1.0 + sgn[k][0] * a, h = 1.0 + sgn[k][1] * b;
+      N[k] = 0.25 * g * h;
+      dxi[k] = 0.25 * sgn[k][0] * h;
+      deta[k] = 0.25 * sgn[k][1] * g;
+    }
+    return;
+  }
+  for (int k = 0; k < 4; ++k) {
+    const double sa = sgn[k][0], sb = sgn[k][1];
+    const double g = 1.0 + sa * a, h = 1.0 + sb * b;
+    N[k] = 0.25 * g * h * (sa * a + sb * b - 1.0);
+    dxi[k] = 0.25 * (sa * h * (sa * a + sb * b - 1.0) + g * h * sa);
+    deta[k] = 0.25 * (sb * g * (sa * a + sb * b - 1.0) + g * h * sb);
+  }
+  static const int edge_axis[4] = {0, 1, 0, 1};
+  static const double edge_fix[4] = {-1, 1, 1, -1};
+  for (int e = 0; e < 4; ++e) {
+    const int node = 4 + e;
+    if (edge_axis[e] == 0) {
+      const double sb = edge_fix[e];
+      N[node] = 0.5 * (1.0 - a * a) * (1.0 + sb * b);
+      dxi[node] = 0.5 * (-2.0 * a) * (1.0 + sb * b);
+      deta[node] = 0.5 * (1.0 - a * a) * sb;
+    } else {
+      const double sa = edge_fix[e];
+      N[node] = 0.5 * (1.0 + sa * a) * (1.0 - b * b);
+      dxi[node] = 0.5 * sa * (1.0 - b * b);
+      deta[node] = 0.5 * (1.0 + sa * a) * (-2.0 * b);
+    }
+  }
+}
+
+/* face_surface_integrals, loads.cpp:361-389: mass[nf*nf] = int N_i N_j dA and
+ * load[nf] = int N_i dA over face `face` of an element with node coordinates x; the
+ * 3-point triangle rule or the 2x2 quad rule (loads.cpp:54-66), dA = |t_xi x t_eta| w. */
+static int face_surface_integrals(int type, int face, const double* x, int* fn, int* nf_out, double* mass,
+                                  double* load) {
+  static const double kTri[3][3] = {{1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0},
+                                    {2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0},
+                                    {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0}};
+  const double qg = 0.577350269189625764;
+  const double kQuad[4][3] = {{-qg, -qg, 1.0}, {qg, -qg, 1.0}, {qg, qg, 1.0}, {-qg, qg, 1.0}};
+  int nf = 0, quad = 0;
+  if (face_kind(type, face, fn, &nf, &quad)) return -1;
+  *nf_out = nf;
+  for (int i = 0; i < nf; ++i) load[i] = 0.0;
+  for (int i = 0; i < nf * nf; ++i) mass[i] = 0.0;
+  const int ng = quad ? 4 : 3;
+  for (int q = 0; q < ng; ++q) {
+    const double* gp = quad ? kQuad[q] : kTri[q];
+    double N[8], dxi[8], deta[8], txi[3] = {0, 0, 0}, teta[3] = {0, 0, 0};
+    face_shape(quad, nf, gp[0], gp[1], N, dxi, deta);
+    for (int i = 0; i < nf; ++i)
+      for (int d = 0; d < 3; ++d) {
+        txi[d] += dxi[i] * x[3 * fn[i] + d];
+        teta[d] += deta[i] * x[3 * fn[i] + d];
+      }
+    const double nrm[3] = {txi[1] * teta[2] - txi[2] * teta[1], txi[2] * teta[0] - txi[0] * teta[2],
+                           txi[0] * teta[1] - txi[1] * teta[0]};
+    const double dA = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]) * gp[2];
+    for (int i = 0; i < nf; ++i) {
+      const double Ni = N[i];
+      load[i] += Ni * dA;
+      for (int j = 0; j < nf; ++j) mass[i * nf + j] += Ni * N[j] * dA;
+    }
+  }
+  return 0;
+}
+
+/* assemble_conduction, thermal.cpp:92-141, with *FILM faces (thermal.cpp:113-126): after
+ * the elements, each film adds h * mass to the matrix (scattered like an element block)
+ * and h * T_sink * load to the free rhs rows; then the nodal flux. */
+cxo_system* cxo_assemble_conduction_films(int64_t n_nodes, const double* coords, int64_t n_elems,
+                                          const int32_t* types, const int64_t* conn_ptr, const int32_t* conn,
+                                          const double* conductivity, const int32_t* t_dof_eq,
+                                          const double* t_prescribed, int32_t n_free, const double* flux,
+                                          int64_t n_films, const int64_t* film_elem, const int32_t* film_face,
+                                          const double* film_h, const double* film_sink) {
   triplets_t t = {0};
   double* rhs = calloc((size_t)n_free + 1, sizeof(double));
   double x[3 * MAXN], Kt[MAXN * MAXN];
@@ -1108,6 +1249,28 @@ cxo_system* cxo_assemble_conduction(int64_t n_nodes, const double* coords, int64
     if (cxo_element_conduction(types[e], x, conductivity[e], Kt)) goto error;
     if (scatter(Kt, n, gd, t_dof_eq, t_prescribed, n_free, &t, rhs)) goto error;
   }
+  for (int64_t f = 0; f < n_films; ++f) {
+    const int64_t e = film_elem[f];
+    if (e < 0 || e >= n_elems) {
+      fail("*FILM references unknown element");
+      goto error;
+    }
+    const int n = cxo_nodes_per_element(types[e]);
+    const int32_t* c = conn + conn_ptr[e];
+    for (int k = 0; k < n; ++k)
+      for (int d = 0; d < 3; ++d) x[3 * k + d] = coords[3 * (int64_t)c[k] + d];
+    int fn[8], nf = 0;
+    double mass[64], load[8], hM[64];
+    int64_t fg[8];
+    if (face_surface_integrals(types[e], film_face[f], x, fn, &nf, mass, load)) goto error;
+    for (int i = 0; i < nf * nf; ++i) hM[i] = film_h[f] * mass[i];
+    for (int i = 0; i < nf; ++i) fg[i] = c[fn[i]];
+    if (scatter(hM, nf, fg, t_dof_eq, t_prescribed, n_free, &t, rhs)) goto error;
+    for (int i = 0; i < nf; ++i) {
+      const int32_t eq = t_dof_eq[fg[i]];
+      if (eq >= 0) rhs[eq] += film_h[f] * film_sink[f] * load[i];
+    }
+  }
   if (flux)
     for (int64_t i = 0; i < n_nodes; ++i)
       if (t_dof_eq[i] >= 0) rhs[t_dof_eq[i]] += flux[i];
@@ -1121,6 +1284,14 @@ error:
   free(t.val);
   free(rhs);
   return NULL;
+}
+
+cxo_system* cxo_assemble_conduction(int64_t n_nodes, const double* coords, int64_t n_elems, const int32_t* types,
+                                    const int64_t* conn_ptr, const int32_t* conn, const double* conductivity,
+                                    const int32_t* t_dof_eq, const double* t_prescribed, int32_t n_free,
+                                    const double* flux) {
+  return cxo_assemble_conduction_films(n_nodes, coords, n_elems, types, conn_ptr, conn, conductivity, t_dof_eq,
+                                       t_prescribed, n_free, flux, 0, NULL, NULL, NULL, NULL);
 }
 
 /* ---- field recovery and thermal strain: src/fem/stress.cpp, src/fem/loads.cpp ---- */

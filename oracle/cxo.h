@@ -129,6 +129,14 @@ cxo_system* cxo_assemble_conduction(int64_t n_nodes, const double* coords, int64
                                     const int64_t* conn_ptr, const int32_t* conn, const double* conductivity,
                                     const int32_t* t_dof_eq, const double* t_prescribed, int32_t n_free,
                                     const double* flux);
+/* assemble_conduction with *FILM faces (thermal.cpp:113-126): film f on face film_face[f]
+ * (1-based) of element film_elem[f], coefficient film_h[f], sink temperature film_sink[f]. */
+cxo_system* cxo_assemble_conduction_films(int64_t n_nodes, const double* coords, int64_t n_elems,
+                                          const int32_t* types, const int64_t* conn_ptr, const int32_t* conn,
+                                          const double* conductivity, const int32_t* t_dof_eq,
+                                          const double* t_prescribed, int32_t n_free, const double* flux,
+                                          int64_t n_films, const int64_t* film_elem, const int32_t* film_face,
+                                          const double* film_h, const double* film_sink);
 
 int cxo_system_info(const cxo_system* s, int32_t* n_free, int64_t* nnz);
 int cxo_system_copy(const cxo_system* s, int64_t* row_ptr, int32_t* col_idx,

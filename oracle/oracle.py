@@ -110,6 +110,8 @@ PORT_SIGS = dict(_COMMON, **{
     "recover_fields_th": (_i, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                _vp, _vp, _vp]),
     "assemble_conduction": (_vp, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _i32t, _vp]),
+    "assemble_conduction_films": (_vp, [_i64t, _vp, _i64t, _vp, _vp, _vp, _vp, _vp, _vp, _i32t, _vp, _i64t, _vp,
+                                        _vp, _vp, _vp]),
     "system_info": (_i, [_vp, _vp, _vp]),
     "system_copy": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "system_free": (None, [_vp]),
@@ -129,6 +131,7 @@ REF_SIGS = dict(_COMMON, **{
     "recover_fields": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "model_set_expansion": (_i, [_vp, _i32t, _vp, _vp, _vp, _vp]),
     "model_set_temperature": (_i, [_vp, _i64t, _vp, _vp]),
+    "model_add_film": (_i, [_vp, _i64t, _i32t, _d, _d]),
     "thermal_strain_load_vector": (_i, [_vp, _vp]),
     "assemble_conduction": (_vp, [_vp, _i32t, _vp, _i64t, _vp, _vp]),
     "assemble_linear_static": (_vp, [_vp]),
@@ -419,6 +422,20 @@ class Port(_Base):
               _p(_i32(t_dof_eq)), _p(_f64(t_prescribed)), int(n_free), _p(None if flux is None else _f64(flux)))
         return self._system(s)
 
+    def assemble_conduction_films(self, mesh, conductivity, t_dof_eq, t_prescribed, n_free, films, flux=None):
+        """assemble_conduction with *FILM faces (thermal.cpp:92-141); films = (elem, face,
+        h, sink) arrays, elements 0-based, faces 1-based: (rp, ci, vals, rhs)."""
+        E = mesh.n_elems
+        n = mesh.conn.shape[1]
+        fe = np.ascontiguousarray(films[0], dtype=np.int64)
+        ff, fh, fs = _i32(films[1]), _f64(films[2]), _f64(films[3])
+        f = self._fn("assemble_conduction_films")
+        s = f(mesh.n_nodes, _p(_f64(mesh.coords)), E, _p(np.full(E, mesh.etype, dtype=np.int32)),
+              _p(np.arange(E + 1, dtype=np.int64) * n), _p(_i32(mesh.conn.ravel())), _p(_f64(conductivity)),
+              _p(_i32(t_dof_eq)), _p(_f64(t_prescribed)), int(n_free), _p(None if flux is None else _f64(flux)),
+              fe.size, _p(fe), _p(ff), _p(fh), _p(fs))
+        return self._system(s)
+
     def element_compliance_grad_fd(self, etype, coords, ue, E, nu, h):
         n = NODES[etype]
         out = np.zeros(3 * n)
@@ -569,6 +586,10 @@ class RefModel:
         tr = _f64(trefs)
         self.ref._check(self.ref._fn("model_set_expansion")(_vp(self.h), C.c_int32(npts.size), _p(npts), _p(vals),
                                                              _p(temps), _p(tr)))
+
+    def add_film(self, elem, face, h, sink):
+        """A *FILM face (Model::films): element 0-based, face 1-based."""
+        self.ref._check(self.ref._fn("model_add_film")(_vp(self.h), int(elem), int(face), float(h), float(sink)))
 
     def set_temperature(self, nodes, temps):
         """Applied temperatures (Model::applied_temperature), nodes 0-based."""

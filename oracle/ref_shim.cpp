@@ -353,6 +353,21 @@ int ref_model_set_expansion(void* model, int32_t n_mats, const int32_t* n_points
   }
 }
 
+// A *FILM face (Model::films): element 0-based, face 1-based.
+int ref_model_add_film(void* model, int64_t elem, int32_t face, double h, double sink) {
+  try {
+    Film f;
+    f.elem_id = static_cast<Index>(elem + 1);
+    f.face = face;
+    f.h = h;
+    f.sink_temp = sink;
+    static_cast<RefModel*>(model)->model.films.push_back(f);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
 // Applied temperatures (Model::applied_temperature): nodes 0-based.
 int ref_model_set_temperature(void* model, int64_t n, const int32_t* nodes, const double* temps) {
   try {

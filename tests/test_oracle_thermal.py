@@ -68,3 +68,47 @@ def test_thermal_strain_identical(port, ref, etype):
     b = rm.recover_fields(u)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+N_FACES = {mg.C3D4: 4, mg.C3D10: 4, mg.C3D8: 6, mg.C3D8R: 6, mg.C3D20: 6, mg.C3D20R: 6, mg.C3D6: 5, mg.C3D15: 5}
+
+
+def film_case(etype, seed):
+    """Films on random element faces (some elements with two), prescribed temperatures on
+    one face."""
+    from tests.helpers import box_model as _box
+    quad = etype in (mg.C3D20, mg.C3D20R, mg.C3D15, mg.C3D10)
+    dims = (2, 2, 1) if quad else (3, 2, 2)
+    model = _box(etype, *dims, jitter=0.1, seed=seed)
+    m = model.mesh
+    rng = np.random.default_rng(seed)
+    elems = rng.choice(m.n_elems, size=min(m.n_elems, 6), replace=False)
+    elems = np.concatenate([elems, elems[:2]])
+    faces = rng.integers(1, N_FACES[etype] + 1, size=elems.size)
+    h = rng.uniform(5.0, 50.0, elems.size)
+    sink = rng.uniform(-20.0, 80.0, elems.size)
+    hot = mg.face_nodes(m, 0, 0.0)
+    tv = np.full(hot.size, 100.0)
+    return model, m, (elems, faces, h, sink), hot, tv
+
+
+@pytest.mark.parametrize("etype", ALL_TYPES)
+def test_conduction_films_identical(port, ref, etype):
+    """assemble_conduction with *FILM faces (src/fem/thermal.cpp:113-126, face integrals of
+    loads.cpp:361-389) of the restatement against the reference, bit for bit."""
+    from calculixpp_b200.meshgen import thermal_dof_map
+    from oracle.oracle import coo_to_csr
+    model, m, films, tn, tv = film_case(etype, 90 + etype)
+    mats, em = per_element_materials(model)
+    k_mat = 40.0 + 5.0 * np.arange(len(mats))
+    rm = ref.model(m, mats, em, model.spc, model.cloads)
+    for e, f, h, s in zip(*films):
+        rm.add_film(e, f, h, s)
+    s = rm.assemble_conduction(k_mat, tn, tv)
+    deq, pre, nf = thermal_dof_map(m.n_nodes, tn, tv)
+    rp, ci, v = coo_to_csr(s["n_free"], s["rows"], s["cols"], s["vals"])
+    rp2, ci2, v2, rhs2 = port.assemble_conduction_films(m, k_mat[em], deq, pre, nf, films)
+    assert np.array_equal(rp, rp2) and np.array_equal(ci, ci2) and np.array_equal(v, v2)
+    assert np.array_equal(s["rhs"], rhs2)
+    _, _, v0, rhs0 = port.assemble_conduction(m, k_mat[em], deq, pre, nf)
+    assert not np.array_equal(rhs0, rhs2)
