@@ -88,6 +88,7 @@ SIGNATURES = {
     "cxg_plan_set_j2_fp32_return": (C.c_int, [_vp, C.c_int32]),
     "cxg_plan_set_thermal_strain": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "cxg_thermal_strain_load": (C.c_int, [_vp, _vp, _vp]),
+    "cxg_thermal_plan_set_films": (C.c_int, [_vp, C.c_int64, _vp, _vp, _vp, _vp]),
     "cxg_plan_set_ring_bytes": (C.c_int, [_vp, C.c_int64]),
     "cxg_plan_create_mpc": (C.c_int, [_vp, _vp, _vp, C.c_int32, _vp]),
     "cxg_solve_sparse": (C.c_int, [C.c_int32, C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_int32, C.c_double, C.c_int32,

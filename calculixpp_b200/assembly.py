@@ -470,6 +470,19 @@ class ThermalPlan(Plan):
         self.n_gauss = int(info.n_gauss_points)
         self._pattern = None
 
+    def set_films(self, elem=(), face=(), h=(), sink=()):
+        """*FILM faces (cxg_thermal_plan_set_films): element (0-based), face (1-based),
+        coefficient and sink temperature per film; empty clears."""
+        e = np.ascontiguousarray(elem, dtype=np.int64)
+        f = np.ascontiguousarray(face, dtype=np.int32)
+        hh = np.ascontiguousarray(h, dtype=np.float64)
+        sk = np.ascontiguousarray(sink, dtype=np.float64)
+        if not (e.size == f.size == hh.size == sk.size):
+            raise ValueError("elem, face, h and sink must have one entry per film")
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p) if a.size else None
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.cxg_thermal_plan_set_films(self.h, e.size, ptr(e), ptr(f), ptr(hh), ptr(sk)))
+
     def assemble_conduction(self, conductivity, flux=None, vals=None, rhs=None, check=True):
         """(Kt_ff values, rhs = q_f - Kt_fc T_c); conductivity per element, flux per node."""
         dev = self.device

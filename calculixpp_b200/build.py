@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libcxg.so")
 SOURCES = ["cxg_api.cu", "cxg_kernels.cu", "cxg_pattern.cu", "cxg_v2.cu", "cxg_solve.cu", "cxg_batch.cu", "cxg_recover.cu",
-           "cxg_refpattern.cu", "cxg_mpc.cu", "cxg_sparse_solve.cu"]
+           "cxg_refpattern.cu", "cxg_mpc.cu", "cxg_sparse_solve.cu", "cxg_film.cu"]
 # Per-file flags: the reference-pattern mask evaluates K_e in the reference's own FP64
 # operation order, so it must not contract multiply-adds.
 EXTRA_FLAGS = {"cxg_refpattern.cu": ["-fmad=false"]}

@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "cxg_faces.hpp"
 #include "cxg_plan.hpp"
 
 using namespace cxg;
@@ -608,6 +609,7 @@ int cxg_plan_destroy(cxg_plan* p) {
   if (!p) return CXG_OK;
   if (p->last_stream) cudaStreamSynchronize(p->last_stream);
   thermal::release(p);
+  cudaFree(p->film_mem);
   void* bufs[] = {p->coords, p->conn, p->young, p->poisson, p->elem_mat, p->mats, p->dof_eq, p->prescribed,
                   p->pat.row_ptr, p->pat.col_idx, p->pat.node_base, p->pat.node_rowlen, p->pat.node_mask,
                   p->pat.node_eq0, p->pat.slot, p->pat.adj_len, p->pat.bnd_ptr, p->pat.bnd_node, p->pat.inc_ptr, p->pat.inc_code, p->state[0], p->state[1],
@@ -1026,6 +1028,108 @@ int cxg_thermal_plan_create(const cxg_mesh_desc* m, const int32_t* t_dof_eq, con
   return CXG_OK;
 }
 
+int cxg_thermal_plan_set_films(cxg_plan* p, int64_t n_films, const int64_t* elem, const int32_t* face,
+                               const double* h, const double* sink) {
+  if (!p || n_films < 0 || (n_films > 0 && (!elem || !face || !h || !sink)))
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");
+  if (!p->thermal) return set_err(CXG_ERR_INVALID_ARGUMENT, "films need a plan from cxg_thermal_plan_create");
+  if (n_films >= (int64_t{1} << 28)) return set_err(CXG_ERR_UNSUPPORTED, "too many films");
+  if (p->last_stream) CHECK_CUDA(cudaStreamSynchronize(p->last_stream), "synchronize");
+  cudaFree(p->film_mem);
+  p->film_mem = nullptr;
+  p->films = FilmArgs{};
+  if (n_films == 0) return CXG_OK;
+  // host arrays (staged copies when the caller passed device pointers)
+  std::vector<int64_t> fe(static_cast<size_t>(n_films));
+  std::vector<int32_t> ff(static_cast<size_t>(n_films));
+  std::vector<double> fh(static_cast<size_t>(n_films)), fs(static_cast<size_t>(n_films));
+  CHECK_CUDA(cudaMemcpy(fe.data(), elem, sizeof(int64_t) * fe.size(), cudaMemcpyDefault), "film elements");
+  CHECK_CUDA(cudaMemcpy(ff.data(), face, sizeof(int32_t) * ff.size(), cudaMemcpyDefault), "film faces");
+  CHECK_CUDA(cudaMemcpy(fh.data(), h, sizeof(double) * fh.size(), cudaMemcpyDefault), "film coefficients");
+  CHECK_CUDA(cudaMemcpy(fs.data(), sink, sizeof(double) * fs.size(), cudaMemcpyDefault), "film sinks");
+  std::vector<int32_t> conn(static_cast<size_t>(p->n_elems) * nodes_of(p->type));
+  CHECK_CUDA(cudaMemcpy(conn.data(), p->conn, sizeof(int32_t) * conn.size(), cudaMemcpyDeviceToHost), "connectivity");
+  const int n = nodes_of(p->type);
+  // films grouped by element, film order kept within each element
+  std::vector<int32_t> order(static_cast<size_t>(n_films));
+  for (int32_t i = 0; i < n_films; ++i) order[static_cast<size_t>(i)] = i;
+  for (int64_t i = 0; i < n_films; ++i) {
+    int fn[8], nf = 0;
+    bool quad = false;
+    if (fe[static_cast<size_t>(i)] < 0 || fe[static_cast<size_t>(i)] >= p->n_elems)
+      return set_err(CXG_ERR_INVALID_ARGUMENT, "*FILM references unknown element (film " + std::to_string(i) + ")");
+    if (!face_nodes_of(p->type, ff[static_cast<size_t>(i)], fn, &nf, &quad))
+      return set_err(CXG_ERR_INVALID_ARGUMENT, "face number out of range for this element type (film " +
+                                                   std::to_string(i) + ")");
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return fe[x] < fe[y]; });
+  std::vector<int64_t> felem;
+  std::vector<int32_t> fptr(1, 0);
+  for (size_t k = 0; k < order.size(); ++k) {
+    if (k == 0 || fe[static_cast<size_t>(order[k])] != fe[static_cast<size_t>(order[k - 1])]) {
+      if (k) fptr.push_back(static_cast<int32_t>(k));
+      felem.push_back(fe[static_cast<size_t>(order[k])]);
+    }
+  }
+  fptr.push_back(static_cast<int32_t>(order.size()));
+  // per face node, its (film, local index) entries in film order
+  std::vector<std::pair<int64_t, int32_t>> inc;
+  for (int32_t i = 0; i < n_films; ++i) {
+    int fn[8], nf = 0;
+    bool quad = false;
+    face_nodes_of(p->type, ff[static_cast<size_t>(i)], fn, &nf, &quad);
+    for (int j = 0; j < nf; ++j)
+      inc.emplace_back(conn[static_cast<size_t>(fe[static_cast<size_t>(i)]) * n + fn[j]], i * 8 + j);
+  }
+  std::stable_sort(inc.begin(), inc.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+  std::vector<int64_t> fnode;
+  std::vector<int32_t> fnptr(1, 0), fnlist;
+  for (size_t k = 0; k < inc.size(); ++k) {
+    if (k == 0 || inc[k].first != inc[k - 1].first) {
+      if (k) fnptr.push_back(static_cast<int32_t>(k));
+      fnode.push_back(inc[k].first);
+    }
+    fnlist.push_back(inc[k].second);
+  }
+  fnptr.push_back(static_cast<int32_t>(inc.size()));
+  // one device block: int64 arrays, doubles, then int32 arrays
+  const size_t nF = static_cast<size_t>(n_films);
+  const size_t bytes = 8 * (felem.size() + fnode.size() + 3 * nF + 8 * nF) +
+                       4 * (fptr.size() + order.size() + nF + fnptr.size() + fnlist.size()) + 64;
+  char* mem = nullptr;
+  CHECK_CUDA(cudaMalloc(&mem, bytes), "film arrays");
+  p->film_mem = mem;
+  size_t off = 0;
+  auto put = [&](const void* src, size_t b) {
+    char* dst = mem + off;
+    off += (b + 7) / 8 * 8;
+    return cudaMemcpy(dst, src, b, cudaMemcpyHostToDevice) == cudaSuccess ? dst : nullptr;
+  };
+  FilmArgs& F = p->films;
+  F.n_films = n_films;
+  F.n_felem = static_cast<int64_t>(felem.size());
+  F.n_fnode = static_cast<int64_t>(fnode.size());
+  F.felem = reinterpret_cast<const int64_t*>(put(felem.data(), 8 * felem.size()));
+  F.fnode = reinterpret_cast<const int64_t*>(put(fnode.data(), 8 * fnode.size()));
+  F.h = reinterpret_cast<const double*>(put(fh.data(), 8 * nF));
+  F.sink = reinterpret_cast<const double*>(put(fs.data(), 8 * nF));
+  F.load = reinterpret_cast<double*>(mem + off);
+  off += 8 * 8 * nF;
+  F.fptr = reinterpret_cast<const int32_t*>(put(fptr.data(), 4 * fptr.size()));
+  F.flist = reinterpret_cast<const int32_t*>(put(order.data(), 4 * order.size()));
+  F.face = reinterpret_cast<const int32_t*>(put(ff.data(), 4 * nF));
+  F.fnptr = reinterpret_cast<const int32_t*>(put(fnptr.data(), 4 * fnptr.size()));
+  F.fnlist = reinterpret_cast<const int32_t*>(put(fnlist.data(), 4 * fnlist.size()));
+  if (off > bytes || !F.felem || !F.fnode || !F.h || !F.sink || !F.fptr || !F.flist || !F.face || !F.fnptr ||
+      !F.fnlist) {
+    cudaFree(p->film_mem);
+    p->film_mem = nullptr;
+    p->films = FilmArgs{};
+    return set_err(CXG_ERR_CUDA, "film arrays upload");
+  }
+  return CXG_OK;
+}
+
 int cxg_assemble_conduction(cxg_plan* p, const double* conductivity, const double* flux, double* vals, double* rhs,
                             void* stream) {
   if (!p || !conductivity || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "plan, conductivity and vals are required");
@@ -1040,8 +1144,8 @@ int cxg_assemble_conduction(cxg_plan* p, const double* conductivity, const doubl
   if (!rc) rc = staged(p, 1, rhs, rb, false, s, &dr);
   if (!rc) rc = staged(p, 5, conductivity, sizeof(double) * static_cast<size_t>(p->n_elems), true, s, &dk);
   if (rc) return rc;
-  if (flux) {
-    // nodal flux into component 0 of a 3N load vector (plan staging slot 2)
+  if (flux || p->films.n_films > 0) {
+    // nodal flux (and film loads) into component 0 of a 3N load vector (plan staging slot 2)
     if (p->stage_bytes[2] < 24 * N) {
       cudaFree(p->stage[2]);
       p->stage[2] = nullptr;
@@ -1051,7 +1155,7 @@ int cxg_assemble_conduction(cxg_plan* p, const double* conductivity, const doubl
     }
     df = p->stage[2];
     CHECK_CUDA(cudaMemsetAsync(df, 0, 24 * N, s), "flux staging");
-    CHECK_CUDA(cudaMemcpy2DAsync(df, 24, flux, 8, 8, N, cudaMemcpyDefault, s), "flux upload");
+    if (flux) CHECK_CUDA(cudaMemcpy2DAsync(df, 24, flux, 8, 8, N, cudaMemcpyDefault, s), "flux upload");
   }
   const size_t need = v2_edata_bytes(p->type, p->n_elems, CXG_FP64);
   if (p->edata_bytes < need) {
@@ -1068,6 +1172,9 @@ int cxg_assemble_conduction(cxg_plan* p, const double* conductivity, const doubl
   a.rhs = static_cast<double*>(dr);
   const V2Args v = v2_args(p, static_cast<const double*>(df), false);
   CHECK_CUDA(launch_scalar_pass(p->type, 4, a, v, static_cast<const double*>(dk), nullptr, s), "element pass");
+  if (p->films.n_films > 0)
+    CHECK_CUDA(launch_films(p->type, a, p->films, static_cast<double*>(p->edata), static_cast<double*>(df), s),
+               "film faces");
   LaunchCfg gather_only;
   gather_only.passes = 2;
   CHECK_CUDA(launch_v2(p->type, MODE_LINEAR, CXG_FP64, a, v, s, gather_only), "row gather");

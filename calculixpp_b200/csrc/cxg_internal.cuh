@@ -206,6 +206,26 @@ cudaError_t launch_state_transpose(const double* src, double* dst, int64_t G, bo
 cudaError_t launch_recover(int elem_type, const ElemArgs& a, const int64_t* inc_ptr, const int32_t* inc_code,
                            double* gp_stress, double* emean, double* felem, const double* f_ext, double* strain,
                            double* stress, double* reaction, bool thermal_load, cudaStream_t s);
+// *FILM faces of a temperature plan (cxg_film.cu), device arrays built once per film set:
+// films grouped by element (felem[g] owns flist[fptr[g] .. fptr[g+1]), in film order),
+// and per face node the (film, face-local index) entries film * 8 + i it receives
+// (fnode[g] owns fnlist[fnptr[g] .. fnptr[g+1]), in film order); load[8 * n_films] holds
+// h T_sink int N_i dA between the two passes.
+struct FilmArgs {
+  int64_t n_films = 0, n_felem = 0, n_fnode = 0;
+  const int64_t* felem = nullptr;
+  const int32_t* fptr = nullptr;
+  const int32_t* flist = nullptr;
+  const int32_t* face = nullptr;
+  const double* h = nullptr;
+  const double* sink = nullptr;
+  const int64_t* fnode = nullptr;
+  const int32_t* fnptr = nullptr;
+  const int32_t* fnlist = nullptr;
+  double* load = nullptr;
+};
+cudaError_t launch_films(int elem_type, const ElemArgs& a, const FilmArgs& f, double* edata, double* f_ext3,
+                         cudaStream_t s);
 cudaError_t launch_adjoint(int elem_type, const ElemArgs& a, double* dc_dE, double* dc_dX,
                            cudaStream_t s);
 cudaError_t launch_spmv(int32_t nrows, const int64_t* rp, const int32_t* ci, const double* v, const double* x,

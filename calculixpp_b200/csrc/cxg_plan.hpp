@@ -109,6 +109,9 @@ struct cxg_plan {
   double* th_alpha = nullptr;
   double* th_tref = nullptr;
   double* th_load = nullptr;  // [3N] scratch: thermal-strain load (+ f_ext) of the linear assembly
+  // *FILM faces of a temperature plan (cxg_thermal_plan_set_films); one device block
+  cxg::FilmArgs films;
+  void* film_mem = nullptr;
 };
 
 

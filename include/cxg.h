@@ -250,7 +250,7 @@ CXG_API int cxg_assemble_mass(cxg_plan* plan, const double* density, int32_t lum
  * order then the Gauss rule's order; NULL means a zero field. */
 CXG_API int cxg_assemble_geometric(cxg_plan* plan, const double* gp_stress, double* vals, void* stream);
 
-/* ---- heat conduction (assemble_conduction, src/fem/thermal.cpp:92-141, without films)
+/* ---- heat conduction (assemble_conduction, src/fem/thermal.cpp:92-141)
  * A temperature plan carries one DOF per node: t_dof_eq[n_nodes] (free equation or -1,
  * free nodes numbered in node order, build_thermal_dof_map, thermal.cpp:71-90) and
  * t_prescribed[n_nodes]; its pattern is the scalar conduction pattern. The mesh's
@@ -261,6 +261,14 @@ CXG_API int cxg_thermal_plan_create(const cxg_mesh_desc* mesh, const int32_t* t_
                                     int32_t n_free, cxg_plan** out);
 CXG_API int cxg_assemble_conduction(cxg_plan* plan, const double* conductivity, const double* flux, double* vals,
                                     double* rhs, void* stream);
+/* *FILM faces of a temperature plan (Model::films; assemble_conduction, thermal.cpp:
+ * 113-126): film f is face face[f] (1-based: tet 1..4, hex 1..6, wedge 1..5, the
+ * reference's face numbering, src/fem/loads.cpp:13-46) of element elem[f] (0-based),
+ * coefficient h[f], sink temperature sink[f]; host or device arrays, copied. From then on
+ * cxg_assemble_conduction adds h int N_a N_b dA to the matrix and h T_sink int N_a dA to
+ * the free rows of the rhs (3-point triangle / 2x2 quad face rules). n_films = 0 clears. */
+CXG_API int cxg_thermal_plan_set_films(cxg_plan* plan, int64_t n_films, const int64_t* elem, const int32_t* face,
+                                       const double* h, const double* sink);
 
 /* ---- thermal strain (*EXPANSION with an applied temperature field) ---------------------
  * Inputs of the reference's thermal-strain path (Material::expansion,

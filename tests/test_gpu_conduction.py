@@ -68,3 +68,35 @@ def test_steady_linear_profile_and_plan_kind(cuda):
     rc = mech.lib.cxg_assemble_conduction(mech.h, C.c_void_p(k.data_ptr()), None, C.c_void_p(v.data_ptr()), None,
                                           None)
     assert rc == 1 and b"cxg_thermal_plan_create" in mech.lib.cxg_last_error()
+
+
+@pytest.mark.parametrize("etype", ALL_TYPES)
+def test_conduction_films_match_oracle(cuda, port, etype):
+    """*FILM faces (thermal.cpp:113-126) against the oracle's restatement (pinned bit-exact
+    to the reference): films on random faces, two on some elements, with prescribed
+    temperatures on one face; matrix and rhs within 1e-12; clearing the films restores
+    the film-free system."""
+    from tests.test_oracle_thermal import film_case
+    model, m, films, tn, tv = film_case(etype, 90 + etype)
+    k = np.random.default_rng(etype).uniform(10.0, 60.0, m.n_elems)
+    q = np.random.default_rng(etype + 1).uniform(-1.0, 1.0, m.n_nodes)
+    plan = ThermalPlan(m, tn, tv)
+    v0, r0 = (to_np(t).copy() for t in plan.assemble_conduction(k, q))
+    plan.set_films(*films)
+    vals, rhs = (to_np(t).copy() for t in plan.assemble_conduction(k, q))
+    deq, pre, nf = mg.thermal_dof_map(m.n_nodes, tn, tv)
+    rp, ci, v, r = port.assemble_conduction_films(m, k, deq, pre, nf, films, q)
+    rpg, cig = (to_np(t) for t in plan.pattern())
+    kg = np.repeat(np.arange(nf), np.diff(rpg)).astype(np.int64) * nf + cig
+    ko = np.repeat(np.arange(nf), np.diff(rp)).astype(np.int64) * nf + ci
+    keep = np.isin(kg, ko)
+    assert keep.sum() == ko.size
+    assert rel_fro(vals[keep], v) <= 1e-12
+    assert np.abs(vals[~keep]).max(initial=0.0) <= 1e-12 * np.abs(v).max()
+    assert rel_fro(rhs, r) <= 1e-12
+    plan.set_films()
+    v1, r1 = (to_np(t) for t in plan.assemble_conduction(k, q))
+    assert np.array_equal(v1, v0) and np.array_equal(r1, r0)
+    with pytest.raises(Exception):
+        plan.set_films([0], [99], [1.0], [0.0])  # face out of range
+    plan.close()
