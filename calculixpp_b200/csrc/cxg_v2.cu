@@ -8,7 +8,8 @@
 // Gauss points from float4/double4 gradient loads; elastic points use the Gram form
 // K_ab = lam G + mu (G^T + tr(G) I) with G = sum_q s_q g_a g_b^T, plastic elements the
 // full tangent sum_q s [lam* g_a g_b^T + mu* (g_b g_a^T + (g_a.g_b) I) - c m_a m_b^T]
-// (m = N g, N the return direction). The upper blocks (a <= b) go to a per-element
+// (m = N g, N the return direction, formed in the tile loop from the gradients and the
+// stored N of the Gauss point). The upper blocks (a <= b) go to a per-element
 // buffer, FP32 in mixed precision, FP64 otherwise; the internal force goes beside them.
 //
 // P2 (row gather): one warp per node. It walks the node's incident elements in
@@ -388,7 +389,7 @@ struct P1Smem {
   static constexpr int kVec = EPW * nq * VecIdx<R, npad>::kBlock;
   static constexpr int HG = ET == C3D8R ? EPW : 1;  // hourglass data (C3D8R only)
   R g[kVec];                                      // node vectors, see VecIdx
-  R m[T ? kVec : 4];
+  R nvq[T ? EPW * nq * 8 : 4];  // return direction N (Voigt, 6 used) per plastic Gauss point
   R s[EPW][nq];
   R dp[T ? EPW : 1][T ? nq : 1][4];
   double x[EPW][3 * n];
@@ -413,12 +414,16 @@ constexpr size_t p1_smem_bytes() {
 // Resident blocks per SM the element pass asks the register allocator for: as many as
 // its shared memory allows, at most 3 (<= 170 registers per thread) for the tiles whose
 // accumulators fit that budget without spilling (2x2, and 2x4 in FP32), else 2 (no
-// limit below the 255-register ceiling).
+// limit below the 255-register ceiling). The mixed-precision material-point pass with
+// 2x2 tiles takes 4 (<= 128 registers): it spills 28 bytes per thread there and still
+// ran 10 % faster on the C3D8 J2 block, where the FP64 one lost 8 % to its spills.
 template <int ET, int MODE, typename R, int TILE>
 constexpr int p1_min_blocks() {
   constexpr size_t per_sm = 227 * 1024;
   constexpr int by_smem = static_cast<int>(per_sm / (p1_smem_bytes<ET, MODE, R, TILE>() + 1024));
-  constexpr int cap = (TILE == 1 || (TILE == 0 && sizeof(R) == 4)) ? 3 : 2;
+  constexpr int cap = (TILE == 1 && MODE == MODE_TANGENT && sizeof(R) == 4)   ? 4
+                      : (TILE == 1 || (TILE == 0 && sizeof(R) == 4)) ? 3
+                                                                     : 2;
   return by_smem < 1 ? 1 : (by_smem > cap ? cap : by_smem);
 }
 
@@ -450,7 +455,6 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
   // zero the padded gradient slots once; they are never written afterwards
   for (int t = lane; t < WS::kVec; t += 32) {
     W.g[t] = R(0);
-    if (TAN) W.m[t % (sizeof(W.m) / sizeof(R))] = R(0);
   }
   __syncthreads();
 
@@ -563,14 +567,8 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
         W.dp[ei][q][2] = static_cast<R>(sq * ct);
         if (pl) {
           W.plastic[ei] = 1;
-          for (int k = 0; k < n; ++k) {
-            const int b = ei * nq + q, sl = node_slot(k, npad);
-            R rx, ry, rz;
-            ld3<R, npad>(W.g, b, sl, rx, ry, rz);
-            const double gx = rx, gy = ry, gz = rz;
-            st3<R, npad>(W.m, b, sl, nv[0] * gx + nv[3] * gy + nv[4] * gz, nv[3] * gx + nv[1] * gy + nv[5] * gz,
-                         nv[4] * gx + nv[5] * gy + nv[2] * gz);
-          }
+#pragma unroll
+          for (int c = 0; c < 6; ++c) W.nvq[(ei * nq + q) * 8 + c] = static_cast<R>(nv[c]);
         }
         if constexpr (ET == C3D8R) {
           if (q == nq - 1) W.mu_hg[ei] = mhg;
@@ -682,13 +680,22 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
                     acc[i][j][3 * x + y] += (sl * ga[i][x]) * gb[j][y] + (sm * gb[j][x]) * ga[i][y] + (x == y ? dot : R(0));
               }
             if (sc != R(0)) {
+              // m = N g for the tile's nodes, from the stored return direction
+              const R* N = W.nvq + (ei * nq + q) * 8;
+              const R n0 = N[0], n1 = N[1], n2 = N[2], n3 = N[3], n4 = N[4], n5 = N[5];
               R ma[TR][3], mb[TC][3];
 #pragma unroll
-              for (int i = 0; i < TR; ++i)
-                ld3<R, npad>(W.m, ei * nq + q, node_slot(a0 + i, npad), ma[i][0], ma[i][1], ma[i][2]);
+              for (int i = 0; i < TR; ++i) {
+                ma[i][0] = n0 * ga[i][0] + n3 * ga[i][1] + n4 * ga[i][2];
+                ma[i][1] = n3 * ga[i][0] + n1 * ga[i][1] + n5 * ga[i][2];
+                ma[i][2] = n4 * ga[i][0] + n5 * ga[i][1] + n2 * ga[i][2];
+              }
 #pragma unroll
-              for (int j = 0; j < TC; ++j)
-                ld3<R, npad>(W.m, ei * nq + q, node_slot(b0 + j, npad), mb[j][0], mb[j][1], mb[j][2]);
+              for (int j = 0; j < TC; ++j) {
+                mb[j][0] = n0 * gb[j][0] + n3 * gb[j][1] + n4 * gb[j][2];
+                mb[j][1] = n3 * gb[j][0] + n1 * gb[j][1] + n5 * gb[j][2];
+                mb[j][2] = n4 * gb[j][0] + n5 * gb[j][1] + n2 * gb[j][2];
+              }
 #pragma unroll
               for (int i = 0; i < TR; ++i)
 #pragma unroll
