@@ -461,19 +461,34 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
   const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * kW1 + warp;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kW1;
   const int64_t e_end = V.e_end;  // elements [V.e_begin, V.e_end) of this window
+  // The connectivity of a warp's next elements is loaded while it integrates the current
+  // ones, so the coordinate gather of the next iteration waits for one round of loads.
+  constexpr int PA = (EPW * n + 31) / 32;
+  int conn_next[PA];
+  auto load_conn = [&](int64_t e0x) {
+#pragma unroll
+    for (int p = 0; p < PA; ++p) {
+      const int t = lane + 32 * p;
+      const int64_t e = e0x + t / n;
+      conn_next[p] = t < EPW * n && e < e_end ? A.conn[e * n + t % n] : -1;
+    }
+  };
+  load_conn(V.e_begin + gwarp * EPW);
   for (int64_t e0 = V.e_begin + gwarp * EPW; e0 < e_end; e0 += nwarps * EPW) {
     // ---- phase A ---------------------------------------------------------------
-    for (int t = lane; t < EPW * n; t += 32) {
-      const int ei = t / n, k = t % n;
-      const int64_t e = e0 + ei;
-      if (e < e_end) {
-        const int node = A.conn[e * n + k];
+#pragma unroll
+    for (int p = 0; p < PA; ++p) {
+      const int t = lane + 32 * p;
+      const int node = conn_next[p];
+      if (node >= 0) {
+        const int ei = t / n, k = t % n;
         for (int d = 0; d < 3; ++d) {
           W.x[ei][3 * k + d] = A.coords[3 * static_cast<int64_t>(node) + d];
           if (TAN) W.u[ei][3 * k + d] = A.u[3 * static_cast<int64_t>(node) + d];
         }
       }
     }
+    load_conn(e0 + nwarps * EPW);
     if (lane < EPW) {
       const int64_t e = e0 + lane;
       const double E = e < e_end ? A.young[e] : 1.0, nu = e < e_end ? A.poisson[e] : 0.0;
