@@ -958,28 +958,16 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
     };
     if (DIAGFIX) {
       // diagonal block of node a: minus the FP64 sum of every off-diagonal block in its
-      // rows; lane l sums the blocks of neighbours l, l + 32, ..., then a butterfly
-      // (the same bits on every lane)
+      // rows. Lane 9 p + q (p < 3) sums entry q of the blocks of neighbours p, p + 3,
+      // ... in neighbour order; lane q then adds the three phases in phase order.
       slot_aa = static_cast<int>(__reduce_max_sync(kAll, static_cast<unsigned>(slot_aa)));
-      double d[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-      for (int s = lane; s < K; s += 32) {
-        if (s == slot_aa) continue;
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int j = 0; j < 3; ++j) d[3 * i + j] += staged(i * W + 3 * s + j);
-      }
-#pragma unroll
-      for (int q = 0; q < 9; ++q)
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) d[q] += __shfl_xor_sync(kAll, d[q], off);
-      if (lane < 9 && i1 > i0) {
-        double dq = d[0];
-#pragma unroll
-        for (int q = 1; q < 9; ++q)
-          if (q == lane) dq = d[q];
-        buf[(lane / 3) * W + 3 * slot_aa + lane % 3] = -dq;
-      }
+      const int q = lane % 9, p = lane / 9, qi = q / 3, qj = q - 3 * qi;
+      double d = 0.0;
+      if (p < 3)
+        for (int s = p; s < K; s += 3)
+          if (s != slot_aa) d += staged(qi * W + 3 * s + qj);
+      const double d1 = __shfl_sync(kAll, d, (lane + 9) & 31), d2 = __shfl_sync(kAll, d, (lane + 18) & 31);
+      if (lane < 9 && i1 > i0) buf[qi * W + 3 * slot_aa + qj] = -((d + d1) + d2);
       __syncwarp();
     }
     // Interior nodes (every neighbour fully free, L == W) store the staged rows as they
