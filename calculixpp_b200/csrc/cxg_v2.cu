@@ -846,6 +846,10 @@ struct P2Geo {
   static constexpr int n = nodes_of(ET);
   static constexpr int GS = n <= 16 ? 16 : 32;
   static constexpr int EG = 32 / GS;
+  // lanes n .. n + 2 of a group are idle in the block loop and gather the three
+  // components of the element forces (all families but C3D15, whose 16-lane groups
+  // leave one lane, and whose diagonal-block lane takes them)
+  static constexpr bool FIDLE = n + 3 <= GS;
 };
 
 template <typename R>
@@ -921,10 +925,16 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
     const int total = 3 * W;
     const int64_t i0 = cur_node.i0, i1 = cur_node.i1;
     const int L = cur_node.L;
+    // every copy starts 16-byte aligned (stride is even) and holds at least total + 1
+    // doubles when total is odd
     for (int g = 0; g < EG; ++g)
-      for (int t = lane; t < total; t += 32) buf[g * stride + t] = 0.0;
+      for (int t = lane; 2 * t < total; t += 32)
+        reinterpret_cast<double2*>(buf + g * stride)[t] = make_double2(0.0, 0.0);
     __syncwarp();
-    double fs[3] = {0.0, 0.0, 0.0};
+    constexpr bool FIDLE = P2Geo<ET, DIAGFIX>::FIDLE;
+    // a's internal force: component lb - n on lanes lb = n .. n + 2 (FIDLE), else all
+    // three on the lane of each element's diagonal block
+    double fs[FIDLE ? 1 : 3] = {};
     int slot_aa = 0;  // position of node a in its own adjacency list (DIAGFIX)
     for (int64_t c0 = i0; c0 < i1; c0 += 32) {
       const int cnt = static_cast<int>(i1 - c0 < 32 ? i1 - c0 : 32);
@@ -941,9 +951,14 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
             c[i * W + 2] += cur.v[3 * i + 2];
           }
         }
-        if (TAN && cur.active && lb == cur.la) {
+        if constexpr (TAN && FIDLE) {
+          if (lb >= n && lb < n + 3 && k + sub < cnt)
+            fs[0] += __ldg(V.fdata + (WIN ? ring_slot(cur.e, V) : cur.e) * (3 * n) + 3 * cur.la + (lb - n));
+        } else if constexpr (TAN) {
+          if (cur.active && lb == cur.la)
 #pragma unroll
-          for (int d = 0; d < 3; ++d) fs[d] += __ldg(V.fdata + (WIN ? ring_slot(cur.e, V) : cur.e) * (3 * n) + 3 * cur.la + d);
+            for (int d = 0; d < 3; ++d)
+              fs[d] += __ldg(V.fdata + (WIN ? ring_slot(cur.e, V) : cur.e) * (3 * n) + 3 * cur.la + d);
         }
         if (DIAGFIX && cur.active && lb == cur.la) slot_aa = cur.slotv;
         __syncwarp();
@@ -1033,7 +1048,9 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         double v = rr[r];
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kAll, v, off);
+        // interior nodes have no prescribed columns: every lane's term is +0.0
+        if (L != W)
+          for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kAll, v, off);
         if (lane == 0 && ((ma >> r) & 1)) {
           const int64_t eq = A.node_eq0[a] + __popc(ma & ((1 << r) - 1));
           const double prev = V.accumulate ? A.rhs[eq] : (V.f_ext ? V.f_ext[3 * a + r] : 0.0);
@@ -1042,11 +1059,22 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
       }
     }
     if (TAN && A.f_int) {
+      if constexpr (FIDLE) {
+        // group partials (each in incidence order) added in group order
+        double v = fs[0];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double v = fs[d];
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kAll, v, off);
-        if (lane == 0) A.f_int[3 * a + d] = (V.accumulate ? A.f_int[3 * a + d] : 0.0) + v;
+        for (int g = 1; g < EG; ++g) v += __shfl_sync(kAll, fs[0], (lane + g * GS) & 31);
+        if (lane >= n && lane < n + 3) {
+          const int d = lane - n;
+          A.f_int[3 * a + d] = (V.accumulate ? A.f_int[3 * a + d] : 0.0) + v;
+        }
+      } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double v = fs[d];
+          for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kAll, v, off);
+          if (lane == 0) A.f_int[3 * a + d] = (V.accumulate ? A.f_int[3 * a + d] : 0.0) + v;
+        }
       }
     }
     __syncwarp();
