@@ -342,7 +342,24 @@ def batched(args, world, rank, dev, stream):
            "models": len(models), "elements": E_tot, "elements_by_type": by_type, "nnz": b.nnz,
            "n_free": b.n_free, "plan_build_s": t_build}
     plain = plain_fp64_per_model(models, args, dev, stream) if world == 1 else None
+
+    def signature():
+        # sum and a strided sample of the batch's values: equal outputs give equal
+        # signatures (the full vals buffer is too large to keep a copy of)
+        return float(vals.sum().item()), vals[::9973].clone(), rhs.clone()
+
+    def one_launch(prec, ref):
+        # the same step with the whole batch as one element pass + one row gather
+        b.set_launch("one_launch")
+        r = run(prec)
+        sig = signature()
+        r["equal_to_per_group"] = bool(sig[0] == ref[0] and torch.equal(sig[1], ref[1]) and torch.equal(sig[2], ref[2]))
+        r["how"] = "one element pass + one row gather for all groups (cxg_batch_set_launch ONE_LAUNCH), one CUDA graph"
+        b.set_launch("per_group")
+        return r
+
     res["mixed"] = run("mixed")
+    res["mixed_one_launch"] = one_launch("mixed", signature())
     keep = vals.clone() if b.nnz * 8 < 0.2 * torch.cuda.mem_get_info()[0] else None
     free = torch.cuda.mem_get_info()[0]
     # FP64 element buffers replace the FP32 ones group by group (each FP32 buffer is
@@ -357,6 +374,7 @@ def batched(args, world, rank, dev, stream):
         fits = bool(flag.item() > 0.5)
     if fits:
         res["fp64"] = run("fp64")
+        res["fp64_one_launch"] = one_launch("fp64", signature())
         res["speedup_mixed_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
         if keep is not None:
             res["mixed_K_rel_fro_vs_fp64"] = float(torch.linalg.norm(keep - vals) / torch.linalg.norm(vals))
@@ -516,7 +534,7 @@ def cpu_baseline(seconds, seed=0, as_shipped=True):
         ref = Ref()
         elems, t0 = 0, time.perf_counter()
         while True:
-            ref.assemble_csr_threads(m, dof_eq, pre, rp, ci, threads)
+            kv, kr = ref.assemble_csr_threads(m, dof_eq, pre, rp, ci, threads)
             elems += m.n_elems
             if time.perf_counter() - t0 >= seconds:
                 break
@@ -526,6 +544,10 @@ def cpu_baseline(seconds, seed=0, as_shipped=True):
                          f"element_stiffness (src/fem/element.cpp) on {threads} threads + exact CSR scatter"}
         if not as_shipped:
             return out
+        # the reference's FP64 system of the sampled block, the checker of the GPU's
+        # mixed and FP64 outputs on the same block (popped before the line is printed)
+        out["_ref_system"] = {"n": n, "seed": seed, "row_ptr": rp, "col_idx": ci, "vals": kv, "rhs": kr,
+                              "dof_eq": dof_eq}
         # beside it, the reference's own assembly driver as shipped: one thread, its hash-map
         # scatter and unordered COO flush (assemble_linear_static, src/fem/assembly.cpp:225-257)
         try:
@@ -556,6 +578,40 @@ def cpu_baseline(seconds, seed=0, as_shipped=True):
     dt = time.perf_counter() - t0
     return {"value": elems / dt, "unit": "element-integrations/s", "cores": 1, "kind": "port",
             "sample": f"C3D20 {n}^3 block x {elems // m.n_elems} passes through the oracle's C restatement"}
+
+
+def accuracy_vs_reference(sysref):
+    """Errors of the GPU's FP64 and mixed outputs against the reference's own FP64
+    system of the same block (its element_stiffness + exact CSR scatter): K relative
+    Frobenius, and displacements relative L2 after the same host sparse direct solve."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    import torch
+
+    from calculixpp_b200 import Plan
+    model, f = c3d20_model(sysref["n"], seed=sysref["seed"])
+    nf = sysref["row_ptr"].size - 1
+    k_ref = sp.csr_matrix((sysref["vals"], sysref["col_idx"], sysref["row_ptr"]), shape=(nf, nf))
+    deq = sysref["dof_eq"]
+    f_red = np.zeros(nf)
+    free = deq >= 0
+    np.add.at(f_red, deq[free], np.asarray(f, dtype=np.float64)[free])
+    u_ref = spla.spsolve(k_ref.tocsc(), f_red + sysref["rhs"])
+    plan = Plan(model)
+    rp, ci = (t.cpu().numpy() for t in plan.pattern())
+    out = {"block": f"{sysref['n']}^3", "checker": "reference element_stiffness + exact CSR scatter (FP64)",
+           "bar_mixed_disp": 1e-6, "bar_fp64_K": 1e-12, "bar_fp64_disp": 1e-10}
+    for prec in ("fp64", "mixed"):
+        plan.set_precision(prec)
+        v, r = plan.assemble_linear(torch.as_tensor(f, device=plan.device))
+        k = sp.csr_matrix((v.cpu().numpy(), ci, rp), shape=(plan.n_free, plan.n_free))
+        u = spla.spsolve(k.tocsc(), r.cpu().numpy())
+        out[prec] = {"K_rel_fro": float(spla.norm(k - k_ref) / spla.norm(k_ref)),
+                     "disp_rel_l2": float(np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref))}
+    plan.close()
+    out["pass"] = bool(out["mixed"]["disp_rel_l2"] <= 1e-6 and out["fp64"]["K_rel_fro"] <= 1e-12 and
+                       out["fp64"]["disp_rel_l2"] <= 1e-10)
+    return out
 
 
 def reference_arm(args, rank, world):
@@ -676,6 +732,8 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_seconds)
+        if acc is not None and "_ref_system" in cpu:
+            acc["vs_reference"] = accuracy_vs_reference(cpu.pop("_ref_system"))
 
     if rank != 0:
         return

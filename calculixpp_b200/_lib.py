@@ -126,6 +126,8 @@ SIGNATURES = {
     "cxg_batch_get_model_info": (C.c_int, [_vp, C.c_int32, C.POINTER(CxgBatchModelInfo)]),
     "cxg_batch_get_pattern": (C.c_int, [_vp, C.c_int32, _vp, _vp]),
     "cxg_batch_set_precision": (C.c_int, [_vp, C.c_int32]),
+    "cxg_batch_set_launch": (C.c_int, [_vp, C.c_int32]),
+    "cxg_batch_get_launch": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "cxg_batch_assemble": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "cxg_batch_graph_launch": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "cxg_batch_check": (C.c_int, [_vp]),

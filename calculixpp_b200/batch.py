@@ -103,6 +103,19 @@ class Batch:
     def set_precision(self, precision: str):
         _lib.check(self.lib.cxg_batch_set_precision(self.h, _lib.MIXED if precision == "mixed" else _lib.FP64))
 
+    LAUNCH_MODES = {"per_group": 0, "one_launch": 1}
+
+    def set_launch(self, mode: str):
+        """"per_group" (default): one element pass and one row gather per element-type
+        group; "one_launch": one element pass and one row gather for the whole batch
+        (cxg_batch_set_launch)."""
+        _lib.check(self.lib.cxg_batch_set_launch(self.h, self.LAUNCH_MODES[mode]))
+
+    def launch_mode(self) -> str:
+        m = C.c_int32()
+        _lib.check(self.lib.cxg_batch_get_launch(self.h, C.byref(m)))
+        return {v: k for k, v in self.LAUNCH_MODES.items()}[m.value]
+
     def group_config(self, g):
         t, tile, p1, w = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
         _lib.check(self.lib.cxg_batch_group_config(self.h, g, C.byref(t), C.byref(tile), C.byref(p1), C.byref(w)))

@@ -5,9 +5,12 @@
 // its models: node, element and equation numbers of model k are shifted by the totals
 // of models 0..k-1, so the group's CSR is block diagonal, every model's rows are a
 // contiguous range of it, and the row gather sums each model's entries in the same
-// element order as a plan of that model alone (identical results). One assembly of
-// the batch is one element pass plus one row gather per group; the graph form captures
-// the groups as independent branches so small groups run side by side.
+// element order as a plan of that model alone (identical results). By default one
+// assembly of the batch is one element pass plus one row gather per group, and the
+// graph form captures the groups as independent branches so small groups run side by
+// side. In the one-launch mode (cxg_batch_set_launch) the whole batch is one element
+// pass and one row gather: every group is a slot of the same two kernels, with a share
+// of the persistent grid in proportion to its measured (or estimated) pass time.
 //
 // The autotuner times candidate launch shapes of each pass with CUDA events on the
 // batch's own data and keeps the fastest; a JSON file caches the choices.
@@ -31,6 +34,10 @@ namespace {
 struct Group {
   int32_t type = 0;
   cxg_plan* plan = nullptr;
+  // one-launch mode, per precision: element-pass tile and the slot's pass times in ms
+  // from the tuner (0: estimated from the element count and family)
+  int ftile[2] = {1, 1};
+  double fms1[2] = {0.0, 0.0}, fms2[2] = {0.0, 0.0};
   int64_t node0 = 0, vals0 = 0, rhs0 = 0;  // offsets in the batch's node / vals / rhs order
   cudaStream_t side = nullptr;               // branch stream of the graph
   cudaEvent_t join = nullptr;
@@ -83,6 +90,8 @@ struct cxg_batch {
   const void* key[3] = {nullptr, nullptr, nullptr};
   int32_t key_precision = -1;
   uint64_t key_cfg = 0;
+  int32_t launch = CXG_BATCH_PER_GROUP;
+  int fwarps[2] = {0, 0};  // one-launch row gather: warps per block (0: as many as fit, <= 8)
 };
 
 namespace {
@@ -93,7 +102,12 @@ uint64_t cfg_hash(const cxg_batch* b) {
     for (int pr = 0; pr < 2; ++pr) {
       const LaunchCfg& c = g.plan->cfg[pr];
       for (int v : {c.tile, c.p1_blocks_per_sm, c.p2_warps, c.p2_blocks_per_sm}) h = (h ^ static_cast<uint64_t>(v + 7)) * 1099511628211ull;
+      uint64_t w1 = 0, w2 = 0;
+      std::memcpy(&w1, &g.fms1[pr], 8);
+      std::memcpy(&w2, &g.fms2[pr], 8);
+      for (uint64_t v : {static_cast<uint64_t>(g.ftile[pr]), w1, w2}) h = (h ^ v) * 1099511628211ull;
     }
+  for (int v : {b->launch, b->fwarps[0], b->fwarps[1]}) h = (h ^ static_cast<uint64_t>(v + 7)) * 1099511628211ull;
   return h;
 }
 
@@ -121,6 +135,62 @@ cudaError_t launch_group(cxg_batch* b, Group& g, double* vals, double* rhs, cons
   V2Args v = v2_args(p, f_ext ? f_ext + 3 * g.node0 : nullptr, false);
   apply_windows(p, false, v);
   return launch_v2(p->type, MODE_LINEAR, b->precision, a, v, s, override_cfg ? *override_cfg : p->cfg[b->precision]);
+}
+
+// Pass-time estimates of a group when the tuner has not measured it: element pass ~
+// node pairs x (Gauss points + block stores), row gather ~ stored blocks.
+double p1_estimate(int t, int64_t ne) {
+  const double n = nodes_of(t), nq = gauss_of(t);
+  return static_cast<double>(ne) * n * n * (nq + 4.0);
+}
+double p2_estimate(int t, int64_t ne) {
+  const double n = nodes_of(t);
+  return static_cast<double>(ne) * n * (n + 1.0) / 2.0;
+}
+
+// Every group as one slot of the one-launch kernels. Linear mode when u is null, else
+// the material-point (tangent) assembly. Weights are the tuned times when every group
+// has one, else the estimates.
+int fill_slots(cxg_batch* b, const double* u, double* vals, double* f_int, double* rhs, const double* f_ext,
+               cudaStream_t s, std::vector<BatchSlotIn>& slots) {
+  const int pr = b->precision ? 1 : 0;
+  const bool tan = u != nullptr;
+  if (b->groups.size() > static_cast<size_t>(kMaxBatchSlots))
+    return set_err(CXG_ERR_UNSUPPORTED, "one-launch batch holds at most 8 element-type groups");
+  bool tuned = true;
+  for (const Group& g : b->groups) tuned = tuned && g.fms1[pr] > 0.0 && g.fms2[pr] > 0.0;
+  slots.clear();
+  for (Group& g : b->groups) {
+    cxg_plan* p = g.plan;
+    p->last_stream = s;
+    BatchSlotIn in;
+    in.a = base_args(p);
+    in.a.vals = vals + g.vals0;
+    in.a.rhs = rhs ? rhs + g.rhs0 : nullptr;
+    if (tan) {
+      in.a.f_int = f_int ? f_int + 3 * g.node0 : nullptr;
+      in.a.u = u + 3 * g.node0;
+      in.a.state_c = p->state[0];
+      in.a.state_t = p->state[1];
+      in.a.state_comps = state_comps(p);
+    }
+    in.v = v2_args(p, f_ext ? f_ext + 3 * g.node0 : nullptr, false);
+    apply_windows(p, tan, in.v);
+    if (in.v.n_win > 1 || in.v.node_order)
+      return set_err(CXG_ERR_UNSUPPORTED, "one-launch batch assembles every group as one window (no element-buffer budget)");
+    in.type = g.type;
+    in.cfg = tan ? p->tcfg[pr] : p->cfg[pr];
+    in.cfg.tile = tan ? 1 : g.ftile[pr];
+    in.cfg.p2_warps = b->fwarps[pr];
+    in.p1_weight = tuned ? g.fms1[pr] : p1_estimate(g.type, p->n_elems);
+    in.p2_weight = tuned ? g.fms2[pr] : p2_estimate(g.type, p->n_elems);
+    slots.push_back(in);
+  }
+  return CXG_OK;
+}
+
+cudaError_t launch_one(cxg_batch* b, const std::vector<BatchSlotIn>& slots, int mode, int passes, cudaStream_t s) {
+  return launch_v2_batch(mode, b->precision, slots.data(), static_cast<int>(slots.size()), passes, s);
 }
 
 int prepare(cxg_batch* b) {
@@ -216,6 +286,120 @@ int time_pass(cxg_batch* b, Group& g, double* vals, double* rhs, const double* f
   }
   std::sort(t.begin(), t.end());
   *ms_out = t[t.size() / 2];
+  return CXG_OK;
+}
+
+// Median of `reps` timed one-launch passes over `slots` (after one untimed launch);
+// -1 when the shape cannot launch here.
+int time_one(cxg_batch* b, const std::vector<BatchSlotIn>& slots, int passes, cudaStream_t s, cudaEvent_t e0,
+             cudaEvent_t e1, double* ms_out) {
+  const int reps = 3;
+  std::vector<float> t;
+  for (int r = 0; r <= reps; ++r) {
+    CHECK_CUDA(cudaEventRecord(e0, s), "tune event");
+    if (launch_one(b, slots, MODE_LINEAR, passes, s) != cudaSuccess) {
+      cudaGetLastError();
+      *ms_out = -1.0;
+      return cudaStreamSynchronize(s) == cudaSuccess ? CXG_OK : cuda_err(cudaErrorLaunchFailure, "tune");
+    }
+    CHECK_CUDA(cudaEventRecord(e1, s), "tune event");
+    CHECK_CUDA(cudaEventSynchronize(e1), "tune sync");
+    float ms = 0.f;
+    CHECK_CUDA(cudaEventElapsedTime(&ms, e0, e1), "tune time");
+    if (r > 0) t.push_back(ms);
+  }
+  std::sort(t.begin(), t.end());
+  *ms_out = t[t.size() / 2];
+  return CXG_OK;
+}
+
+// One-launch tuner: per group, the element-pass tile (2x2, and 2x4 in mixed precision)
+// timed as a slot alone, whose time becomes its share weight; then the row gather's
+// warps per block over the whole batch, and each group's gather time alone at that
+// shape. Cache keys carry "/one-launch".
+int tune_one_launch(cxg_batch* b, double* vals, double* rhs, const double* f_ext,
+                    std::map<std::string, CacheEntry>& cache, bool* changed, cudaStream_t s) {
+  const int pr = b->precision ? 1 : 0;
+  std::vector<BatchSlotIn> all;
+  int rc = fill_slots(b, nullptr, vals, nullptr, rhs, f_ext, s, all);
+  if (rc) return rc;
+  bool cached = true;
+  for (Group& g : b->groups) {
+    auto it = cache.find(cache_key(b, g) + "/one-launch");
+    if (it == cache.end()) {
+      cached = false;
+      break;
+    }
+  }
+  if (cached) {
+    for (Group& g : b->groups) {
+      const CacheEntry& c = cache[cache_key(b, g) + "/one-launch"];
+      g.ftile[pr] = c.tile;
+      g.fms1[pr] = c.p1_ms;
+      g.fms2[pr] = c.p2_ms;
+      b->fwarps[pr] = c.warps;
+    }
+  } else {
+    cudaEvent_t e0, e1;
+    CHECK_CUDA(cudaEventCreate(&e0), "event");
+    CHECK_CUDA(cudaEventCreate(&e1), "event");
+    for (size_t gi = 0; gi < b->groups.size() && !rc; ++gi) {
+      Group& g = b->groups[gi];
+      double best = 1e30;
+      int best_tile = 1;
+      for (int tile : {1, 0}) {
+        if (!batch_tile_ok(MODE_LINEAR, b->precision, tile)) continue;
+        std::vector<BatchSlotIn> one(1, all[gi]);
+        one[0].cfg.tile = tile;
+        double ms = 0.0;
+        if ((rc = time_one(b, one, 1, s, e0, e1, &ms))) break;
+        if (ms >= 0.0 && ms < best) {
+          best = ms;
+          best_tile = tile;
+        }
+      }
+      g.ftile[pr] = best_tile;
+      all[gi].cfg.tile = best_tile;
+      g.fms1[pr] = best < 1e30 ? best : 0.0;
+    }
+    double best = 1e30;
+    int best_warps = 0;
+    for (int warps : {8, 4, 2}) {
+      if (rc) break;
+      std::vector<BatchSlotIn> sl = all;
+      for (BatchSlotIn& in : sl) in.cfg.p2_warps = warps;
+      double ms = 0.0;
+      if ((rc = time_one(b, sl, 2, s, e0, e1, &ms))) break;
+      if (ms >= 0.0 && ms < best) {
+        best = ms;
+        best_warps = warps;
+      }
+    }
+    b->fwarps[pr] = best_warps;
+    for (size_t gi = 0; gi < b->groups.size() && !rc; ++gi) {
+      std::vector<BatchSlotIn> one(1, all[gi]);
+      one[0].cfg.p2_warps = best_warps;
+      double ms = 0.0;
+      if ((rc = time_one(b, one, 2, s, e0, e1, &ms))) break;
+      b->groups[gi].fms2[pr] = ms > 0.0 ? ms : 0.0;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    for (Group& g : b->groups) {
+      CacheEntry c;
+      c.tile = g.ftile[pr];
+      c.warps = b->fwarps[pr];
+      c.p1_ms = g.fms1[pr];
+      c.p2_ms = g.fms2[pr];
+      cache[cache_key(b, g) + "/one-launch"] = c;
+    }
+    *changed = true;
+  }
+  // leave a complete assembly with the chosen shapes in vals / rhs
+  if ((rc = fill_slots(b, nullptr, vals, nullptr, rhs, f_ext, s, all))) return rc;
+  CHECK_CUDA(launch_one(b, all, MODE_LINEAR, 3, s), "batch assembly (one launch)");
+  CHECK_CUDA(cudaStreamSynchronize(s), "tuning");
   return CXG_OK;
 }
 
@@ -473,6 +657,21 @@ int cxg_batch_set_precision(cxg_batch* b, int32_t precision) {
   return CXG_OK;
 }
 
+int cxg_batch_set_launch(cxg_batch* b, int32_t mode) {
+  if (!b || (mode != CXG_BATCH_PER_GROUP && mode != CXG_BATCH_ONE_LAUNCH))
+    return set_err(CXG_ERR_INVALID_ARGUMENT, "bad batch launch mode");
+  if (mode == CXG_BATCH_ONE_LAUNCH && b->groups.size() > static_cast<size_t>(kMaxBatchSlots))
+    return set_err(CXG_ERR_UNSUPPORTED, "one-launch batch holds at most 8 element-type groups");
+  b->launch = mode;
+  return CXG_OK;
+}
+
+int cxg_batch_get_launch(const cxg_batch* b, int32_t* mode) {
+  if (!b || !mode) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad argument");
+  *mode = b->launch;
+  return CXG_OK;
+}
+
 int cxg_batch_assemble(cxg_batch* b, double* vals, double* rhs, const double* f_ext, void* stream) {
   if (!b || !vals) return set_err(CXG_ERR_INVALID_ARGUMENT, "batch and vals are required");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -486,7 +685,19 @@ int cxg_batch_assemble(cxg_batch* b, double* vals, double* rhs, const double* f_
     CHECK_CUDA(cudaMallocAsync(&df, 24 * b->n_nodes, s), "load staging");
     CHECK_CUDA(cudaMemcpyAsync(df, f_ext, 24 * b->n_nodes, cudaMemcpyHostToDevice, s), "load upload");
   }
-  for (Group& g : b->groups) CHECK_CUDA(launch_group(b, g, dv, dr, df, s), "batch assembly");
+  if (b->launch == CXG_BATCH_ONE_LAUNCH) {
+    std::vector<BatchSlotIn> slots;
+    rc = fill_slots(b, nullptr, dv, nullptr, dr, df, s, slots);
+    if (rc) {
+      if (hv) cudaFreeAsync(dv, s);
+      if (hr) cudaFreeAsync(dr, s);
+      if (hf) cudaFreeAsync(df, s);
+      return rc;
+    }
+    CHECK_CUDA(launch_one(b, slots, MODE_LINEAR, 3, s), "batch assembly (one launch)");
+  } else {
+    for (Group& g : b->groups) CHECK_CUDA(launch_group(b, g, dv, dr, df, s), "batch assembly");
+  }
   if (hv) CHECK_CUDA(cudaMemcpyAsync(vals, dv, 8 * b->nnz, cudaMemcpyDeviceToHost, s), "vals download");
   if (hr) CHECK_CUDA(cudaMemcpyAsync(rhs, dr, 8 * b->n_free, cudaMemcpyDeviceToHost, s), "rhs download");
   if (hv) cudaFreeAsync(dv, s);
@@ -510,16 +721,23 @@ int cxg_batch_graph_launch(cxg_batch* b, double* vals, double* rhs, const double
     }
     int rc = prepare(b);
     if (rc) return rc;
+    const bool one = b->launch == CXG_BATCH_ONE_LAUNCH;
+    std::vector<BatchSlotIn> slots;
+    if (one && (rc = fill_slots(b, nullptr, vals, nullptr, rhs, f_ext, s, slots))) return rc;
     // launch once outside capture so kernel attributes are set before capturing
-    for (Group& g : b->groups) CHECK_CUDA(launch_group(b, g, vals, rhs, f_ext, s), "batch assembly");
+    if (one)
+      CHECK_CUDA(launch_one(b, slots, MODE_LINEAR, 3, s), "batch assembly (one launch)");
+    else
+      for (Group& g : b->groups) CHECK_CUDA(launch_group(b, g, vals, rhs, f_ext, s), "batch assembly");
     cudaStream_t cs = nullptr;
     CHECK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
     CHECK_CUDA(cudaStreamSynchronize(s), "synchronize");
     cudaGraph_t graph = nullptr;
     cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-    if (err == cudaSuccess) err = cudaEventRecord(b->fork, cs);
+    if (err == cudaSuccess && one) err = launch_one(b, slots, MODE_LINEAR, 3, cs);
+    if (err == cudaSuccess && !one) err = cudaEventRecord(b->fork, cs);
     for (Group& g : b->groups) {
-      if (err != cudaSuccess) break;
+      if (err != cudaSuccess || one) break;
       err = cudaStreamWaitEvent(g.side, b->fork, 0);
       if (err == cudaSuccess) err = launch_group(b, g, vals, rhs, f_ext, g.side);
       if (err == cudaSuccess) err = cudaEventRecord(g.join, g.side);
@@ -564,6 +782,12 @@ int cxg_batch_tune(cxg_batch* b, double* vals, double* rhs, const double* f_ext,
   if (rc) return rc;
   std::map<std::string, CacheEntry> cache = read_cache(cache_path);
   bool changed = false;
+  if (b->launch == CXG_BATCH_ONE_LAUNCH) {
+    rc = tune_one_launch(b, vals, rhs, f_ext, cache, &changed, s);
+    if (!rc && changed && !write_cache(cache_path, cache))
+      rc = set_err(CXG_ERR_INVALID_ARGUMENT, std::string("cannot write tuning cache ") + cache_path);
+    return rc;
+  }
   cudaEvent_t e0, e1;
   CHECK_CUDA(cudaEventCreate(&e0), "event");
   CHECK_CUDA(cudaEventCreate(&e1), "event");
@@ -633,6 +857,14 @@ int cxg_batch_group_config(const cxg_batch* b, int32_t gi, int32_t* type, int32_
   if (!b || gi < 0 || gi >= static_cast<int32_t>(b->groups.size())) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad group");
   const Group& g = b->groups[static_cast<size_t>(gi)];
   const LaunchCfg& c = g.plan->cfg[b->precision];
+  if (b->launch == CXG_BATCH_ONE_LAUNCH) {
+    const int pr = b->precision ? 1 : 0;
+    if (type) *type = g.type;
+    if (tile) *tile = g.ftile[pr];
+    if (p1) *p1 = 0;
+    if (warps) *warps = b->fwarps[pr];
+    return CXG_OK;
+  }
   if (type) *type = g.type;
   if (tile) *tile = c.tile;
   if (p1) *p1 = c.p1_blocks_per_sm;
@@ -644,6 +876,14 @@ int cxg_batch_set_group_config(cxg_batch* b, int32_t gi, int32_t tile, int32_t p
   if (!b || gi < 0 || gi >= static_cast<int32_t>(b->groups.size())) return set_err(CXG_ERR_INVALID_ARGUMENT, "bad group");
   if (tile < 0 || tile > 2 || (tile == 2 && b->precision == CXG_FP64) || p1 < 0 || warps < 0 || warps > 8)
     return set_err(CXG_ERR_INVALID_ARGUMENT, "bad launch shape (4x4 tiles need mixed precision)");
+  if (b->launch == CXG_BATCH_ONE_LAUNCH) {
+    if (!batch_tile_ok(MODE_LINEAR, b->precision, tile))
+      return set_err(CXG_ERR_INVALID_ARGUMENT, "one-launch batch takes 2x2 tiles (and 2x4 in mixed precision)");
+    const int pr = b->precision ? 1 : 0;
+    b->groups[static_cast<size_t>(gi)].ftile[pr] = tile;
+    b->fwarps[pr] = warps;
+    return CXG_OK;
+  }
   LaunchCfg& c = b->groups[static_cast<size_t>(gi)].plan->cfg[b->precision];
   c.tile = tile;
   c.p1_blocks_per_sm = p1;
@@ -658,6 +898,19 @@ int cxg_batch_assemble_tangent(cxg_batch* b, const double* u, double* vals, doub
       (f_ext && !on_device(f_ext)))
     return set_err(CXG_ERR_INVALID_ARGUMENT, "batched tangent assembly needs device buffers");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (b->launch == CXG_BATCH_ONE_LAUNCH) {
+    for (Group& g : b->groups) {
+      g.plan->precision = b->precision;
+      int rc = ensure_state(g.plan, s);
+      if (!rc) rc = ensure_v2(g.plan, true);
+      if (rc) return rc;
+    }
+    std::vector<BatchSlotIn> slots;
+    const int rc = fill_slots(b, u, vals, f_int, rhs, f_ext, s, slots);
+    if (rc) return rc;
+    CHECK_CUDA(launch_one(b, slots, MODE_TANGENT, 3, s), "batch tangent (one launch)");
+    return CXG_OK;
+  }
   for (Group& g : b->groups) {
     cxg_plan* p = g.plan;
     p->precision = b->precision;

@@ -144,6 +144,21 @@ struct LaunchCfg {
   // of FP64
   int j2_fp32 = 0;
 };
+// One element pass and one row gather for a whole batch of element-type groups: slot k
+// is group k's arguments (one window, mesh node order), its element type and launch
+// shape; the weights share the persistent grid of each pass between the slots.
+constexpr int kMaxBatchSlots = 8;
+struct BatchSlotIn {
+  ElemArgs a;
+  V2Args v;
+  int32_t type = 0;
+  LaunchCfg cfg;
+  double p1_weight = 1.0, p2_weight = 1.0;
+};
+cudaError_t launch_v2_batch(int mode, int precision, const BatchSlotIn* slots, int n_slots, int passes,
+                            cudaStream_t s);
+// Tiles the batch kernels take (2x2; 2x4 in the mixed-precision linear pass).
+bool batch_tile_ok(int mode, int precision, int tile);
 size_t v2_edata_bytes(int elem_type, int64_t n_elems, int precision);
 // Bytes of element buffer per element (blocks, plus the internal force in tangent mode).
 size_t v2_bytes_per_element(int elem_type, int precision, bool tangent);

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 
 #include "cxg_internal.cuh"
@@ -429,8 +430,9 @@ constexpr int p1_min_blocks() {
 
 // J2F32 (mixed-precision material-point pass only): the J2 return in FP32
 // (j2_point_mixed) instead of FP64.
+// bid / nblk: this block's index among the nblk blocks that share the element range.
 template <int ET, int MODE, typename R, int TILE, bool J2F32>
-__global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_kernel(ElemArgs A, V2Args V) {
+__device__ __forceinline__ void p1_body(const ElemArgs& A, const V2Args& V, unsigned bid, unsigned nblk) {
   using G = Geo<ET, TILE>;
   constexpr int n = G::n, nq = G::nq, npad = G::npad, EPW = G::EPW, NT = G::NT, NB = G::NB;
   constexpr int TR = G::TR, TC = G::TC;
@@ -458,8 +460,8 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
   }
   __syncthreads();
 
-  const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * kW1 + warp;
-  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kW1;
+  const int64_t gwarp = static_cast<int64_t>(bid) * kW1 + warp;
+  const int64_t nwarps = static_cast<int64_t>(nblk) * kW1;
   const int64_t e_end = V.e_end;  // elements [V.e_begin, V.e_end) of this window
   // The connectivity of a warp's next elements is loaded while it integrates the current
   // ones, so the coordinate gather of the next iteration waits for one round of loads.
@@ -820,6 +822,11 @@ __global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_
   }
 }
 
+template <int ET, int MODE, typename R, int TILE, bool J2F32>
+__global__ void __launch_bounds__(kT1, (p1_min_blocks<ET, MODE, R, TILE>())) p1_kernel(ElemArgs A, V2Args V) {
+  p1_body<ET, MODE, R, TILE, J2F32>(A, V, blockIdx.x, gridDim.x);
+}
+
 // ---- P2: row gather ------------------------------------------------------------------
 // One warp per node a. The node's three rows are staged in shared memory at full width:
 // row i holds 3 entries for each node of a's adjacency list (position s, from the
@@ -884,7 +891,7 @@ __device__ __forceinline__ void p2_fetch(const ElemArgs& A, const V2Args& V, con
 }
 
 template <int ET, bool TAN, typename R, bool DIAGFIX, bool WIN>
-__device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
+__device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V, unsigned bid, unsigned nblk) {
   constexpr int n = nodes_of(ET);
   constexpr int GS = P2Geo<ET, DIAGFIX>::GS, EG = P2Geo<ET, DIAGFIX>::EG;
   constexpr unsigned kAll = 0xffffffffu;
@@ -892,8 +899,8 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int stride = static_cast<int>(V.row_stride);  // doubles of one row-buffer copy
   double* buf = reinterpret_cast<double*>(smem) + warp * (EG * stride);
-  const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
-  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  const int64_t gwarp = static_cast<int64_t>(bid) * (blockDim.x >> 5) + warp;
+  const int64_t nwarps = static_cast<int64_t>(nblk) * (blockDim.x >> 5);
   const R* ed = reinterpret_cast<const R*>(V.edata);
   const int sub = lane / GS, lb = lane % GS;
   const bool lane_ok = lb < n;
@@ -1086,7 +1093,7 @@ __device__ __forceinline__ void p2_body(const ElemArgs& A, const V2Args& V) {
 // compiled without either, so it keeps the registers of a plain node loop.
 template <int ET, bool TAN, typename R, bool DIAGFIX, bool WIN>
 __global__ void p2_kernel(ElemArgs A, V2Args V) {
-  p2_body<ET, TAN, R, DIAGFIX, WIN>(A, V);
+  p2_body<ET, TAN, R, DIAGFIX, WIN>(A, V, blockIdx.x, gridDim.x);
 }
 
 int sm_count() {
@@ -1376,6 +1383,263 @@ cudaError_t launch_v2(int t, int mode, int precision, const ElemArgs& a, const V
     case C3D15: return launch_v2_type<C3D15>(mode, precision, a, v, c, s);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// ---- one launch per pass for a batch of element-type groups ---------------------------
+// Slot k of a pass is one group (one element type, the concatenated models of that type)
+// and owns blocks [blk0_k, blk0_{k+1}) of the grid. A block copies its slot's arguments
+// into shared memory and runs the group's element-pass or row-gather body with its
+// index among the slot's blocks in place of blockIdx. The bodies are the ones the
+// per-group kernels inline, so every value is the same bit for bit; the kernel holds
+// the largest register count of its bodies, which is what a group pays for sharing
+// the launch.
+struct BatchSlot {
+  ElemArgs a;
+  V2Args v;
+  int64_t blk0;
+  int32_t type, tile;
+};
+struct BatchPass {
+  BatchSlot s[kMaxBatchSlots];
+  int32_t n;
+};
+static_assert(sizeof(BatchPass) <= 4096, "batch pass arguments exceed the kernel parameter space");
+
+// Block-uniform: slot of this block, copied to S; returns the slot's block count.
+__device__ __forceinline__ unsigned take_slot(const BatchPass& P, BatchSlot& S) {
+  int k = 0;
+  while (k + 1 < P.n && static_cast<int64_t>(blockIdx.x) >= P.s[k + 1].blk0) ++k;
+  const uint64_t* src = reinterpret_cast<const uint64_t*>(&P.s[k]);
+  uint64_t* dst = reinterpret_cast<uint64_t*>(&S);
+  for (int i = threadIdx.x; i < static_cast<int>(sizeof(BatchSlot) / 8); i += blockDim.x) dst[i] = src[i];
+  const int64_t end = k + 1 < P.n ? P.s[k + 1].blk0 : static_cast<int64_t>(gridDim.x);
+  __syncthreads();
+  return static_cast<unsigned>(end - S.blk0);
+}
+
+template <int ET, int MODE, typename R, int TILE, bool J2F32>
+__device__ __forceinline__ void p1_slot(const ElemArgs& A, const V2Args& V, unsigned bid, unsigned nblk) {
+  p1_body<ET, MODE, R, TILE, J2F32>(A, V, bid, nblk);
+}
+
+// The batch kernels carry the tiles whose accumulators fit 168 registers, so that 3
+// blocks of 4 warps stay resident per SM whatever families share the launch: 2x2
+// everywhere and 2x4 in the mixed-precision linear pass.
+bool batch_tile_ok(int mode, int precision, int tile) {
+  return tile == 1 || (tile == 0 && mode == MODE_LINEAR && precision);
+}
+
+template <int ET, int MODE, typename R, bool J2F32>
+__device__ __forceinline__ void p1_slot_tile(int tile, const ElemArgs& A, const V2Args& V, unsigned bid, unsigned nblk) {
+  if constexpr (MODE == MODE_LINEAR && sizeof(R) == 4) {
+    if (tile == 0) {
+      p1_slot<ET, MODE, R, 0, J2F32>(A, V, bid, nblk);
+      return;
+    }
+  }
+  p1_slot<ET, MODE, R, 1, J2F32>(A, V, bid, nblk);
+}
+
+template <int MODE, typename R, bool J2F32>
+__global__ void __launch_bounds__(kT1, 3) p1_batch_kernel(const __grid_constant__ BatchPass P) {
+  __shared__ __align__(16) BatchSlot S;
+  const unsigned nblk = take_slot(P, S);
+  const unsigned bid = blockIdx.x - static_cast<unsigned>(S.blk0);
+  switch (S.type) {
+    case C3D4: p1_slot_tile<C3D4, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
+    case C3D10: p1_slot_tile<C3D10, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
+    case C3D8: p1_slot_tile<C3D8, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
+    case C3D8R: p1_slot_tile<C3D8R, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
+    case C3D20: p1_slot_tile<C3D20, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
+    case C3D20R: p1_slot_tile<C3D20R, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
+    case C3D6: p1_slot_tile<C3D6, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
+    case C3D15: p1_slot_tile<C3D15, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
+    default: break;
+  }
+}
+
+template <int ET, bool TAN, typename R, bool DF>
+__device__ __forceinline__ void p2_slot(const ElemArgs& A, const V2Args& V, unsigned bid, unsigned nblk) {
+  p2_body<ET, TAN, R, DF, false>(A, V, bid, nblk);
+}
+
+template <bool TAN, typename R, bool DF>
+__global__ void p2_batch_kernel(const __grid_constant__ BatchPass P) {
+  __shared__ __align__(16) BatchSlot S;
+  const unsigned nblk = take_slot(P, S);
+  const unsigned bid = blockIdx.x - static_cast<unsigned>(S.blk0);
+  switch (S.type) {
+    case C3D4: p2_slot<C3D4, TAN, R, DF>(S.a, S.v, bid, nblk); break;
+    case C3D10: p2_slot<C3D10, TAN, R, DF>(S.a, S.v, bid, nblk); break;
+    case C3D8: p2_slot<C3D8, TAN, R, DF>(S.a, S.v, bid, nblk); break;
+    case C3D8R: p2_slot<C3D8R, TAN, R, DF>(S.a, S.v, bid, nblk); break;
+    case C3D20: p2_slot<C3D20, TAN, R, DF>(S.a, S.v, bid, nblk); break;
+    case C3D20R: p2_slot<C3D20R, TAN, R, DF>(S.a, S.v, bid, nblk); break;
+    case C3D6: p2_slot<C3D6, TAN, R, DF>(S.a, S.v, bid, nblk); break;
+    case C3D15: p2_slot<C3D15, TAN, R, DF>(S.a, S.v, bid, nblk); break;
+    default: break;
+  }
+}
+
+// Per-(family, tile) figures the launcher needs at run time.
+struct P1Shape {
+  size_t smem = 0;
+  int epw = 1;
+};
+template <int ET, int MODE, typename R, int TILE>
+P1Shape p1_shape_of() {
+  return {p1_smem_bytes<ET, MODE, R, TILE>(), Geo<ET, TILE>::EPW};
+}
+template <int ET, int MODE, typename R>
+P1Shape p1_shape_tile(int tile) {
+  if constexpr (MODE == MODE_LINEAR && sizeof(R) == 4) {
+    if (tile == 0) return p1_shape_of<ET, MODE, R, 0>();
+  }
+  return p1_shape_of<ET, MODE, R, 1>();
+}
+template <int MODE, typename R>
+P1Shape p1_shape(int t, int tile) {
+  switch (t) {
+    case C3D4: return p1_shape_tile<C3D4, MODE, R>(tile);
+    case C3D10: return p1_shape_tile<C3D10, MODE, R>(tile);
+    case C3D8: return p1_shape_tile<C3D8, MODE, R>(tile);
+    case C3D8R: return p1_shape_tile<C3D8R, MODE, R>(tile);
+    case C3D20: return p1_shape_tile<C3D20, MODE, R>(tile);
+    case C3D20R: return p1_shape_tile<C3D20R, MODE, R>(tile);
+    case C3D6: return p1_shape_tile<C3D6, MODE, R>(tile);
+    default: return p1_shape_tile<C3D15, MODE, R>(tile);
+  }
+}
+int p2_groups_of(int t, bool df) {
+  const int n = nodes_of(t);
+  (void)df;
+  return n <= 16 ? 2 : 1;  // P2Geo::EG
+}
+
+// Blocks of a persistent grid of `total` blocks shared out in proportion to the
+// slots' weights, at least one and at most `need` per slot.
+void share_blocks(const double* weight, const int64_t* need, int n, int64_t total, int64_t* grid) {
+  double sum = 0.0;
+  for (int k = 0; k < n; ++k) sum += weight[k] > 0.0 ? weight[k] : 0.0;
+  for (int k = 0; k < n; ++k) {
+    const double f = sum > 0.0 ? std::max(weight[k], 0.0) / sum : 1.0 / n;
+    const int64_t g = static_cast<int64_t>(std::llround(f * static_cast<double>(total)));
+    grid[k] = std::max<int64_t>(1, std::min<int64_t>(need[k], g));
+  }
+}
+
+template <int MODE, typename R, bool J2F32>
+cudaError_t launch_p1_batch(const BatchSlotIn* in, int n, cudaStream_t s) {
+  auto kern = p1_batch_kernel<MODE, R, J2F32>;
+  BatchPass P{};
+  size_t smem = 0;
+  int64_t need[kMaxBatchSlots], grid[kMaxBatchSlots];
+  double w[kMaxBatchSlots];
+  for (int k = 0; k < n; ++k) {
+    const P1Shape sh = p1_shape<MODE, R>(in[k].type, in[k].cfg.tile);
+    smem = std::max(smem, sh.smem);
+    const int64_t count = in[k].v.e_end - in[k].v.e_begin;
+    need[k] = std::max<int64_t>(1, (count + kW1 * sh.epw - 1) / (kW1 * sh.epw));
+    w[k] = in[k].p1_weight;
+  }
+  if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  int per_sm = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT1, smem);
+  if (err != cudaSuccess) return err;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  share_blocks(w, need, n, static_cast<int64_t>(per_sm) * sm_count(), grid);
+  int64_t blk = 0;
+  for (int k = 0; k < n; ++k) {
+    P.s[k].a = in[k].a;
+    P.s[k].v = in[k].v;
+    P.s[k].blk0 = blk;
+    P.s[k].type = in[k].type;
+    P.s[k].tile = in[k].cfg.tile;
+    blk += grid[k];
+  }
+  P.n = n;
+  kern<<<static_cast<unsigned>(blk), kT1, smem, s>>>(P);
+  return cudaGetLastError();
+}
+
+template <bool TAN, typename R, bool DF>
+cudaError_t launch_p2_batch(const BatchSlotIn* in, int n, cudaStream_t s) {
+  auto kern = p2_batch_kernel<TAN, R, DF>;
+  BatchPass P{};
+  // one block shape for every slot: the most warps every slot's row buffers allow in
+  // ~160 KB, at most 8 (or the smallest configured count)
+  int warps = 8;
+  int64_t wbytes_max = 0;
+  for (int k = 0; k < n; ++k) {
+    const int64_t stride = std::max<int64_t>(2, (9 * in[k].v.max_adj + 1) / 2 * 2);
+    const int64_t wbytes = p2_groups_of(in[k].type, DF) * stride * 8;
+    wbytes_max = std::max(wbytes_max, wbytes);
+    if (in[k].cfg.p2_warps > 0) warps = std::min(warps, in[k].cfg.p2_warps);
+  }
+  while (warps > 1 && warps * wbytes_max > 160 * 1024) warps /= 2;
+  const size_t smem = static_cast<size_t>(warps) * wbytes_max;
+  if (smem > 220 * 1024) return cudaErrorInvalidConfiguration;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  int per_sm = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
+  if (err != cudaSuccess) return err;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  int64_t need[kMaxBatchSlots], grid[kMaxBatchSlots];
+  double w[kMaxBatchSlots];
+  for (int k = 0; k < n; ++k) {
+    const int64_t count = in[k].v.n_end - in[k].v.n_begin;
+    need[k] = std::max<int64_t>(1, (count + warps - 1) / warps);
+    w[k] = in[k].p2_weight;
+  }
+  share_blocks(w, need, n, static_cast<int64_t>(per_sm) * sm_count(), grid);
+  int64_t blk = 0;
+  for (int k = 0; k < n; ++k) {
+    P.s[k].a = in[k].a;
+    P.s[k].v = in[k].v;
+    P.s[k].v.row_stride = std::max<int64_t>(2, (9 * in[k].v.max_adj + 1) / 2 * 2);
+    P.s[k].blk0 = blk;
+    P.s[k].type = in[k].type;
+    P.s[k].tile = in[k].cfg.tile;
+    blk += grid[k];
+  }
+  P.n = n;
+  kern<<<static_cast<unsigned>(blk), warps * 32, smem, s>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_v2_batch(int mode, int precision, const BatchSlotIn* in, int n, int passes, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (n > kMaxBatchSlots) return cudaErrorInvalidValue;
+  const bool j2f32 = mode == MODE_TANGENT && precision && in[0].cfg.j2_fp32;
+  for (int k = 0; k < n; ++k) {
+    if (in[k].type < kFirstType || in[k].type > kLastType || in[k].v.n_win > 1 || in[k].v.node_order)
+      return cudaErrorInvalidValue;
+    if ((mode == MODE_TANGENT && precision && (in[k].cfg.j2_fp32 != 0) != j2f32) ||
+        !batch_tile_ok(mode, precision, in[k].cfg.tile))
+      return cudaErrorInvalidValue;
+  }
+  cudaError_t err = cudaSuccess;
+  if (passes & 1) {
+    if (mode == MODE_LINEAR)
+      err = precision ? launch_p1_batch<MODE_LINEAR, float, false>(in, n, s)
+                      : launch_p1_batch<MODE_LINEAR, double, false>(in, n, s);
+    else if (precision)
+      err = j2f32 ? launch_p1_batch<MODE_TANGENT, float, true>(in, n, s)
+                  : launch_p1_batch<MODE_TANGENT, float, false>(in, n, s);
+    else
+      err = launch_p1_batch<MODE_TANGENT, double, false>(in, n, s);
+    if (err != cudaSuccess) return err;
+  }
+  if (passes & 2) {
+    if (mode == MODE_LINEAR)
+      err = precision ? launch_p2_batch<false, float, true>(in, n, s) : launch_p2_batch<false, double, false>(in, n, s);
+    else
+      err = precision ? launch_p2_batch<true, float, true>(in, n, s) : launch_p2_batch<true, double, false>(in, n, s);
+  }
+  return err;
 }
 
 cudaError_t launch_scalar_pass(int t, int kind, const ElemArgs& a, const V2Args& v, const double* density,

@@ -391,8 +391,9 @@ CXG_API int cxg_adjoint_compliance(cxg_plan* plan, const double* u, double* dc_d
  * maps concatenated in input order) that one element pass and one row gather
  * assemble. All models' outputs share one vals and one rhs buffer at the offsets that
  * cxg_batch_get_model_info reports, and the load vector is read at 3 * node_offset.
- * Groups are ordered by element type code. Models whose material has a *PLASTIC table
- * are rejected with CXG_ERR_UNSUPPORTED. */
+ * Groups are ordered by element type code. Models may be elastic or J2 (materials with a
+ * *PLASTIC table); cxg_batch_assemble_tangent assembles the material-point tangent of
+ * every model at once. */
 typedef struct cxg_batch cxg_batch;
 
 typedef struct {
@@ -426,6 +427,21 @@ CXG_API int cxg_batch_get_model_info(const cxg_batch* batch, int32_t model, cxg_
  * model's equation numbers. */
 CXG_API int cxg_batch_get_pattern(const cxg_batch* batch, int32_t model, int64_t* row_ptr, int32_t* col_idx);
 CXG_API int cxg_batch_set_precision(cxg_batch* batch, int32_t precision);
+/* How one assembly of the batch is launched. CXG_BATCH_PER_GROUP (the default): one
+ * element pass and one row gather per element-type group, the groups as independent
+ * branches of the graph form. CXG_BATCH_ONE_LAUNCH: one element pass and one row
+ * gather for the whole batch (at most 8 groups, one window each), every group a slot
+ * of the same persistent grid with a share of its blocks in proportion to the group's
+ * pass time as cxg_batch_tune measures it (estimated from the element counts until
+ * then). Its element pass takes 2x2 tiles, and 2x4 in mixed precision; the kernel
+ * holds the register count of its largest family. Results are the same bit for bit in
+ * both modes. Applies to cxg_batch_assemble, cxg_batch_graph_launch,
+ * cxg_batch_assemble_tangent and cxg_batch_tune; cxg_batch_group_config and
+ * cxg_batch_set_group_config read and pin the current mode's shapes. */
+#define CXG_BATCH_PER_GROUP 0
+#define CXG_BATCH_ONE_LAUNCH 1
+CXG_API int cxg_batch_set_launch(cxg_batch* batch, int32_t mode);
+CXG_API int cxg_batch_get_launch(const cxg_batch* batch, int32_t* mode);
 /* Assemble every model on `stream` (vals, rhs, f_ext host or device; f_ext may be
  * NULL). */
 CXG_API int cxg_batch_assemble(cxg_batch* batch, double* vals, double* rhs, const double* f_ext, void* stream);
