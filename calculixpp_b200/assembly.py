@@ -270,6 +270,9 @@ class Plan:
                 t.append(s.elapsed_time(e))
             return sorted(t)[len(t) // 2]
 
+        # every launch shape is timed with one window first (a budget left by an earlier
+        # tuning, e.g. of the other precision, would otherwise stand in for it)
+        self.set_ring_bytes(0)
         best = None
         for tile in ((0, 1) if tangent else (0, 1, 2)):
             for bps in (0, 1, 2):
