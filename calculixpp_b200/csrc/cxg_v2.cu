@@ -1387,9 +1387,11 @@ cudaError_t launch_v2(int t, int mode, int precision, const ElemArgs& a, const V
 
 // ---- one launch per pass for a batch of element-type groups ---------------------------
 // Slot k of a pass is one group (one element type, the concatenated models of that type)
-// and owns blocks [blk0_k, blk0_{k+1}) of the grid. A block copies its slot's arguments
-// into shared memory and runs the group's element-pass or row-gather body with its
-// index among the slot's blocks in place of blockIdx. The bodies are the ones the
+// and owns blocks [blk0_k, blk0_{k+1}) of the grid. A block reads its slot's arguments
+// in place from the kernel's parameter space (a copy in shared memory measured slower:
+// the bodies' shared-memory stores made every argument a reload) and runs the group's
+// element-pass or row-gather body with its index among the slot's blocks in place of
+// blockIdx. The bodies are the ones the
 // per-group kernels inline, so every value is the same bit for bit; the kernel holds
 // the largest register count of its bodies, which is what a group pays for sharing
 // the launch.
@@ -1405,16 +1407,18 @@ struct BatchPass {
 };
 static_assert(sizeof(BatchPass) <= 4096, "batch pass arguments exceed the kernel parameter space");
 
-// Block-uniform: slot of this block, copied to S; returns the slot's block count.
-__device__ __forceinline__ unsigned take_slot(const BatchPass& P, BatchSlot& S) {
+// Slot of this block (block-uniform).
+__device__ __forceinline__ int slot_of(const BatchPass& P) {
   int k = 0;
   while (k + 1 < P.n && static_cast<int64_t>(blockIdx.x) >= P.s[k + 1].blk0) ++k;
-  const uint64_t* src = reinterpret_cast<const uint64_t*>(&P.s[k]);
-  uint64_t* dst = reinterpret_cast<uint64_t*>(&S);
-  for (int i = threadIdx.x; i < static_cast<int>(sizeof(BatchSlot) / 8); i += blockDim.x) dst[i] = src[i];
+  return k;
+}
+
+// This block's index among its slot's blocks, and their count.
+__device__ __forceinline__ void slot_blocks(const BatchPass& P, int k, unsigned& bid, unsigned& nblk) {
   const int64_t end = k + 1 < P.n ? P.s[k + 1].blk0 : static_cast<int64_t>(gridDim.x);
-  __syncthreads();
-  return static_cast<unsigned>(end - S.blk0);
+  bid = blockIdx.x - static_cast<unsigned>(P.s[k].blk0);
+  nblk = static_cast<unsigned>(end - P.s[k].blk0);
 }
 
 template <int ET, int MODE, typename R, int TILE, bool J2F32>
@@ -1442,9 +1446,11 @@ __device__ __forceinline__ void p1_slot_tile(int tile, const ElemArgs& A, const 
 
 template <int MODE, typename R, bool J2F32>
 __global__ void __launch_bounds__(kT1, 3) p1_batch_kernel(const __grid_constant__ BatchPass P) {
-  __shared__ __align__(16) BatchSlot S;
-  const unsigned nblk = take_slot(P, S);
-  const unsigned bid = blockIdx.x - static_cast<unsigned>(S.blk0);
+  // the slot's arguments are read in place from the (read-only) parameter space
+  const int k = slot_of(P);
+  const BatchSlot& S = P.s[k];
+  unsigned bid, nblk;
+  slot_blocks(P, k, bid, nblk);
   switch (S.type) {
     case C3D4: p1_slot_tile<C3D4, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
     case C3D10: p1_slot_tile<C3D10, MODE, R, J2F32>(S.tile, S.a, S.v, bid, nblk); break;
@@ -1465,9 +1471,10 @@ __device__ __forceinline__ void p2_slot(const ElemArgs& A, const V2Args& V, unsi
 
 template <bool TAN, typename R, bool DF>
 __global__ void p2_batch_kernel(const __grid_constant__ BatchPass P) {
-  __shared__ __align__(16) BatchSlot S;
-  const unsigned nblk = take_slot(P, S);
-  const unsigned bid = blockIdx.x - static_cast<unsigned>(S.blk0);
+  const int k = slot_of(P);
+  const BatchSlot& S = P.s[k];
+  unsigned bid, nblk;
+  slot_blocks(P, k, bid, nblk);
   switch (S.type) {
     case C3D4: p2_slot<C3D4, TAN, R, DF>(S.a, S.v, bid, nblk); break;
     case C3D10: p2_slot<C3D10, TAN, R, DF>(S.a, S.v, bid, nblk); break;
