@@ -1517,11 +1517,9 @@ P1Shape p1_shape(int t, int tile) {
     default: return p1_shape_tile<C3D15, MODE, R>(tile);
   }
 }
-int p2_groups_of(int t, bool df) {
-  const int n = nodes_of(t);
-  (void)df;
-  return n <= 16 ? 2 : 1;  // P2Geo::EG
-}
+// Row-buffer copies per warp of the row gather (P2Geo::EG): two 16-lane groups for the
+// families of at most 16 nodes, one 32-lane group above.
+int p2_groups_of(int t) { return nodes_of(t) <= 16 ? 2 : 1; }
 
 // Blocks of a persistent grid of `total` blocks shared out in proportion to the
 // slots' weights, at least one and at most `need` per slot.
@@ -1581,7 +1579,7 @@ cudaError_t launch_p2_batch(const BatchSlotIn* in, int n, cudaStream_t s) {
   int64_t wbytes_max = 0;
   for (int k = 0; k < n; ++k) {
     const int64_t stride = std::max<int64_t>(2, (9 * in[k].v.max_adj + 1) / 2 * 2);
-    const int64_t wbytes = p2_groups_of(in[k].type, DF) * stride * 8;
+    const int64_t wbytes = p2_groups_of(in[k].type) * stride * 8;
     wbytes_max = std::max(wbytes_max, wbytes);
     if (in[k].cfg.p2_warps > 0) warps = std::min(warps, in[k].cfg.p2_warps);
   }

@@ -437,7 +437,9 @@ CXG_API int cxg_batch_set_precision(cxg_batch* batch, int32_t precision);
  * holds the register count of its largest family. Results are the same bit for bit in
  * both modes. Applies to cxg_batch_assemble, cxg_batch_graph_launch,
  * cxg_batch_assemble_tangent and cxg_batch_tune; cxg_batch_group_config and
- * cxg_batch_set_group_config read and pin the current mode's shapes. */
+ * cxg_batch_set_group_config read and pin the current mode's shapes (in the one-launch
+ * mode the row gather's warps per block are one value for the whole batch, the last one
+ * set, and the element-pass blocks per SM are not used). */
 #define CXG_BATCH_PER_GROUP 0
 #define CXG_BATCH_ONE_LAUNCH 1
 CXG_API int cxg_batch_set_launch(cxg_batch* batch, int32_t mode);
