@@ -231,7 +231,7 @@ def j2_newton(args, world, dev, stream):
                         "state_max_abs": float((sm - s64).abs().max())},
         "roofline_fp64": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                           "traffic": traffic.get(f"c3d8_j2_{args.j2_n}_fp64_tangent"),
-                          "kernel": "p1_kernel + p2_kernel (element pass with J2 return + row gather), C3D8 tangent, FP64",
+                          "kernel": "p1_kernel + p2_kernel_small (element pass with J2 return + row gather), C3D8 tangent, FP64",
                           "algorithmic_bytes": B, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "gpu_launches_per_step": 2,
     }

@@ -1096,6 +1096,14 @@ __global__ void p2_kernel(ElemArgs A, V2Args V) {
   p2_body<ET, TAN, R, DIAGFIX, WIN>(A, V, blockIdx.x, gridDim.x);
 }
 
+// The gather of the <= 8-node families, compiled for 5 resident 8-warp blocks per SM
+// (<= 48 registers): their row buffers are small, so registers, not shared memory, bound
+// their resident warps, and the latency-bound gather runs faster with more of them.
+template <int ET, bool TAN, typename R, bool DIAGFIX, bool WIN>
+__global__ void __launch_bounds__(256, 5) p2_kernel_small(ElemArgs A, V2Args V) {
+  p2_body<ET, TAN, R, DIAGFIX, WIN>(A, V, blockIdx.x, gridDim.x);
+}
+
 int sm_count() {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -1147,6 +1155,8 @@ cudaError_t launch_p1_t(const ElemArgs& a, const V2Args& v, const LaunchCfg& cfg
 template <int ET, bool TAN, typename R, bool DF>
 cudaError_t launch_p2_t(const ElemArgs& a, V2Args v, const LaunchCfg& cfg, cudaStream_t s) {
   auto kern = v.node_order ? p2_kernel<ET, TAN, R, DF, true> : p2_kernel<ET, TAN, R, DF, false>;
+  if constexpr (nodes_of(ET) <= 8)
+    kern = v.node_order ? p2_kernel_small<ET, TAN, R, DF, true> : p2_kernel_small<ET, TAN, R, DF, false>;
   // warps per block: as many as fit in ~160 KB of row buffers, up to 8 (or the
   // configured count when it fits). Per warp: EG full-width copies of three rows of
   // 3 x max_adj doubles. (Shared memory beyond that comes out of the L1 cache the
